@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the fused B200 step on the scaled-cascade
+workload (1e7 electrons, gamma0 = 2000 +- 1 %, sigma_perp = 1 um,
+sigma_par = 5 um, head-on with a linearly polarised Gaussian pulse a0 = 200,
+lambda = 0.8 um, w0 = 3 um, 25 fs intensity FWHM; photon emission and pair
+creation; dt = T0/100; 3000 steps).  Synthetic, seeded inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one simulation step of the whole cascade (all species).
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own
+instance (seed = rank): weak scaling with no data-path collective; the time
+is the max over ranks of CUDA-event time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+C = 299792458.0
+LAMBDA = 0.8e-6
+T0 = LAMBDA / C
+FWHM = 25e-15
+CTAU = C * FWHM / (2 * math.sqrt(math.log(2) / 2))  # 1/e field half-width from the intensity FWHM
+A0 = 200.0
+W0 = 3e-6
+GAMMA0 = 2000.0
+STEPS_FULL = 3000
+DT = T0 / 100
+# algorithmic bytes per particle-step (float64 state read once + written once)
+BYTES_EPM = 97   # x,y,z,ux,uy,uz read+write + alive flag
+BYTES_PHOTON = 73  # x,y,z,ux,uy,uz read + alive flag + position write
+BYTES_APPEND = 49  # appended particle: state + flag written
+
+WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
+           "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
+
+
+def beam(n, seed, steps=STEPS_FULL):
+    rng = np.random.default_rng(seed)
+    L = C * (steps * DT) / 2
+    g = GAMMA0 * (1 + 0.01 * rng.normal(size=n))
+    x = rng.normal(-L, 5e-6, n)
+    y = rng.normal(0, 1e-6, n)
+    z = rng.normal(0, 1e-6, n)
+    return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
+
+
+def make_sim(n, seed, form="fp64"):
+    import sfparticles_b200 as S
+    from sfparticles_b200.fields import gaussian_laser_pulse
+    props, L = beam(n, seed)
+    ele = S.Particles("electron", -1, 1, N=n, props=props)
+    pos = S.Particles("positron", 1, 1)
+    pho = S.Particles("photon", 0, 0)
+    ele.set_photon(pho)
+    pos.set_photon(pho)
+    pho.set_pair(ele, pos)
+    fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
+    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form)
+    return sim
+
+
+def make_oracle_sim(n, seed):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+    from sfparticles_b200.qed import tables
+    props, L = beam(n, seed)
+    ele = orc.Species("electron", -1, 1, N=n, props=props)
+    pos = orc.Species("positron", 1, 1)
+    pho = orc.Species("photon", 0, 0)
+    ele.set_photon(pho)
+    pos.set_photon(pho)
+    pho.set_pair(ele, pos)
+    iA, dA, _, zmax = tables.rs_tables()
+    terms = orc.gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
+    return orc.OracleSim([ele, pos, pho], DT, terms, ("rs", iA, dA), seed=seed, z_max=zmax)
+
+
+def cpu_sample(n_e, max_steps, budget_s, warmup):
+    """Oracle port (C, OpenMP, all host threads) on a bounded sample."""
+    sim = make_oracle_sim(n_e, 12345)
+    sim.run(warmup)
+    ps0 = sim.particle_steps
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and time.perf_counter() - t0 < budget_s:
+        sim.run(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    ps = sim.particle_steps - ps0
+    return ps / dt, steps, ps, dt
+
+
+def omp_threads():
+    v = os.environ.get("OMP_NUM_THREADS")
+    return int(v) if v else (os.cpu_count() or 1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_ours(args, rank, world):
+    import torch
+    import sfparticles_b200 as S
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    seed = 1000 + rank
+    # warm-up: compile / load the module, W steps of a small instance, then a fresh timed instance
+    wsim = make_sim(max(1000, args.electrons // 1000), seed, args.form)
+    wsim.run_on_device(args.warmup)
+    wsim.finish()
+    del wsim
+    sim = make_sim(args.electrons, seed, args.form)
+    sim._begin()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = sim.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        e0.record()
+        sim.run_on_device(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sim.kernel_launches - launches0
+    ps = sim.particle_steps
+    counts = {p.name: p.N_buffered for p in sim.all_particles}
+    # roofline of the step kernel at the final state: CUDA events around each launch
+    alive = {p.name: p.Npart for p in sim.all_particles}
+    kms, before, after = sim.time_step_kernel(args.roofline_steps)
+    k_avg_ms = float(np.mean(kms))
+    appended = (sum(after) - sum(before)) / args.roofline_steps
+    alg_bytes = ((alive["electron"] + alive["positron"]) * BYTES_EPM + alive["photon"] * BYTES_PHOTON
+                 + appended * BYTES_APPEND)
+    sim.finish()
+    del sim
+    torch.cuda.empty_cache()
+
+    # end to end through the public API from host arrays
+    e2e = None
+    if not args.no_e2e:
+        sim2 = make_sim(args.electrons, seed, args.form)
+        h2d = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record()
+        sim2.start(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms2 = e0.elapsed_time(e1)
+        d2h = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
+        e2e = dict(value=sim2.particle_steps / (max(ms2, wall * 1e3) * 1e-3), unit="particle-steps/s",
+                   h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
+                   wall_s=wall)
+        del sim2
+
+    # max over ranks of the device time; sum of work
+    tot_ps = ps
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        w = torch.tensor([float(ps)], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+        tot_ps = float(w.item())
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / (k_avg_ms * 1e-3) / 1e9
+    return dict(ms=ms, particle_steps=tot_ps, counts=counts, launches=launches, clocks=clk.summary(),
+                roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                          "kernel": "sfp_step_" + args.form + "_rs", "kernel_avg_ms": k_avg_ms,
+                          "alg_bytes_per_launch": alg_bytes, "launches_timed": args.roofline_steps},
+                e2e=e2e)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=STEPS_FULL)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--electrons", type=int, default=10_000_000)
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--roofline-steps", type=int, default=8)
+    ap.add_argument("--cpu-electrons", type=int, default=10_000)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference's CPU algorithm (oracle port) on the host cores; rank 0 only
+        if rank != 0:
+            return
+        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, args.steps, args.cpu_budget * 3, args.warmup)
+        cores = omp_threads()
+        sample = f"{args.cpu_electrons} e- of the same cascade, {steps} steps after {args.warmup} warm-up"
+        line = {"impl": "reference", "metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
+                "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(steps, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "sample_electrons": args.cpu_electrons},
+                "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    # CPU baseline first (rank 0, N=1), before any CUDA context exists
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, STEPS_FULL, args.cpu_budget, 1)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": omp_threads(), "kind": "port",
+               "sample": f"{args.cpu_electrons} e- of the same cascade (1/1000 of the beam), first {steps} steps, "
+                         f"{ps:.3g} particle-steps in {dt:.1f}s"}
+
+    r = run_ours(args, rank, world)
+    if rank == 0:
+        value = r["particle_steps"] / (r["ms"] * 1e-3)
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "electrons_per_gpu": args.electrons, "form": args.form,
+                           "l2": "state > 1 GB per step, larger than L2 (no flush needed)",
+                           "final_counts": r["counts"]},
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
+                "clocks": r["clocks"], "particle_steps": r["particle_steps"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,167 @@
+/*
+ * sfp.h -- C-ABI of libsfp.so, the B200 implementation of the sfparticles
+ * per-particle step.
+ *
+ * Conventions
+ *   - every entry point returns 0 on success or a negative SFP_E* code; the
+ *     message of the last failure on the calling thread is sfp_last_error();
+ *   - array arguments are DEVICE pointers (float64 / uint8 bool / int64);
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default);
+ *   - no entry point synchronises the device unless it says so.
+ *
+ * Reference interfaces replaced (paths inside xsgeng/sfparticles v0.4.12):
+ * the 12 kernels bound at sfparticles/particles.py:14-25 (from cpu.py /
+ * gpu.py), the QED samplers bound at particles.py:8-12, the field launcher
+ * Fields.field_func (fields.py:26-49, called at particles.py:310-323) and the
+ * step loop Simulation.start (simulation.py:74-160).
+ */
+#ifndef SFP_H
+#define SFP_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "sfp_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFP_OK 0
+#define SFP_EINVAL (-1)   /* bad argument                                  */
+#define SFP_ECUDA (-2)    /* CUDA runtime error                            */
+#define SFP_ENVRTC (-3)   /* NVRTC compilation failed (log returned)       */
+#define SFP_ENOMEM (-4)   /* device allocation failed                      */
+#define SFP_EDEVICE (-5)  /* device-side error word set (see sfp_run_state) */
+#define SFP_ENOKERNEL (-6) /* kernel not found in a module                  */
+
+/* ---- library ------------------------------------------------------------- */
+const char *sfp_version(void);
+const char *sfp_last_error(void);
+int sfp_device_count(int *count);
+/* free a buffer returned by this library (NVRTC image / log) */
+void sfp_free(void *p);
+
+/* ---- field programs (NVRTC) ------------------------------------------------
+ * Replaces Fields.__init__'s jitting of a user/preset callable
+ * (fields.py:26-50): `src` is CUDA C++ defining sfp_field_program() followed
+ * by the step source.  Compiles for sm_100a to a cubin image; needs no GPU. */
+int sfp_nvrtc_compile(const char *src, const char *name, const char *const *opts, int n_opts, void **image,
+                      size_t *image_size, char **log);
+typedef struct sfp_module sfp_module;
+int sfp_module_load(const void *image, size_t image_size, sfp_module **out);
+int sfp_module_unload(sfp_module *m);
+
+/* Fields.field_func[bpg, tpb](x, y, z, t, N, to_be_pruned, Ex..Bz)
+ * (fields.py:31-35 / 41-46, particles.py:310-323).  params: the program's
+ * term parameters (device). */
+int sfp_field_eval(sfp_module *m, const double *params, const double *x, const double *y, const double *z, double t,
+                   int64_t N, const uint8_t *to_be_pruned, double *Ex, double *Ey, double *Ez, double *Bx, double *By,
+                   double *Bz, void *stream);
+
+/* ---- per-op kernels: the reference's plugin boundary ----------------------- */
+/* push_position, cpu.py:5-19 */
+int sfp_push_position(double *x, double *y, double *z, const double *ux, const double *uy, const double *uz,
+                      const double *inv_gamma, int64_t N, const uint8_t *to_be_pruned, double dt, void *stream);
+/* boris, cpu.py:22-31 (inline.py:4-36) */
+int sfp_boris(double *ux, double *uy, double *uz, double *inv_gamma, const double *Ex, const double *Ey,
+              const double *Ez, const double *Bx, const double *By, const double *Bz, double q, int64_t N,
+              const uint8_t *to_be_pruned, double dt, void *stream);
+/* boris_tbmt, cpu.py:33-42 (inline.py:39-100) */
+int sfp_boris_tbmt(double *ux, double *uy, double *uz, double *inv_gamma, double *sx, double *sy, double *sz,
+                   const double *Ex, const double *Ey, const double *Ez, const double *Bx, const double *By,
+                   const double *Bz, double q, double ae, int64_t N, const uint8_t *to_be_pruned, double dt,
+                   void *stream);
+/* LL_push / CLL_push, cpu.py:44-60 (inline.py:104-123) */
+int sfp_LL_push(double *ux, double *uy, double *uz, double *inv_gamma, const double *chi, int64_t N,
+                const uint8_t *to_be_pruned, double dt, void *stream);
+int sfp_CLL_push(double *ux, double *uy, double *uz, double *inv_gamma, const double *chi, int64_t N,
+                 const uint8_t *to_be_pruned, double dt, void *stream);
+/* update_chi, cpu.py:62-74 (inline.py:126-134) */
+int sfp_update_chi(const double *Ex, const double *Ey, const double *Ez, const double *Bx, const double *By,
+                   const double *Bz, const double *ux, const double *uy, const double *uz, const double *inv_gamma,
+                   double *chi, int64_t N, const uint8_t *to_be_pruned, void *stream);
+/* photon_recoil, cpu.py:76-87 */
+int sfp_photon_recoil(double *ux, double *uy, double *uz, double *inv_gamma, const uint8_t *event,
+                      const double *photon_delta, int64_t N, const uint8_t *to_be_pruned, void *stream);
+/* pick_hard_photon, cpu.py:226-231 */
+int sfp_pick_hard_photon(uint8_t *event, const double *delta, const double *inv_gamma, double threshold, int64_t N,
+                         void *stream);
+/* bool_sum, cpu.py:217-224: count written to *count (device int64) */
+int sfp_bool_sum(const uint8_t *event, int64_t N, int64_t *count, void *stream);
+/* find_event_index, cpu.py:192-215: ascending indices of the N_event set
+ * entries of event[0:N], into index (device int64[N_event]).  workspace:
+ * caller-provided device scratch of sfp_find_event_index_workspace(N) bytes. */
+size_t sfp_find_event_index_workspace(int64_t N);
+int sfp_find_event_index(const uint8_t *event, int64_t N_event, int64_t N, int64_t *index, void *workspace,
+                         size_t workspace_bytes, void *stream);
+/* create_photon, cpu.py:89-116 */
+int sfp_create_photon(const double *x_src, const double *y_src, const double *z_src, const double *ux_src,
+                      const double *uy_src, const double *uz_src, double *x_dst, double *y_dst, double *z_dst,
+                      double *ux_dst, double *uy_dst, double *uz_dst, double *inv_gamma_dst,
+                      uint8_t *photon_to_be_pruned, const int64_t *event_index, const double *photon_delta,
+                      int64_t N_buffered, int64_t N_photon, void *stream);
+/* create_pair, cpu.py:119-189 */
+int sfp_create_pair(const double *x_src, const double *y_src, const double *z_src, const double *ux_src,
+                    const double *uy_src, const double *uz_src, uint8_t *photon_to_be_pruned, double *x_dst,
+                    double *y_dst, double *z_dst, double *ux_dst, double *uy_dst, double *uz_dst,
+                    double *inv_gamma_dst, uint8_t *pair_to_be_pruned, const int64_t *event_index,
+                    const double *pair_delta, int64_t N_buffered, int64_t N_pair, int inverse_delta, void *stream);
+/* photon_from_rejection_sampling / pair_from_rejection_sampling,
+ * qed/rejection_sampling.py:73-107.  The reference draws from Numba's
+ * per-thread generator; here draws are Philox-4x32-10 keyed by
+ * (seed, rng_stream, step, slot). */
+int sfp_photon_from_rejection_sampling(const double *inv_gamma, const double *chi_e, double dt, int64_t N,
+                                       const uint8_t *to_be_pruned, uint8_t *event, double *delta,
+                                       const sfp_rs_table *table, uint64_t seed, uint32_t rng_stream, uint32_t step,
+                                       void *stream);
+int sfp_pair_from_rejection_sampling(const double *inv_gamma, const double *chi_gamma, double dt, int64_t N,
+                                     const uint8_t *to_be_pruned, uint8_t *event, double *delta,
+                                     const sfp_rs_table *table, uint64_t seed, uint32_t rng_stream, uint32_t step,
+                                     void *stream);
+/* update_tau_e / update_tau_gamma, qed/optical_depth.py:15-111 */
+int sfp_update_tau(double *tau, const double *inv_gamma, const double *chi, double dt, int64_t N,
+                   const uint8_t *to_be_pruned, uint8_t *event, double *delta, const sfp_od_table *table,
+                   uint64_t seed, uint32_t rng_stream, uint32_t step, void *stream);
+/* inv_gamma from u for a whole buffer (particles.py:119 / 122), used to
+ * refresh the stored 1/gamma after fused steps, which keep only x and u. */
+int sfp_inv_gamma(const double *ux, const double *uy, const double *uz, double *inv_gamma, int64_t N, int massless,
+                  void *stream);
+
+/* ---- fused step: Simulation.start (simulation.py:74-160) -------------------
+ * A run owns the device bookkeeping of one or more instances whose species
+ * buffers are described by segments (device pointers owned by the caller). */
+typedef struct sfp_run sfp_run;
+typedef struct sfp_run_config {
+    double dt;
+    double photon_threshold; /* Simulation(photon_threshold=...), units of m_e c^2 */
+    double t0;
+    int64_t step0;           /* steps already taken (Philox step key)     */
+    int32_t qed;             /* SFP_QED_*                                  */
+    int32_t form;            /* SFP_FORM_*                                 */
+    sfp_rs_table rs;
+    sfp_od_table od_photon;
+    sfp_od_table od_pair;
+} sfp_run_config;
+
+int sfp_run_create(sfp_module *m, const sfp_run_config *cfg, int n_inst, const sfp_instance *inst, int n_seg,
+                   const sfp_segment *seg, const int64_t *n_buffered, sfp_run **out);
+/* after buffers were regrown / moved: new segment table and counts */
+int sfp_run_update(sfp_run *r, int n_seg, const sfp_segment *seg, const int64_t *n_buffered);
+/* advance up to nsteps steps (stops early, halted=1, when a destination
+ * lacks the worst-case headroom); graph_chunk > 0 replays CUDA graphs of
+ * that many steps.  Asynchronous on `stream`. */
+int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
+/* like sfp_run_steps without graphs, with CUDA events recorded around every
+ * step-kernel launch on the run's stream; synchronous.  kernel_ms[i] is the
+ * duration of launch i (n_steps entries). */
+int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stream);
+/* synchronous: state and per-segment buffered counts (n_seg entries) */
+int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);
+/* clear the halted flag after the caller made room */
+int sfp_run_clear_halt(sfp_run *r, void *stream);
+int sfp_run_destroy(sfp_run *r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,952 @@
+// sfp_capi.cu -- libsfp.so: the C-ABI of the B200 sfparticles step.
+//
+//   * per-op kernels that replace the reference's Numba kernels one for one
+//     (the plugin boundary, sfparticles/particles.py:14-25);
+//   * NVRTC compilation / loading of field-specialised step modules;
+//   * fused-step runs: device bookkeeping, persistent launches, CUDA graphs.
+//
+// Device memory of particle buffers belongs to the caller; a run allocates
+// only its own bookkeeping (segment tables, tile look-back flags, counters).
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sfp.h"
+#include "sfp_device.cuh"
+#include "sfp_run.cuh"
+
+#define SFP_VERSION_STRING "sfparticles_b200 0.1.0 (sm_100a)"
+// particles per tile of the fused step; the NVRTC modules are built with SFP_TILE equal to it
+#define SFP_TILE_HOST 256
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define SFP_CUDA(call)                                                                           \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(SFP_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define SFP_CHECK_LAUNCH() SFP_CUDA(cudaGetLastError())
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cached[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
+constexpr int kBlock = 256;
+
+inline unsigned int grid_for(long long n) {
+    if (n <= 0) return 1;
+    long long b = (n + kBlock - 1) / kBlock;
+    long long cap = (long long)sm_count() * 16;
+    return (unsigned int)(b < cap ? b : cap);
+}
+
+#define GRID_STRIDE(i, n) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// ------------------------------- per-op kernels ------------------------------
+
+__global__ void k_push_position(double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                                const double* __restrict__ ux, const double* __restrict__ uy,
+                                const double* __restrict__ uz, const double* __restrict__ ig, long long N,
+                                const unsigned char* __restrict__ pr, double dt) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) continue;
+        double a = x[i], b = y[i], c = z[i];
+        sfp::push_position(a, b, c, ux[i], uy[i], uz[i], ig[i], dt);
+        x[i] = a; y[i] = b; z[i] = c;
+    }
+}
+
+__global__ void k_boris(double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
+                        double* __restrict__ ig, const double* __restrict__ Ex, const double* __restrict__ Ey,
+                        const double* __restrict__ Ez, const double* __restrict__ Bx, const double* __restrict__ By,
+                        const double* __restrict__ Bz, double q, long long N, const unsigned char* __restrict__ pr,
+                        double dt) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) continue;
+        const double F[6] = {Ex[i], Ey[i], Ez[i], Bx[i], By[i], Bz[i]};
+        double a = ux[i], b = uy[i], c = uz[i];
+        ig[i] = sfp::boris(a, b, c, F, q, dt);
+        ux[i] = a; uy[i] = b; uz[i] = c;
+    }
+}
+
+__global__ void k_boris_tbmt(double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
+                             double* __restrict__ ig, double* __restrict__ sx, double* __restrict__ sy,
+                             double* __restrict__ sz, const double* __restrict__ Ex, const double* __restrict__ Ey,
+                             const double* __restrict__ Ez, const double* __restrict__ Bx,
+                             const double* __restrict__ By, const double* __restrict__ Bz, double q, double ae,
+                             long long N, const unsigned char* __restrict__ pr, double dt) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) continue;
+        const double F[6] = {Ex[i], Ey[i], Ez[i], Bx[i], By[i], Bz[i]};
+        double a = ux[i], b = uy[i], c = uz[i], s1 = sx[i], s2 = sy[i], s3 = sz[i];
+        ig[i] = sfp::boris_tbmt(a, b, c, s1, s2, s3, F, q, ae, dt);
+        ux[i] = a; uy[i] = b; uz[i] = c;
+        sx[i] = s1; sy[i] = s2; sz[i] = s3;
+    }
+}
+
+__global__ void k_ll(double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
+                     double* __restrict__ ig, const double* __restrict__ chi, long long N,
+                     const unsigned char* __restrict__ pr, double dt, int quantum) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) continue;
+        double a = ux[i], b = uy[i], c = uz[i];
+        ig[i] = sfp::ll_push(a, b, c, ig[i], chi[i], dt, quantum != 0);
+        ux[i] = a; uy[i] = b; uz[i] = c;
+    }
+}
+
+__global__ void k_update_chi(const double* __restrict__ Ex, const double* __restrict__ Ey,
+                             const double* __restrict__ Ez, const double* __restrict__ Bx,
+                             const double* __restrict__ By, const double* __restrict__ Bz,
+                             const double* __restrict__ ux, const double* __restrict__ uy,
+                             const double* __restrict__ uz, const double* __restrict__ ig, double* __restrict__ chi,
+                             long long N, const unsigned char* __restrict__ pr) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) continue;
+        const double F[6] = {Ex[i], Ey[i], Ez[i], Bx[i], By[i], Bz[i]};
+        chi[i] = sfp::chi_of(F, ux[i], uy[i], uz[i], ig[i]);
+    }
+}
+
+__global__ void k_photon_recoil(double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
+                                double* __restrict__ ig, const unsigned char* __restrict__ ev,
+                                const double* __restrict__ delta, long long N, const unsigned char* __restrict__ pr) {
+    GRID_STRIDE(i, N) {
+        if (pr[i] || !ev[i]) continue;
+        const double f = 1.0 - delta[i];
+        const double a = ux[i] * f, b = uy[i] * f, c = uz[i] * f;
+        ux[i] = a; uy[i] = b; uz[i] = c;
+        ig[i] = sfp::inv_gamma_massive(a, b, c);
+    }
+}
+
+__global__ void k_pick_hard(unsigned char* __restrict__ ev, const double* __restrict__ delta,
+                            const double* __restrict__ ig, double thr, long long N) {
+    GRID_STRIDE(i, N) {
+        if (ev[i] && delta[i] / ig[i] < thr) ev[i] = 0;
+    }
+}
+
+__global__ void k_bool_sum(const unsigned char* __restrict__ ev, long long N, unsigned long long* __restrict__ out) {
+    unsigned long long n = 0;
+    GRID_STRIDE(i, N) n += ev[i] ? 1ull : 0ull;
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    __shared__ unsigned long long s[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        n = threadIdx.x < kBlock / 32 ? s[threadIdx.x] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+        if (threadIdx.x == 0 && n) atomicAdd(out, n);
+    }
+}
+
+// ordered compaction (find_event_index): 16 items per thread, 4096 per block
+constexpr int kItems = 16;
+constexpr long long kChunk = (long long)kBlock * kItems;
+
+__global__ void k_fei_count(const unsigned char* __restrict__ ev, long long N, long long* __restrict__ counts) {
+    const long long base = blockIdx.x * kChunk;
+    unsigned int n = 0;
+    for (int k = 0; k < kItems; ++k) {
+        const long long i = base + (long long)k * kBlock + threadIdx.x;
+        if (i < N && ev[i]) ++n;
+    }
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    __shared__ unsigned int s[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = 0;
+        for (int w = 0; w < kBlock / 32; ++w) t += s[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// single-block exclusive scan of n counts (in place)
+__global__ void k_fei_scan(long long* __restrict__ counts, long long n) {
+    __shared__ long long s_carry;
+    __shared__ long long s_w[32];
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (long long base = 0; base < n; base += blockDim.x) {
+        const long long i = base + threadIdx.x;
+        const long long v = i < n ? counts[i] : 0;
+        long long inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) s_w[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            long long w = lane < nw ? s_w[lane] : 0;
+            long long wi = w;
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long u = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += u;
+            }
+            if (lane < nw) s_w[lane] = wi - w;
+        }
+        __syncthreads();
+        const long long excl = s_carry + s_w[warp] + inc - v;
+        if (i < n) counts[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry = excl + v;
+        __syncthreads();
+    }
+}
+
+__global__ void k_fei_scatter(const unsigned char* __restrict__ ev, long long N, const long long* __restrict__ offs,
+                              long long* __restrict__ index, long long N_event) {
+    const long long base = blockIdx.x * kChunk;
+    // each thread owns kItems consecutive elements so the output stays ordered
+    const long long first = base + (long long)threadIdx.x * kItems;
+    unsigned int mask = 0;
+    for (int k = 0; k < kItems; ++k) {
+        const long long i = first + k;
+        if (i < N && ev[i]) mask |= 1u << k;
+    }
+    const unsigned int n = __popc(mask);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned int inc = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    __shared__ unsigned int s_w[kBlock / 32];
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned int w = lane < kBlock / 32 ? s_w[lane] : 0u;
+        unsigned int wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        if (lane < kBlock / 32) s_w[lane] = wi - w;
+    }
+    __syncthreads();
+    long long pos = offs[blockIdx.x] + s_w[warp] + (inc - n);
+    while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
+        if (pos < N_event) index[pos] = first + k;
+        ++pos;
+    }
+}
+
+__global__ void k_create_photon(const double* __restrict__ xs, const double* __restrict__ ys,
+                                const double* __restrict__ zs, const double* __restrict__ uxs,
+                                const double* __restrict__ uys, const double* __restrict__ uzs, double* __restrict__ xd,
+                                double* __restrict__ yd, double* __restrict__ zd, double* __restrict__ uxd,
+                                double* __restrict__ uyd, double* __restrict__ uzd, double* __restrict__ igd,
+                                unsigned char* __restrict__ prd, const long long* __restrict__ idx,
+                                const double* __restrict__ delta, long long Nb, long long Np) {
+    GRID_STRIDE(k, Np) {
+        const long long s = idx[k], d = Nb + k;
+        xd[d] = xs[s]; yd[d] = ys[s]; zd[d] = zs[s];
+        const double dl = delta[s];
+        const double a = dl * uxs[s], b = dl * uys[s], c = dl * uzs[s];
+        uxd[d] = a; uyd[d] = b; uzd[d] = c;
+        igd[d] = sfp::inv_gamma_photon(a, b, c);
+        prd[d] = 0;
+    }
+}
+
+__global__ void k_create_pair(const double* __restrict__ xs, const double* __restrict__ ys,
+                              const double* __restrict__ zs, const double* __restrict__ uxs,
+                              const double* __restrict__ uys, const double* __restrict__ uzs,
+                              unsigned char* __restrict__ prs, double* __restrict__ xd, double* __restrict__ yd,
+                              double* __restrict__ zd, double* __restrict__ uxd, double* __restrict__ uyd,
+                              double* __restrict__ uzd, double* __restrict__ igd, unsigned char* __restrict__ prd,
+                              const long long* __restrict__ idx, const double* __restrict__ delta, long long Nb,
+                              long long Np, int inverse) {
+    GRID_STRIDE(k, Np) {
+        const long long s = idx[k], d = Nb + k;
+        xd[d] = xs[s]; yd[d] = ys[s]; zd[d] = zs[s];
+        double dl = delta[s];
+        if (inverse) dl = 1.0 - dl;
+        const double a = dl * uxs[s], b = dl * uys[s], c = dl * uzs[s];
+        uxd[d] = a; uyd[d] = b; uzd[d] = c;
+        igd[d] = sfp::inv_gamma_massive(a, b, c);
+        prd[d] = 0;
+        prs[s] = 1;
+    }
+}
+
+__global__ void k_rs(const double* __restrict__ ig, const double* __restrict__ chi, double dt, long long N,
+                     const unsigned char* __restrict__ pr, unsigned char* __restrict__ ev, double* __restrict__ delta,
+                     sfp_rs_table tab, unsigned long long seed, unsigned int stream, unsigned int step, int pair) {
+    GRID_STRIDE(i, N) {
+        const double c = chi[i];
+        if (pr[i] || c == 0.0) {
+            ev[i] = 0;
+            continue;
+        }
+        double r1, r2, d;
+        sfp::uniform2(seed, stream, step, 0u, i, r1, r2);
+        const bool e = pair ? sfp::pair_event_rs(c, ig[i], dt, r1, r2, tab.int_Ai, tab.Aip, tab.z_N, tab.z_max, d)
+                            : sfp::photon_event_rs(c, ig[i], dt, r1, r2, tab.int_Ai, tab.Aip, tab.z_N, tab.z_max, d);
+        ev[i] = e ? 1 : 0;
+        delta[i] = d;
+    }
+}
+
+__global__ void k_update_tau(double* __restrict__ tau, const double* __restrict__ ig, const double* __restrict__ chi,
+                             double dt, long long N, const unsigned char* __restrict__ pr, unsigned char* __restrict__ ev,
+                             double* __restrict__ delta, sfp_od_table tab, unsigned long long seed,
+                             unsigned int stream, unsigned int step) {
+    GRID_STRIDE(i, N) {
+        if (pr[i]) {
+            ev[i] = 0;
+            delta[i] = 0.0;
+            continue;
+        }
+        double tv = tau[i], d = 0.0;
+        const bool e = sfp::od_event(chi[i], ig[i], dt, tv, tab, tab.rate_total, seed, stream, step, i, d);
+        tau[i] = tv;
+        ev[i] = e ? 1 : 0;
+        delta[i] = d;
+    }
+}
+
+__global__ void k_inv_gamma(const double* __restrict__ ux, const double* __restrict__ uy,
+                            const double* __restrict__ uz, double* __restrict__ ig, long long N, int massless) {
+    GRID_STRIDE(i, N) {
+        ig[i] = massless ? sfp::inv_gamma_photon(ux[i], uy[i], uz[i]) : sfp::inv_gamma_massive(ux[i], uy[i], uz[i]);
+    }
+}
+
+}  // namespace
+
+// ================================ C-ABI ======================================
+
+struct sfp_module {
+    cudaLibrary_t lib = nullptr;
+    std::mutex mu;
+    std::unordered_map<std::string, cudaKernel_t> kernels;
+};
+
+static int module_kernel(sfp_module* m, const char* name, cudaKernel_t* out) {
+    std::lock_guard<std::mutex> g(m->mu);
+    auto it = m->kernels.find(name);
+    if (it != m->kernels.end()) {
+        *out = it->second;
+        return SFP_OK;
+    }
+    cudaKernel_t k = nullptr;
+    cudaError_t e = cudaLibraryGetKernel(&k, m->lib, name);
+    if (e != cudaSuccess) return fail(SFP_ENOKERNEL, std::string("kernel not in module: ") + name + " (" + cudaGetErrorString(e) + ")");
+    m->kernels[name] = k;
+    *out = k;
+    return SFP_OK;
+}
+
+extern "C" {
+
+const char* sfp_version(void) { return SFP_VERSION_STRING; }
+const char* sfp_last_error(void) { return g_err.c_str(); }
+void sfp_free(void* p) { std::free(p); }
+
+int sfp_device_count(int* count) {
+    if (!count) return fail(SFP_EINVAL, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(SFP_ECUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    *count = n;
+    return SFP_OK;
+}
+
+int sfp_nvrtc_compile(const char* src, const char* name, const char* const* opts, int n_opts, void** image,
+                      size_t* image_size, char** log) {
+    if (!src || !image || !image_size) return fail(SFP_EINVAL, "sfp_nvrtc_compile: NULL argument");
+    *image = nullptr;
+    *image_size = 0;
+    if (log) *log = nullptr;
+    nvrtcProgram prog;
+    nvrtcResult r = nvrtcCreateProgram(&prog, src, name ? name : "sfp_module.cu", 0, nullptr, nullptr);
+    if (r != NVRTC_SUCCESS) return fail(SFP_ENVRTC, std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
+    r = nvrtcCompileProgram(prog, n_opts, opts);
+    size_t ls = 0;
+    nvrtcGetProgramLogSize(prog, &ls);
+    std::string lg(ls, '\0');
+    if (ls) nvrtcGetProgramLog(prog, &lg[0]);
+    if (log && ls) {
+        *log = static_cast<char*>(std::malloc(ls + 1));
+        std::memcpy(*log, lg.data(), ls);
+        (*log)[ls] = 0;
+    }
+    if (r != NVRTC_SUCCESS) {
+        nvrtcDestroyProgram(&prog);
+        return fail(SFP_ENVRTC, std::string("nvrtcCompileProgram: ") + nvrtcGetErrorString(r) + "\n" + lg);
+    }
+    size_t n = 0;
+    r = nvrtcGetCUBINSize(prog, &n);
+    if (r != NVRTC_SUCCESS || n == 0) {
+        nvrtcDestroyProgram(&prog);
+        return fail(SFP_ENVRTC, "nvrtcGetCUBINSize failed (compile with -arch=sm_100a)");
+    }
+    void* buf = std::malloc(n);
+    r = nvrtcGetCUBIN(prog, static_cast<char*>(buf));
+    nvrtcDestroyProgram(&prog);
+    if (r != NVRTC_SUCCESS) {
+        std::free(buf);
+        return fail(SFP_ENVRTC, std::string("nvrtcGetCUBIN: ") + nvrtcGetErrorString(r));
+    }
+    *image = buf;
+    *image_size = n;
+    return SFP_OK;
+}
+
+int sfp_module_load(const void* image, size_t image_size, sfp_module** out) {
+    if (!image || !out) return fail(SFP_EINVAL, "sfp_module_load: NULL argument");
+    (void)image_size;
+    auto* m = new sfp_module();
+    cudaError_t e = cudaLibraryLoadData(&m->lib, image, nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e != cudaSuccess) {
+        delete m;
+        return fail(SFP_ECUDA, std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e));
+    }
+    *out = m;
+    return SFP_OK;
+}
+
+int sfp_module_unload(sfp_module* m) {
+    if (!m) return SFP_OK;
+    cudaError_t e = cudaLibraryUnload(m->lib);
+    delete m;
+    if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("cudaLibraryUnload: ") + cudaGetErrorString(e));
+    return SFP_OK;
+}
+
+int sfp_field_eval(sfp_module* m, const double* params, const double* x, const double* y, const double* z, double t,
+                   int64_t N, const uint8_t* pr, double* Ex, double* Ey, double* Ez, double* Bx, double* By,
+                   double* Bz, void* stream) {
+    if (!m) return fail(SFP_EINVAL, "sfp_field_eval: NULL module");
+    if (N <= 0) return SFP_OK;
+    cudaKernel_t k;
+    int rc = module_kernel(m, "sfp_field_eval_kernel", &k);
+    if (rc) return rc;
+    long long n = N;
+    void* args[] = {&params, &x, &y, &z, &t, &n, &pr, &Ex, &Ey, &Ez, &Bx, &By, &Bz};
+    SFP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid_for(N)), dim3(kBlock), args, 0, as_stream(stream)));
+    return SFP_OK;
+}
+
+#define RETURN_IF_EMPTY(n) \
+    if ((n) <= 0) return SFP_OK
+
+int sfp_push_position(double* x, double* y, double* z, const double* ux, const double* uy, const double* uz,
+                      const double* ig, int64_t N, const uint8_t* pr, double dt, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_push_position<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(x, y, z, ux, uy, uz, ig, N, pr, dt);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_boris(double* ux, double* uy, double* uz, double* ig, const double* Ex, const double* Ey, const double* Ez,
+              const double* Bx, const double* By, const double* Bz, double q, int64_t N, const uint8_t* pr, double dt,
+              void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_boris<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, Ex, Ey, Ez, Bx, By, Bz, q, N, pr, dt);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_boris_tbmt(double* ux, double* uy, double* uz, double* ig, double* sx, double* sy, double* sz,
+                   const double* Ex, const double* Ey, const double* Ez, const double* Bx, const double* By,
+                   const double* Bz, double q, double ae, int64_t N, const uint8_t* pr, double dt, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_boris_tbmt<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, sx, sy, sz, Ex, Ey, Ez, Bx, By, Bz, q,
+                                                                 ae, N, pr, dt);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_LL_push(double* ux, double* uy, double* uz, double* ig, const double* chi, int64_t N, const uint8_t* pr,
+                double dt, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_ll<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, chi, N, pr, dt, 0);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_CLL_push(double* ux, double* uy, double* uz, double* ig, const double* chi, int64_t N, const uint8_t* pr,
+                 double dt, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_ll<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, chi, N, pr, dt, 1);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_update_chi(const double* Ex, const double* Ey, const double* Ez, const double* Bx, const double* By,
+                   const double* Bz, const double* ux, const double* uy, const double* uz, const double* ig,
+                   double* chi, int64_t N, const uint8_t* pr, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_update_chi<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(Ex, Ey, Ez, Bx, By, Bz, ux, uy, uz, ig, chi, N, pr);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_photon_recoil(double* ux, double* uy, double* uz, double* ig, const uint8_t* ev, const double* delta,
+                      int64_t N, const uint8_t* pr, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_photon_recoil<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, ev, delta, N, pr);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_pick_hard_photon(uint8_t* ev, const double* delta, const double* ig, double thr, int64_t N, void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_pick_hard<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ev, delta, ig, thr, N);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_bool_sum(const uint8_t* ev, int64_t N, int64_t* count, void* stream) {
+    if (!count) return fail(SFP_EINVAL, "sfp_bool_sum: count is NULL");
+    SFP_CUDA(cudaMemsetAsync(count, 0, sizeof(int64_t), as_stream(stream)));
+    RETURN_IF_EMPTY(N);
+    k_bool_sum<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ev, N, reinterpret_cast<unsigned long long*>(count));
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+size_t sfp_find_event_index_workspace(int64_t N) {
+    const long long nb = N <= 0 ? 1 : (N + kChunk - 1) / kChunk;
+    return (size_t)nb * sizeof(long long);
+}
+
+int sfp_find_event_index(const uint8_t* ev, int64_t N_event, int64_t N, int64_t* index, void* ws, size_t ws_bytes,
+                         void* stream) {
+    if (N <= 0 || N_event <= 0) return SFP_OK;
+    const long long nb = (N + kChunk - 1) / kChunk;
+    if (!ws || ws_bytes < (size_t)nb * sizeof(long long))
+        return fail(SFP_EINVAL, "sfp_find_event_index: workspace too small");
+    long long* counts = static_cast<long long*>(ws);
+    cudaStream_t s = as_stream(stream);
+    k_fei_count<<<(unsigned int)nb, kBlock, 0, s>>>(ev, N, counts);
+    SFP_CHECK_LAUNCH();
+    k_fei_scan<<<1, 1024, 0, s>>>(counts, nb);
+    SFP_CHECK_LAUNCH();
+    k_fei_scatter<<<(unsigned int)nb, kBlock, 0, s>>>(ev, N, counts, reinterpret_cast<long long*>(index), N_event);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_create_photon(const double* xs, const double* ys, const double* zs, const double* uxs, const double* uys,
+                      const double* uzs, double* xd, double* yd, double* zd, double* uxd, double* uyd, double* uzd,
+                      double* igd, uint8_t* prd, const int64_t* idx, const double* delta, int64_t Nb, int64_t Np,
+                      void* stream) {
+    RETURN_IF_EMPTY(Np);
+    k_create_photon<<<grid_for(Np), kBlock, 0, as_stream(stream)>>>(xs, ys, zs, uxs, uys, uzs, xd, yd, zd, uxd, uyd,
+                                                                     uzd, igd, prd,
+                                                                     reinterpret_cast<const long long*>(idx), delta,
+                                                                     Nb, Np);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_create_pair(const double* xs, const double* ys, const double* zs, const double* uxs, const double* uys,
+                    const double* uzs, uint8_t* prs, double* xd, double* yd, double* zd, double* uxd, double* uyd,
+                    double* uzd, double* igd, uint8_t* prd, const int64_t* idx, const double* delta, int64_t Nb,
+                    int64_t Np, int inverse, void* stream) {
+    RETURN_IF_EMPTY(Np);
+    k_create_pair<<<grid_for(Np), kBlock, 0, as_stream(stream)>>>(xs, ys, zs, uxs, uys, uzs, prs, xd, yd, zd, uxd, uyd,
+                                                                   uzd, igd, prd,
+                                                                   reinterpret_cast<const long long*>(idx), delta, Nb,
+                                                                   Np, inverse);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_photon_from_rejection_sampling(const double* ig, const double* chi, double dt, int64_t N, const uint8_t* pr,
+                                       uint8_t* ev, double* delta, const sfp_rs_table* tab, uint64_t seed,
+                                       uint32_t rng_stream, uint32_t step, void* stream) {
+    if (!tab) return fail(SFP_EINVAL, "rate table is NULL");
+    RETURN_IF_EMPTY(N);
+    k_rs<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ig, chi, dt, N, pr, ev, delta, *tab, seed, rng_stream, step, 0);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_pair_from_rejection_sampling(const double* ig, const double* chi, double dt, int64_t N, const uint8_t* pr,
+                                     uint8_t* ev, double* delta, const sfp_rs_table* tab, uint64_t seed,
+                                     uint32_t rng_stream, uint32_t step, void* stream) {
+    if (!tab) return fail(SFP_EINVAL, "rate table is NULL");
+    RETURN_IF_EMPTY(N);
+    k_rs<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ig, chi, dt, N, pr, ev, delta, *tab, seed, rng_stream, step, 1);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_update_tau(double* tau, const double* ig, const double* chi, double dt, int64_t N, const uint8_t* pr,
+                   uint8_t* ev, double* delta, const sfp_od_table* tab, uint64_t seed, uint32_t rng_stream,
+                   uint32_t step, void* stream) {
+    if (!tab) return fail(SFP_EINVAL, "optical-depth table is NULL");
+    RETURN_IF_EMPTY(N);
+    k_update_tau<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(tau, ig, chi, dt, N, pr, ev, delta, *tab, seed,
+                                                                 rng_stream, step);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+int sfp_inv_gamma(const double* ux, const double* uy, const double* uz, double* ig, int64_t N, int massless,
+                  void* stream) {
+    RETURN_IF_EMPTY(N);
+    k_inv_gamma<<<grid_for(N), kBlock, 0, as_stream(stream)>>>(ux, uy, uz, ig, N, massless);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+}  // extern "C"
+
+// ================================ runs =======================================
+
+struct sfp_run {
+    sfp_module* mod = nullptr;
+    cudaKernel_t k_step = nullptr, k_book = nullptr;
+    int grid = 0;
+    size_t smem = 0;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    int n_seg = 0, n_inst = 0;
+    sfp_run_dev h{};
+    sfp_run_dev* d = nullptr;
+    std::map<int, cudaGraphExec_t> graphs;
+    std::vector<sfp_segment> segs;
+};
+
+static long long tiles_for(const std::vector<sfp_segment>& segs, int tile) {
+    long long t = 0;
+    for (auto& s : segs) t += (s.capacity + tile - 1) / tile;
+    return t + (long long)segs.size() + 1;
+}
+
+static int run_alloc_tiles(sfp_run* r, long long need) {
+    if (need <= r->h.max_tiles) return SFP_OK;
+    long long n = need + need / 4 + 64;
+    if (r->h.tile_flag) cudaFree(r->h.tile_flag);
+    if (r->h.tile_agg) cudaFree(r->h.tile_agg);
+    if (r->h.tile_incl) cudaFree(r->h.tile_incl);
+    r->h.tile_flag = nullptr;
+    r->h.tile_agg = r->h.tile_incl = nullptr;
+    SFP_CUDA(cudaMalloc(&r->h.tile_flag, n * sizeof(unsigned int)));
+    SFP_CUDA(cudaMalloc(&r->h.tile_agg, n * sizeof(uint4)));
+    SFP_CUDA(cudaMalloc(&r->h.tile_incl, n * sizeof(uint4)));
+    SFP_CUDA(cudaMemsetAsync(r->h.tile_flag, 0, n * sizeof(unsigned int), r->s));
+    r->h.max_tiles = n;
+    return SFP_OK;
+}
+
+static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, const sfp_segment* seg) {
+    if (n_seg <= 0 || n_seg > SFP_MAX_SEGMENTS) return fail(SFP_EINVAL, "segment count out of range");
+    if (n_inst <= 0) return fail(SFP_EINVAL, "instance count must be positive");
+    int expect = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        if (inst[i].first_seg != expect || inst[i].n_seg <= 0)
+            return fail(SFP_EINVAL, "instances must cover the segments contiguously in order");
+        expect += inst[i].n_seg;
+    }
+    if (expect != n_seg) return fail(SFP_EINVAL, "instances do not cover all segments");
+    for (int s = 0; s < n_seg; ++s) {
+        const sfp_segment& S = seg[s];
+        if (S.capacity < 0) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": negative capacity");
+        // an empty buffer (capacity 0) may have NULL arrays: nothing reads or writes it
+        if (S.capacity > 0 && (!S.x || !S.y || !S.z || !S.ux || !S.uy || !S.uz || !S.pruned))
+            return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": NULL state pointer");
+        if (S.capacity > 0 && S.spin && (!S.sx || !S.sy || !S.sz))
+            return fail(SFP_EINVAL, "spin segment without spin arrays");
+        if (S.channel < 0 || S.channel >= SFP_MAX_CHANNELS) return fail(SFP_EINVAL, "append channel out of range");
+        const sfp_instance& I = inst[S.instance];
+        auto in_inst = [&](int d) { return d >= I.first_seg && d < I.first_seg + I.n_seg; };
+        if (S.radiating && (!in_inst(S.photon_dest) || !seg[S.photon_dest].massless))
+            return fail(SFP_EINVAL, "radiating segment needs a photon destination in its instance");
+        if (S.bw && (!in_inst(S.ele_dest) || !in_inst(S.pos_dest) || seg[S.ele_dest].massless ||
+                     seg[S.pos_dest].massless))
+            return fail(SFP_EINVAL, "pair-creating segment needs massive destinations in its instance");
+    }
+    return SFP_OK;
+}
+
+static int run_upload(sfp_run* r, const sfp_instance* inst, const int64_t* n_buffered) {
+    if (inst) SFP_CUDA(cudaMemcpyAsync((void*)r->h.inst, inst, r->n_inst * sizeof(sfp_instance), cudaMemcpyHostToDevice, r->s));
+    SFP_CUDA(cudaMemcpyAsync((void*)r->h.seg, r->segs.data(), r->n_seg * sizeof(sfp_segment), cudaMemcpyHostToDevice, r->s));
+    if (n_buffered)
+        SFP_CUDA(cudaMemcpyAsync(r->h.n_buffered, n_buffered, r->n_seg * sizeof(long long), cudaMemcpyHostToDevice, r->s));
+    SFP_CUDA(cudaMemcpyAsync(r->d, &r->h, sizeof(sfp_run_dev), cudaMemcpyHostToDevice, r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    return SFP_OK;
+}
+
+extern "C" {
+
+int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const sfp_instance* inst, int n_seg,
+                   const sfp_segment* seg, const int64_t* n_buffered, sfp_run** out) {
+    if (!cfg || !inst || !seg || !n_buffered || !out) return fail(SFP_EINVAL, "sfp_run_create: NULL argument");
+    int rc = validate_segments(n_inst, inst, n_seg, seg);
+    if (rc) return rc;
+    if (!m) return fail(SFP_EINVAL, "sfp_run_create: NULL module");
+    if (cfg->qed != SFP_QED_REJECTION && cfg->qed != SFP_QED_OPTICAL_DEPTH) return fail(SFP_EINVAL, "unknown QED method");
+    if (cfg->form != SFP_FORM_FP64 && cfg->form != SFP_FORM_FP32) return fail(SFP_EINVAL, "unknown arithmetic form");
+    auto* r = new sfp_run();
+    r->mod = m;
+    r->n_seg = n_seg;
+    r->n_inst = n_inst;
+    r->segs.assign(seg, seg + n_seg);
+    const char* kname = nullptr;
+    if (cfg->form == SFP_FORM_FP64)
+        kname = cfg->qed == SFP_QED_REJECTION ? "sfp_step_fp64_rs" : "sfp_step_fp64_od";
+    else
+        kname = cfg->qed == SFP_QED_REJECTION ? "sfp_step_fp32_rs" : "sfp_step_fp32_od";
+    if ((rc = module_kernel(m, kname, &r->k_step)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
+        delete r;
+        return rc;
+    }
+    auto cleanup = [&](int code) {
+        sfp_run_destroy(r);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&r->s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming) != cudaSuccess)
+        return cleanup(fail(SFP_ECUDA, "stream/event creation failed"));
+    sfp_run_dev& h = r->h;
+    h.n_seg = n_seg;
+    h.n_inst = n_inst;
+    h.dt = cfg->dt;
+    h.photon_threshold = cfg->photon_threshold;
+    h.qed = cfg->qed;
+    h.tile = SFP_TILE_HOST;
+    h.any_appends = 0;
+    for (int s = 0; s < n_seg; ++s) h.any_appends |= (seg[s].radiating || seg[s].bw) ? 1 : 0;
+    h.rs = cfg->rs;
+    h.od_photon = cfg->od_photon;
+    h.od_pair = cfg->od_pair;
+#define ALLOC(ptr, bytes) \
+    if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) return cleanup(fail(SFP_ENOMEM, "cudaMalloc " #ptr))
+    sfp_segment* dseg;
+    sfp_instance* dinst;
+    ALLOC(dseg, n_seg * sizeof(sfp_segment));
+    ALLOC(dinst, n_inst * sizeof(sfp_instance));
+    h.seg = dseg;
+    h.inst = dinst;
+    ALLOC(h.n_buffered, n_seg * sizeof(long long));
+    ALLOC(h.appended, n_seg * sizeof(unsigned long long));
+    ALLOC(h.n_buf_step, n_seg * sizeof(long long));
+    ALLOC(h.tile_start, (n_seg + 1) * sizeof(long long));
+    ALLOC(h.st, sizeof(sfp_step_state));
+    ALLOC(r->d, sizeof(sfp_run_dev));
+#undef ALLOC
+    if (cudaMemsetAsync(h.appended, 0, n_seg * sizeof(unsigned long long), r->s) != cudaSuccess)
+        return cleanup(fail(SFP_ECUDA, "memset"));
+    sfp_step_state st0{};
+    st0.t = cfg->t0;
+    st0.step = cfg->step0;
+    st0.skip = 1;
+    if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
+        return cleanup(fail(SFP_ECUDA, "state upload"));
+    if ((rc = run_alloc_tiles(r, tiles_for(r->segs, SFP_TILE_HOST)))) return cleanup(rc);
+    if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
+    // shared memory for the tables, persistent grid size
+    if (cfg->qed == SFP_QED_REJECTION)
+        r->smem = 2 * (size_t)cfg->rs.z_N * sizeof(double);
+    else
+        r->smem = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
+    if (r->smem > 48 * 1024) {
+        if (cudaFuncSetAttribute((const void*)r->k_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem) !=
+            cudaSuccess)
+            return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory for the table"));
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)r->k_step, SFP_TILE_HOST, r->smem) !=
+            cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 2;
+    }
+    r->grid = sm_count() * per_sm;
+    *out = r;
+    return SFP_OK;
+}
+
+int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t* n_buffered) {
+    if (!r || !seg) return fail(SFP_EINVAL, "sfp_run_update: NULL argument");
+    if (n_seg != r->n_seg) return fail(SFP_EINVAL, "sfp_run_update: segment count changed");
+    r->segs.assign(seg, seg + n_seg);
+    int rc = run_alloc_tiles(r, tiles_for(r->segs, SFP_TILE_HOST));
+    if (rc) return rc;
+    return run_upload(r, nullptr, n_buffered);
+}
+
+static int launch_unit(sfp_run* r, cudaStream_t s) {
+    int prep = 1;
+    void* a_book[] = {&r->d, &prep};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, s));
+    void* a_step[] = {&r->d};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_step, dim3(r->grid), dim3(SFP_TILE_HOST), a_step, r->smem, s));
+    return SFP_OK;
+}
+
+int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
+    if (!r) return fail(SFP_EINVAL, "sfp_run_steps: NULL run");
+    if (nsteps <= 0) return SFP_OK;
+    cudaStream_t cs = as_stream(stream);
+    SFP_CUDA(cudaEventRecord(r->ev_in, cs));
+    SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    int64_t done = 0;
+    if (graph_chunk > 0 && nsteps >= graph_chunk) {
+        auto it = r->graphs.find(graph_chunk);
+        if (it == r->graphs.end()) {
+            cudaGraph_t g;
+            SFP_CUDA(cudaStreamBeginCapture(r->s, cudaStreamCaptureModeThreadLocal));
+            int rc = SFP_OK;
+            for (int k = 0; k < graph_chunk && rc == SFP_OK; ++k) rc = launch_unit(r, r->s);
+            cudaError_t e = cudaStreamEndCapture(r->s, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            cudaGraphExec_t ge;
+            e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            it = r->graphs.emplace(graph_chunk, ge).first;
+        }
+        for (; done + graph_chunk <= nsteps; done += graph_chunk) SFP_CUDA(cudaGraphLaunch(it->second, r->s));
+    }
+    for (; done < nsteps; ++done) {
+        int rc = launch_unit(r, r->s);
+        if (rc) return rc;
+    }
+    int prep = 0;
+    void* a_book[] = {&r->d, &prep};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s));
+    SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
+    SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
+    return SFP_OK;
+}
+
+int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stream) {
+    if (!r || !kernel_ms) return fail(SFP_EINVAL, "sfp_run_steps_timed: NULL argument");
+    if (nsteps <= 0) return SFP_OK;
+    cudaStream_t cs = as_stream(stream);
+    SFP_CUDA(cudaEventRecord(r->ev_in, cs));
+    SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    std::vector<cudaEvent_t> ev(2 * nsteps, nullptr);
+    int rc = SFP_OK;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = fail(SFP_ECUDA, "cudaEventCreate");
+    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) {
+        int prep = 1;
+        void* a_book[] = {&r->d, &prep};
+        void* a_step[] = {&r->d};
+        if (cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s) != cudaSuccess ||
+            cudaEventRecord(ev[2 * k], r->s) != cudaSuccess ||
+            cudaLaunchKernel((const void*)r->k_step, dim3(r->grid), dim3(SFP_TILE_HOST), a_step, r->smem, r->s) !=
+                cudaSuccess ||
+            cudaEventRecord(ev[2 * k + 1], r->s) != cudaSuccess)
+            rc = fail(SFP_ECUDA, std::string("timed launch: ") + cudaGetErrorString(cudaGetLastError()));
+    }
+    if (rc == SFP_OK) {
+        int prep = 0;
+        void* a_book[] = {&r->d, &prep};
+        if (cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s) != cudaSuccess)
+            rc = fail(SFP_ECUDA, "fold launch");
+    }
+    if (rc == SFP_OK && cudaStreamSynchronize(r->s) != cudaSuccess) rc = fail(SFP_ECUDA, "synchronize");
+    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k)
+        if (cudaEventElapsedTime(&kernel_ms[k], ev[2 * k], ev[2 * k + 1]) != cudaSuccess) rc = fail(SFP_ECUDA, "elapsed");
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc) return rc;
+    SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
+    SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
+    return SFP_OK;
+}
+
+int sfp_run_read_state(sfp_run* r, sfp_run_state* state, int64_t* n_buffered, void* stream) {
+    if (!r || !state) return fail(SFP_EINVAL, "sfp_run_read_state: NULL argument");
+    (void)stream;
+    sfp_step_state st;
+    SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
+    if (n_buffered)
+        SFP_CUDA(cudaMemcpyAsync(n_buffered, r->h.n_buffered, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    state->t = st.t;
+    state->step = st.step;
+    state->halted = st.halted;
+    state->error = st.error;
+    state->particle_steps = st.particle_steps;
+    return SFP_OK;
+}
+
+int sfp_run_clear_halt(sfp_run* r, void* stream) {
+    if (!r) return fail(SFP_EINVAL, "NULL run");
+    (void)stream;
+    sfp_step_state st;
+    SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    st.halted = 0;
+    st.skip = 1;
+    SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    return SFP_OK;
+}
+
+int sfp_run_destroy(sfp_run* r) {
+    if (!r) return SFP_OK;
+    if (r->s) cudaStreamSynchronize(r->s);
+    for (auto& kv : r->graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree((void*)r->h.seg);
+    cudaFree((void*)r->h.inst);
+    cudaFree(r->h.n_buffered);
+    cudaFree(r->h.appended);
+    cudaFree(r->h.n_buf_step);
+    cudaFree(r->h.tile_start);
+    cudaFree(r->h.tile_flag);
+    cudaFree(r->h.tile_agg);
+    cudaFree(r->h.tile_incl);
+    cudaFree(r->h.st);
+    cudaFree(r->d);
+    if (r->ev_in) cudaEventDestroy(r->ev_in);
+    if (r->ev_out) cudaEventDestroy(r->ev_out);
+    if (r->s) cudaStreamDestroy(r->s);
+    delete r;
+    return SFP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,315 @@
+"""Simulation: the reference's step loop (sfparticles/simulation.py) driving
+the fused B200 step.
+
+``Simulation(*particles, dt, fields, print_every=100, t0=0.0,
+photon_threshold=2.0)`` and ``start(nstep, total=None, call_back=None)``
+behave as in the reference: species are classified into pushed, pair-creating
+and radiating lists (simulation.py:62-71); every step evaluates fields at t,
+generates QED events, appends photons then pairs, and pushes every pushed
+particle (children included) from t to t+dt (simulation.py:102-144);
+``start`` ends by pruning and returning host arrays (simulation.py:158-161).
+
+Each step is ONE launch of the fused kernel over all species (plus a
+one-block bookkeeping launch); steps between progress reports / callbacks
+run back to back on the device, replayed from CUDA graphs, with no host
+synchronisation.  The kernel never overruns a buffer: a device-side guard
+skips the step when a destination lacks room for the worst case (every
+emitter emits), and the host then grows that buffer by the reference rule
+and continues.
+
+Extra keyword arguments (no reference counterpart):
+  seed        -- 64-bit key of the Philox streams (default: random);
+  form        -- 'fp64' (plain float64, the reference arithmetic) or 'fp32';
+  graph_chunk -- steps per captured CUDA graph (0 disables graphs).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from time import perf_counter_ns
+from typing import Callable
+
+import numpy as np
+
+from . import _lib, program, qed
+from .fields import Fields
+from .particles import Particles, RadiationReactionType, _RR_CODE, _device, _random_seed, _stream_ptr
+
+try:
+    from tqdm.autonotebook import tqdm
+except Exception:  # pragma: no cover
+    tqdm = None
+
+
+class Simulation(object):
+    def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
+                 photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64) -> None:
+        self.all_particles = all_particles
+        self.particles_push = []
+        self.particles_bw = []
+        self.particles_rad = []
+        self.dt = dt
+        self.fields = fields
+        self.print_every = print_every
+        self.photon_threshold = photon_threshold
+        self.t = t0
+        self.step = 0
+        self.progress_bar = None
+        self.seed = _random_seed() if seed is None else int(seed) & (2 ** 64 - 1)
+        if form not in ("fp64", "fp32"):
+            raise ValueError("form must be 'fp64' or 'fp32'")
+        self.form = form
+        self.graph_chunk = int(graph_chunk)
+        self.particle_steps = 0  # sum over executed steps of all species' N_buffered
+        self.kernel_launches = 0  # libsfp kernels launched by start()/run_on_device()
+        self._run = None
+
+        for p in all_particles:
+            if p.bw:
+                assert p.bw_electron_ref() in all_particles, f"{p.bw_electron_ref().name} not included in simulation."
+                assert p.bw_positron_ref() in all_particles, f"{p.bw_positron_ref().name} not included in simulation."
+                self.particles_bw.append(p)
+            if p.radiating:
+                assert p.photon_ref() in all_particles, f"{p.photon_ref().name} not included in simulation."
+                self.particles_rad.append(p)
+            if p.push:
+                self.particles_push.append(p)
+        ods = {p.uses_optical_depth for p in all_particles if p.radiating or p.bw}
+        if len(ods) > 1:
+            raise ValueError("all QED species of a simulation must use the same event method")
+        self.qed_method = "od" if ods == {True} else "rs"
+
+    # ------------------------------------------------------------------
+    def _index(self, p):
+        for i, q in enumerate(self.all_particles):
+            if q is p:
+                return i
+        raise ValueError(f"{p.name} not in simulation")
+
+    def _segments(self):
+        """sfp_segment table of the species (one instance)."""
+        segs = (_lib.Segment * len(self.all_particles))()
+        channels = {}
+
+        def channel(key):
+            if key not in channels:
+                if len(channels) >= 4:
+                    raise ValueError("at most 4 distinct append destinations are supported")
+                channels[key] = len(channels)
+            return channels[key]
+
+        for i, p in enumerate(self.all_particles):
+            s = segs[i]
+            for k in ("x", "y", "z", "ux", "uy", "uz"):
+                setattr(s, k, p._d(k).data_ptr())
+            s.pruned = p._d("_to_be_pruned").data_ptr()
+            spin = "sx" in p.attrs
+            if spin:
+                s.sx, s.sy, s.sz = (p._d(k).data_ptr() for k in ("sx", "sy", "sz"))
+            s.tau = p._d("tau").data_ptr() if "tau" in p.attrs else None
+            s.capacity = p.buffer_size
+            s.q = p.q
+            s.ae = getattr(p, "ae", 0.0) if spin else 0.0
+            s.massless = 1 if p.m == 0 else 0
+            s.push = 1 if p.push else 0
+            s.rr = _RR_CODE[p.RR]
+            s.spin = 1 if spin else 0
+            s.radiating = 1 if p.radiating else 0
+            s.bw = 1 if p.bw else 0
+            s.photon_dest = self._index(p.photon_ref()) if p.radiating else -1
+            s.ele_dest = self._index(p.bw_electron_ref()) if p.bw else -1
+            s.pos_dest = self._index(p.bw_positron_ref()) if p.bw else -1
+            s.channel = 0
+            if p.radiating:
+                s.channel = channel(("ph", s.photon_dest))
+            elif p.bw:
+                s.channel = channel(("pair", s.ele_dest, s.pos_dest))
+            s.instance = 0
+            s.stream = i
+        return segs
+
+    def _worst_case_need(self):
+        need = {id(p): 0 for p in self.all_particles}
+        for p in self.particles_rad:
+            need[id(p.photon_ref())] += p.N_buffered
+        for p in self.particles_bw:
+            need[id(p.bw_electron_ref())] += p.N_buffered
+            need[id(p.bw_positron_ref())] += p.N_buffered
+        return need
+
+    def _ensure_headroom(self) -> bool:
+        """Grow destinations that could overflow in one step; True if any grew."""
+        grew = False
+        need = self._worst_case_need()
+        for p in self.all_particles:
+            n = need[id(p)]
+            if n and p.buffer_size - p.N_buffered < n:
+                p._extend(n)
+                grew = True
+        return grew
+
+    def _run_config(self):
+        from .qed import device_tables
+        dev = _device()
+        cfg = _lib.RunConfig()
+        cfg.dt = self.dt
+        cfg.photon_threshold = self.photon_threshold
+        cfg.t0 = self.t
+        cfg.step0 = self.step
+        cfg.qed = _lib.SFP_QED_OPTICAL_DEPTH if self.qed_method == "od" else _lib.SFP_QED_REJECTION
+        cfg.form = _lib.SFP_FORM_FP32 if self.form == "fp32" else _lib.SFP_FORM_FP64
+        if self.qed_method == "od":
+            cfg.od_photon, cfg.od_pair = device_tables.od_tables(dev)
+        else:
+            cfg.rs = device_tables.rs_table(dev)
+        return cfg
+
+    # ------------------------------------------------------------------
+    def start(self, nstep: int, total: int = None, call_back: Callable[[int], None] = None):
+        """Run `nstep` steps (simulation.py:74-160)."""
+        if total is None:
+            total = nstep
+        if self.progress_bar is None and self.print_every and tqdm is not None:
+            self.progress_bar = tqdm(total=total, unit='step', smoothing=1)
+
+        self._begin()
+        try:
+            self._loop(self._run, nstep, call_back)
+        finally:
+            self._end()
+        for p in self.all_particles:
+            p._prune()
+            p._to_host()
+
+    # -- device-resident driving (start() = _begin + _loop + _end + prune) --
+    def _begin(self):
+        """Move species to the device and create the fused-step run."""
+        for p in self.all_particles:
+            p._to_gpu()
+        self._ensure_headroom()
+        mod = program.get_module(self.fields, form=self.form, qed=self.qed_method)
+        params = self.fields.params_device(_device())
+        inst = (_lib.Instance * 1)()
+        inst[0].seed = self.seed
+        inst[0].field_params = params.data_ptr()
+        inst[0].first_seg = 0
+        inst[0].n_seg = len(self.all_particles)
+        segs = self._segments()
+        nbuf = (ctypes.c_int64 * len(self.all_particles))(*[p.N_buffered for p in self.all_particles])
+        cfg = self._run_config()
+        # the step counter of the device restarts at self.step
+        run = ctypes.c_void_p()
+        _lib.call("sfp_run_create", mod.handle, ctypes.byref(cfg), 1, inst, len(self.all_particles), segs, nbuf,
+                  ctypes.byref(run))
+        self._run = run
+        self._keep = (mod, params)
+        self._ps_base = self.particle_steps  # the device counter restarts with the run
+
+    def _end(self):
+        run = getattr(self, "_run", None)
+        if run is not None:
+            _lib.load().sfp_run_destroy(run)
+        self._run = None
+        self._keep = None
+
+    def run_on_device(self, nstep: int):
+        """Advance `nstep` steps keeping every species on the device (no
+        prune, no host copies); call finish() to end like start()."""
+        if getattr(self, "_run", None) is None:
+            self._begin()
+        self._loop(self._run, nstep, None)
+
+    def finish(self):
+        """End a run_on_device() sequence: prune and return host arrays."""
+        self._end()
+        for p in self.all_particles:
+            p._prune()
+            p._to_host()
+
+    def time_step_kernel(self, nstep: int):
+        """Advance `nstep` steps with one eager launch each and return the
+        CUDA-event durations [ms] of the step-kernel launches (recorded on the
+        stream they run on), with the buffered counts before and after."""
+        if getattr(self, "_run", None) is None:
+            self._begin()
+        if self._ensure_headroom():
+            self._update_run(self._run)
+        need = self._worst_case_need()
+        for p in self.all_particles:  # room for nstep worst-case steps
+            if need[id(p)]:
+                p._extend(need[id(p)] * nstep)
+        self._update_run(self._run)
+        before = [p.N_buffered for p in self.all_particles]
+        ms = (ctypes.c_float * int(nstep))()
+        _lib.check(_lib.load().sfp_run_steps_timed(self._run, nstep, ms, _stream_ptr()), "sfp_run_steps_timed")
+        st = _lib.RunState()
+        nbuf = (ctypes.c_int64 * len(self.all_particles))()
+        _lib.check(_lib.load().sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
+        if st.error or st.halted:
+            raise _lib.SFPError("timed steps did not complete")
+        for i, p in enumerate(self.all_particles):
+            p.N_buffered = int(nbuf[i])
+            p._touch()
+        self.kernel_launches += 2 * int(nstep) + 1
+        self.particle_steps = self._ps_base + int(st.particle_steps)
+        self.step = int(st.step)
+        self.t = float(st.t)
+        return list(ms), before, [p.N_buffered for p in self.all_particles]
+
+    def _loop(self, run, nstep, call_back):
+        L = _lib.load()
+        n_seg = len(self.all_particles)
+        nbuf = (ctypes.c_int64 * n_seg)()
+        st = _lib.RunState()
+        remaining = int(nstep)
+        tic = perf_counter_ns()
+        while remaining > 0:
+            chunk = remaining
+            if call_back:
+                chunk = 1
+            if self.print_every:
+                chunk = min(chunk, self.print_every - (self.step % self.print_every))
+            if self._ensure_headroom():
+                self._update_run(run)
+            _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
+                                       _stream_ptr()), "sfp_run_steps")
+            self.kernel_launches += 2 * chunk + 1
+            _lib.check(L.sfp_run_read_state(run, ctypes.byref(st), nbuf, _stream_ptr()), "sfp_run_read_state")
+            if st.error:
+                raise _lib.SFPError(f"device error in the step kernel: {_lib.DEV_ERRORS.get(st.error, st.error)}")
+            done = int(st.step) - self.step
+            for i, p in enumerate(self.all_particles):
+                p.N_buffered = int(nbuf[i])
+            self.particle_steps = self._ps_base + int(st.particle_steps)
+            if done > 0:
+                for p in self.all_particles:
+                    p._refresh_inv_gamma()
+                    p._touch()
+                self.kernel_launches += len(self.all_particles)
+            self.step = int(st.step)
+            self.t = float(st.t)
+            remaining -= done
+            if st.halted:
+                self._ensure_headroom()
+                self._update_run(run)
+                _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
+            if done == 0 and not st.halted:
+                raise _lib.SFPError("the step made no progress")
+            if call_back and done:
+                call_back(self.step - 1)
+            if self.print_every is None or not done:
+                continue
+            elapsed = perf_counter_ns() - tic
+            tic = perf_counter_ns()
+            if self.step % self.print_every == 0 and self.progress_bar is not None:
+                Ntotal = sum([p.Npart for p in self.all_particles])
+                ns_per_particle = elapsed / max(Ntotal, 1) / max(done, 1)
+                particle_num_str = ','.join([f"{p.Npart} {p.name}" for p in self.all_particles])
+                self.progress_bar.set_postfix_str(f"{particle_num_str}, {ns_per_particle:.0f}ns/particle")
+                self.progress_bar.update(self.print_every)
+
+    def _update_run(self, run):
+        segs = self._segments()
+        n = len(self.all_particles)
+        nbuf = (ctypes.c_int64 * n)(*[p.N_buffered for p in self.all_particles])
+        _lib.call("sfp_run_update", run, n, segs, nbuf)
