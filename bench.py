@@ -57,7 +57,7 @@ def beam(n, seed, steps=STEPS_FULL):
     return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
 
 
-def make_sim(n, seed, form="fp64"):
+def make_sim(n, seed, form="fp64", items=0, min_blocks=0):
     import sfparticles_b200 as S
     from sfparticles_b200.fields import gaussian_laser_pulse
     props, L = beam(n, seed)
@@ -68,7 +68,8 @@ def make_sim(n, seed, form="fp64"):
     pos.set_photon(pho)
     pho.set_pair(ele, pos)
     fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
-    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form)
+    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form, items=items,
+                       min_blocks=min_blocks)
     return sim
 
 
@@ -176,7 +177,7 @@ def run_ours(args, rank, world):
     wsim.run_on_device(args.warmup)
     wsim.finish()
     del wsim
-    sim = make_sim(args.electrons, seed, args.form)
+    sim = make_sim(args.electrons, seed, args.form, args.items, args.min_blocks)
     sim._begin()
     torch.cuda.synchronize()
     if world > 1:
@@ -194,12 +195,18 @@ def run_ours(args, rank, world):
     ps = sim.particle_steps
     counts = {p.name: p.N_buffered for p in sim.all_particles}
     # roofline of the step kernel at the final state: CUDA events around each launch
+    from sfparticles_b200 import autotune
+    variant_ms = {}
+    if not args.no_variants:
+        variant_ms = autotune.measure(sim, steps=2)
+        sim.set_kernel(*min(variant_ms, key=variant_ms.get))
     alive = {p.name: p.Npart for p in sim.all_particles}
     kms, before, after = sim.time_step_kernel(args.roofline_steps)
     k_avg_ms = float(np.mean(kms))
     appended = (sum(after) - sum(before)) / args.roofline_steps
     alg_bytes = ((alive["electron"] + alive["positron"]) * BYTES_EPM + alive["photon"] * BYTES_PHOTON
                  + appended * BYTES_APPEND)
+    sim_items, sim_minb = sim.items, sim.min_blocks
     sim.finish()
     del sim
     torch.cuda.empty_cache()
@@ -223,6 +230,39 @@ def run_ours(args, rank, world):
                    wall_s=wall)
         del sim2
 
+    # chosen form vs the plain float64 form, same seed, on a tenth of the beam
+    compare = None
+    if not args.no_compare:
+        from sfparticles_b200 import diagnostics as D
+        res = {}
+        for form in ("fp64", args.form):
+            if form in res:
+                continue
+            s = make_sim(args.compare_electrons, seed + 7, form)
+            s._begin()
+            torch.cuda.synchronize()
+            e0.record()
+            s.run_on_device(args.steps)
+            e1.record()
+            torch.cuda.synchronize()
+            cms = e0.elapsed_time(e1)
+            cps = s.particle_steps
+            s.finish()
+            ele, pos, pho = s.all_particles
+            res[form] = dict(value=cps / (cms * 1e-3), energies=D.photon_energies(pho), pairs=pos.N_buffered,
+                             photons=pho.N_buffered)
+            del s
+        a, b = res[args.form], res["fp64"]
+        hi = max(a["energies"].max(initial=2.0), b["energies"].max(initial=2.0))
+        ha, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=a["energies"])
+        hb, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=b["energies"])
+        compare = {"electrons": args.compare_electrons, "steps": args.steps, "fp64_value": b["value"],
+                   "form_value": a["value"], "speedup_vs_fp64": a["value"] / b["value"],
+                   "spectrum_rel_l1": D.spectrum_rel_l1(ha, hb), "spectrum_bins": 64,
+                   "pair_yield_rel": D.rel_diff(a["pairs"], b["pairs"]), "pairs_fp64": b["pairs"],
+                   "pairs_form": a["pairs"], "photons_fp64": b["photons"], "photons_form": a["photons"]}
+        torch.cuda.empty_cache()
+
     # max over ranks of the device time; sum of work
     tot_ps = ps
     if world > 1:
@@ -237,9 +277,11 @@ def run_ours(args, rank, world):
     return dict(ms=ms, particle_steps=tot_ps, counts=counts, launches=launches, clocks=clk.summary(),
                 roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                           "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                          "kernel": "sfp_step_" + args.form + "_rs", "kernel_avg_ms": k_avg_ms,
+                          "kernel": f"sfp_step_{args.form}_rs_i{sim_items}_b{sim_minb}",
+                          "variants_ms": {f"i{a}_b{b}": v for (a, b), v in variant_ms.items()},
+                          "kernel_avg_ms": k_avg_ms,
                           "alg_bytes_per_launch": alg_bytes, "launches_timed": args.roofline_steps},
-                e2e=e2e)
+                e2e=e2e, compare=compare)
 
 
 def main():
@@ -249,7 +291,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--electrons", type=int, default=10_000_000)
-    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--compare-electrons", type=int, default=1_000_000)
+    ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--items", type=int, default=0)
+    ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--roofline-steps", type=int, default=8)
@@ -304,7 +351,7 @@ def main():
                            "l2": "state > 1 GB per step, larger than L2 (no flush needed)",
                            "final_counts": r["counts"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
-                "clocks": r["clocks"], "particle_steps": r["particle_steps"]}
+                "clocks": r["clocks"], "particle_steps": r["particle_steps"], "vs_fp64": r["compare"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -138,6 +138,8 @@ typedef struct sfp_run_config {
     int64_t step0;           /* steps already taken (Philox step key)     */
     int32_t qed;             /* SFP_QED_*                                  */
     int32_t form;            /* SFP_FORM_*                                 */
+    int32_t items;           /* particles per thread per tile (0 = default)              */
+    int32_t min_blocks;      /* kernel variant: min resident blocks per SM (0 = default) */
     sfp_rs_table rs;
     sfp_od_table od_photon;
     sfp_od_table od_pair;

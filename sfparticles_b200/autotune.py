@@ -1,0 +1,133 @@
+"""Autotuner of the fused step kernel.
+
+Every NVRTC step module holds several variants of the step kernel, named
+``sfp_step_<form>_<qed>_i<items>_b<blocks>``: ``items`` particles per thread
+per tile (a tile is 256 * items particles) and a register budget that keeps
+at least ``blocks`` blocks of 256 threads resident per SM.  Which variant is
+fastest depends on the particle mix (pushed e+- vs photons), the field
+program and the form, so ``tune`` measures them: it builds a sample of the
+simulation's current state (up to ``sample`` particles per species, copied,
+so the user's run is not advanced), times a few steps of each variant with
+CUDA events on the launching stream, and selects the fastest.  Results are
+cached per (GPU, form, QED method, field structure, population bucket) in
+``autotune.json`` beside the NVRTC module cache.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import threading
+
+import numpy as np
+
+from . import program
+
+VARIANTS = {
+    ("fp64", "rs"): [(1, 2), (1, 3), (2, 2)],
+    ("fp64", "od"): [(1, 2), (2, 2)],
+    ("fp32", "rs"): [(1, 2), (1, 3), (1, 4), (2, 2), (2, 3)],
+    ("fp32", "od"): [(1, 3), (2, 2)],
+}
+DEFAULT = {("fp64", "rs"): (1, 2), ("fp64", "od"): (1, 2), ("fp32", "rs"): (1, 3), ("fp32", "od"): (1, 3)}
+
+_lock = threading.Lock()
+
+
+def _cache_path():
+    return os.path.join(program.CACHE, "autotune.json")
+
+
+def _load():
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store(d):
+    os.makedirs(program.CACHE, exist_ok=True)
+    tmp = _cache_path() + f".{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, _cache_path())
+
+
+def cache_key(sim) -> str:
+    import torch
+    name = torch.cuda.get_device_name()
+    n = sum(p.N_buffered for p in sim.all_particles)
+    bucket = int(math.log2(max(n, 1)))
+    mix = "-".join(("g" if p.m == 0 else "e") for p in sim.all_particles)
+    return f"{name}|{sim.form}|{sim.qed_method}|{sim.fields.structure()}|{mix}|2^{bucket}"
+
+
+def _sample_sim(sim, sample):
+    """A copy of the simulation's current state, at most `sample` alive
+    particles per species, same fields / form / QED method."""
+    from .particles import Particles, SpinParticles
+    from .simulation import Simulation
+    import torch
+    copies = {}
+    for p in sim.all_particles:
+        p._to_gpu()
+        pr = p._d("_to_be_pruned")[: p.N_buffered]
+        keep = torch.nonzero(pr == 0).flatten()[:sample]
+        props = [p._d(k)[keep].cpu().numpy() for k in ("x", "y", "z", "ux", "uy", "uz")]
+        n = int(keep.numel())
+        q = round(p.q / 1.602176634e-19)
+        m = 0 if p.m == 0 else 1
+        if "sx" in p.attrs:
+            props += [p._d(k)[keep].cpu().numpy() for k in ("sx", "sy", "sz")]
+            c = SpinParticles(p.name, q, m, N=n, props=props if n else None, RR=p.RR, ae=p.ae, push=p.push)
+        else:
+            c = Particles(p.name, q, m, N=n, props=props if n else None, RR=p.RR, push=p.push)
+        copies[id(p)] = c
+    for p in sim.all_particles:
+        c = copies[id(p)]
+        if p.radiating:
+            c.set_photon(copies[id(p.photon_ref())])
+        if p.bw:
+            c.set_pair(copies[id(p.bw_electron_ref())], copies[id(p.bw_positron_ref())])
+    s = Simulation(*[copies[id(p)] for p in sim.all_particles], dt=sim.dt, fields=sim.fields, print_every=None,
+                   photon_threshold=sim.photon_threshold, seed=sim.seed, form=sim.form, graph_chunk=0)
+    s.t = sim.t
+    s.step = sim.step
+    return s
+
+
+def measure(sim, variants=None, steps: int = 3):
+    """Median step-kernel time [ms] of each variant on `sim`'s current state.
+    Advances `sim` by len(variants) * steps steps."""
+    variants = variants or VARIANTS[(sim.form, sim.qed_method)]
+    out = {}
+    for items, minb in variants:
+        sim.set_kernel(items, minb)
+        ms, _, _ = sim.time_step_kernel(steps)
+        out[(items, minb)] = float(np.median(ms))
+    return out
+
+
+def tune(sim, sample: int = 2_000_000, steps: int = 3, use_cache: bool = True):
+    """Select the fastest step-kernel variant for `sim` (see module doc)."""
+    key = cache_key(sim)
+    with _lock:
+        cache = _load() if use_cache else {}
+        if key in cache:
+            items, minb = cache[key]["best"]
+            sim.set_kernel(items, minb)
+            return (items, minb), cache[key].get("ms", {})
+    s = _sample_sim(sim, sample)
+    try:
+        times = measure(s, steps=steps)
+    finally:
+        s.finish()
+    best = min(times, key=times.get)
+    sim.set_kernel(*best)
+    if use_cache:
+        with _lock:
+            cache = _load()
+            cache[key] = {"best": list(best), "ms": {f"i{a}_b{b}": v for (a, b), v in times.items()}}
+            _store(cache)
+    return best, times

@@ -59,7 +59,7 @@ def prebuild_modules(verbose: bool = False):
     """Compile the field-specialised step modules of the presets (NVRTC)."""
     from . import fields, program
     for f in fields.preset_structures():
-        for form in ("fp64",):
+        for form in ("fp64", "fp32"):
             for qed in ("rs", "od"):
                 program.get_module(f, form=form, qed=qed, load=False)
         program.get_module(f, form=None, qed=None, load=False)

@@ -729,12 +729,16 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     r->n_seg = n_seg;
     r->n_inst = n_inst;
     r->segs.assign(seg, seg + n_seg);
-    const char* kname = nullptr;
-    if (cfg->form == SFP_FORM_FP64)
-        kname = cfg->qed == SFP_QED_REJECTION ? "sfp_step_fp64_rs" : "sfp_step_fp64_od";
-    else
-        kname = cfg->qed == SFP_QED_REJECTION ? "sfp_step_fp32_rs" : "sfp_step_fp32_od";
-    if ((rc = module_kernel(m, kname, &r->k_step)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
+    const int items = cfg->items > 0 ? cfg->items : 1;
+    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (cfg->form == SFP_FORM_FP64 ? 2 : 3);
+    if (items < 1 || items > 4 || minb < 1 || minb > 8) {
+        delete r;
+        return fail(SFP_EINVAL, "kernel variant out of range");
+    }
+    std::string kname = std::string("sfp_step_") + (cfg->form == SFP_FORM_FP64 ? "fp64_" : "fp32_") +
+                        (cfg->qed == SFP_QED_REJECTION ? "rs" : "od") + "_i" + std::to_string(items) + "_b" +
+                        std::to_string(minb);
+    if ((rc = module_kernel(m, kname.c_str(), &r->k_step)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
         delete r;
         return rc;
     }
@@ -752,7 +756,7 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     h.dt = cfg->dt;
     h.photon_threshold = cfg->photon_threshold;
     h.qed = cfg->qed;
-    h.tile = SFP_TILE_HOST;
+    h.tile = SFP_TILE_HOST * items;
     h.any_appends = 0;
     for (int s = 0; s < n_seg; ++s) h.any_appends |= (seg[s].radiating || seg[s].bw) ? 1 : 0;
     h.rs = cfg->rs;
@@ -781,11 +785,11 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     st0.skip = 1;
     if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "state upload"));
-    if ((rc = run_alloc_tiles(r, tiles_for(r->segs, SFP_TILE_HOST)))) return cleanup(rc);
+    if ((rc = run_alloc_tiles(r, tiles_for(r->segs, h.tile)))) return cleanup(rc);
     if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
     // shared memory for the tables, persistent grid size
     if (cfg->qed == SFP_QED_REJECTION)
-        r->smem = 2 * (size_t)cfg->rs.z_N * sizeof(double);
+        r->smem = 2 * (size_t)cfg->rs.z_N * (cfg->form == SFP_FORM_FP64 ? sizeof(double) : sizeof(float));
     else
         r->smem = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
     if (r->smem > 48 * 1024) {
@@ -809,7 +813,7 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
     if (!r || !seg) return fail(SFP_EINVAL, "sfp_run_update: NULL argument");
     if (n_seg != r->n_seg) return fail(SFP_EINVAL, "sfp_run_update: segment count changed");
     r->segs.assign(seg, seg + n_seg);
-    int rc = run_alloc_tiles(r, tiles_for(r->segs, SFP_TILE_HOST));
+    int rc = run_alloc_tiles(r, tiles_for(r->segs, r->h.tile));
     if (rc) return rc;
     return run_upload(r, nullptr, n_buffered);
 }

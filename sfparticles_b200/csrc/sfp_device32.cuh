@@ -1,0 +1,164 @@
+// sfp_device32.cuh -- float32 arithmetic of the fused step's FP32 form.
+//
+// The particle state stays float64 in HBM.  Fields, chi, the QED samplers
+// and the Boris / Thomas-BMT / Landau-Lifshitz updates are evaluated in
+// float32 (MUFU transcendentals after explicit range reduction), and every
+// update is applied as a float32 INCREMENT to the float64 state:
+//   x += dx,  u += du,  s += ds          (float64 accumulation of float32 steps)
+// so rounding errors scale with the step, not with |x|, |u| (the role Kahan
+// compensation plays for float32 storage).  gamma = sqrt(1 + u^2) is taken in
+// float64 when gamma > 1e4, where 1 + u^2 is below float32 resolution.
+// The phase argument x - x0 - dir c t of the pulses is formed in float64.
+#pragma once
+#include "sfp_device.cuh"
+
+namespace sfp32 {
+
+constexpr float kTwoPi = 6.28318530717958647692f;
+constexpr float kInvTwoPi = 0.15915494309189533577f;
+constexpr float kCf = 299792458.0f;
+// Schwinger field E_s = m^2 c^3 / (e hbar); chi is formed in units of E_s
+constexpr double kEs = (sfp::kMe * sfp::kMe) * (sfp::kC * (sfp::kC * sfp::kC)) / (sfp::kE * sfp::kHbar);
+constexpr float kInvEs = (float)(1.0 / kEs);
+constexpr float kCOverEs = (float)(sfp::kC / kEs);
+constexpr double kGammaSplit = 1.0e4;
+
+// cos / sin of a float32 phase of any size: reduce to [-pi, pi], then MUFU
+SFP_DEVICE_INLINE float cos_r(float a) {
+    const float k = rintf(a * kInvTwoPi);
+    return __cosf(fmaf(-k, kTwoPi, a));
+}
+SFP_DEVICE_INLINE float sin_r(float a) {
+    const float k = rintf(a * kInvTwoPi);
+    return __sinf(fmaf(-k, kTwoPi, a));
+}
+
+// uniforms of 24 bits (r1) and 32-bit resolution near 0 (r2), in (0, 1).
+// They are taken from the same Philox words as the float64 draws
+// (sfp::uniform2: r1 <- word 0, r2 <- word 2), so both forms see the same
+// random numbers to float32 precision and make the same event decisions
+// except within float32 rounding of the acceptance threshold.
+SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, unsigned int step,
+                                 unsigned int purpose, long long slot, float& r1, float& r2) {
+    const unsigned long long s = (unsigned long long)slot;
+    sfp::U4 c{(unsigned int)s, ((unsigned int)(s >> 32) & 0x00FFFFFFu) | (purpose << 24), step, stream};
+    sfp::U4 o = sfp::philox4x32_10(c, (unsigned int)seed, (unsigned int)(seed >> 32));
+    r1 = ((float)(o.x >> 8) + 0.5f) * 0x1p-24f;
+    r2 = __uint2float_rn(o.z) * 0x1p-32f + 0x1p-33f;
+}
+
+// ---- field presets (same parameter blocks as the float64 forms) ----------
+// gaussian_laser_pulse (fields.py:152-168); the curvature term k0 r^2 / (2 Rx)
+// is written as k0 r^2 x / (2 (x^2 + zR^2)), finite at x = 0.
+SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
+                                      float F[6]) {
+    const float E0 = (float)P[0], k0 = (float)P[1], zR = (float)P[2], w0 = (float)P[3], ctau = (float)P[4];
+    const double dir = P[5], x0 = P[6];
+    const float cep = (float)P[7], cp = (float)P[8], sp = (float)P[9];
+    const float xf = (float)x, yf = (float)y, zf = (float)z;
+    const float xr = (float)((x - x0) - (dir * sfp::kC) * t);
+    const float r2 = yf * yf + zf * zf;
+    const float xz = xf / zR;
+    const float q = 1.0f + xz * xz;
+    const float wx2 = (w0 * w0) * q;
+    const float gouy = atanf(xz);
+    const float phi = k0 * xr + (k0 * r2 * xf) / (2.0f * (xf * xf + zR * zR)) - gouy;
+    const float kc = k0 * ctau;
+    const float env = __expf(-(r2 / wx2 + (phi * phi) / (kc * kc)));
+    const float E = E0 * cos_r(phi + cep) * rsqrtf(q) * env;
+    const float Ey = E * cp, Ez = E * sp;
+    const float d = (float)dir;
+    F[0] = 0.0f;
+    F[1] = Ey;
+    F[2] = Ez;
+    F[3] = 0.0f;
+    F[4] = -Ez * (d / kCf);
+    F[5] = Ey * (d / kCf);
+}
+
+// simple_laser_pulse (fields.py:102-116)
+SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, double y, double z, double t, float F[6]) {
+    const float E0 = (float)P[0], k0 = (float)P[1], w0 = (float)P[2], ctau = (float)P[3];
+    const double dir = P[4], x0 = P[5];
+    const float cep = (float)P[6], cp = (float)P[7], sp = (float)P[8];
+    const int tord = (int)P[9];
+    const float yf = (float)y, zf = (float)z;
+    const float phi = k0 * (float)((dir * x - dir * x0) - sfp::kC * t);
+    const float r2 = yf * yf + zf * zf;
+    float num, den;
+    const float kc = k0 * ctau;
+    if (P[10] != 0.0 && tord == 2) {
+        num = phi * phi;
+        den = kc * kc;
+    } else {
+        num = powf(phi, (float)P[9]);
+        den = powf(kc, (float)P[9]);
+    }
+    const float E = E0 * cos_r(phi + cep) * __expf(-(r2 / (w0 * w0)) - num / den);
+    const float Ey = E * cp, Ez = E * sp;
+    const float d = (float)dir;
+    F[0] = 0.0f;
+    F[1] = Ey;
+    F[2] = Ez;
+    F[3] = 0.0f;
+    F[4] = -Ez * (d / kCf);
+    F[5] = Ey * (d / kCf);
+}
+
+SFP_DEVICE_INLINE void field_static(const double* __restrict__ P, float F[6]) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) F[i] = (float)P[i];
+}
+
+// focused_gaussian_laser_pulse: evaluated in float64 (its eps^5 expansion
+// cancels), returned as float32
+SFP_DEVICE_INLINE void field_focused(const double* __restrict__ P, double x, double y, double z, double t, float F[6]) {
+    double D[6];
+    sfp::field_focused(P, x, y, z, t, D);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) F[i] = (float)D[i];
+}
+
+// ---- chi (inline.py:126-134) in Schwinger units ----------------------------
+SFP_DEVICE_INLINE float chi_of(const float F[6], float ux, float uy, float uz, float gamma) {
+    const float Ex = F[0] * kInvEs, Ey = F[1] * kInvEs, Ez = F[2] * kInvEs;
+    const float Bx = F[3] * kCOverEs, By = F[4] * kCOverEs, Bz = F[5] * kCOverEs;
+    const float a = gamma * Ex + (uy * Bz - uz * By);
+    const float b = gamma * Ey + (uz * Bx - ux * Bz);
+    const float c = gamma * Ez + (ux * By - uy * Bx);
+    const float s = ux * Ex + uy * Ey + uz * Ez;
+    const float rad = a * a + b * b + c * c - s * s;
+    return rad > 0.0f ? sqrtf(rad) : 0.0f;
+}
+
+// gamma of u (float64 state), float64 above the split
+SFP_DEVICE_INLINE float gamma_of(double ux, double uy, double uz, bool massless) {
+    const float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    const float u2 = fx * fx + fy * fy + fz * fz;
+    if (massless) return sqrtf(u2);
+    if (u2 < (float)(kGammaSplit * kGammaSplit)) return sqrtf(1.0f + u2);
+    return (float)sqrt(((1.0 + ux * ux) + uy * uy) + uz * uz);
+}
+
+// ---- rejection sampling (qed/rejection_sampling*.py) -----------------------
+SFP_DEVICE_INLINE float ai_lerp(const float* __restrict__ tab, float z, float inv_dz, int zN) {
+    const float fi = z * inv_dz;
+    int i = (int)fi;
+    if (i > zN - 2) i = zN - 2;
+    const float w = fi - (float)i;
+    return fmaf(w, tab[i + 1] - tab[i], tab[i]);
+}
+
+// dW/ddelta up to the common factor alpha m c^2 / hbar; sign s = +1 photon
+// emission (2/z + chi_g sqrt z), -1 pair creation (2/z - chi_g sqrt z)
+SFP_DEVICE_INLINE float rate_core(float chi_g, float base, const float* __restrict__ iAt, const float* __restrict__ dAt,
+                                  float inv_dz, int zN, float base_max, float sgn) {
+    // z = base^(2/3) > z_max  <=>  base > z_max^(3/2) = base_max
+    if (!(base <= base_max)) return 0.0f;
+    const float z = exp2f(0.66666667f * __log2f(base));
+    const float iA = ai_lerp(iAt, z, inv_dz, zN);
+    const float dA = ai_lerp(dAt, z, inv_dz, zN);
+    return iA + (2.0f / z + sgn * chi_g * sqrtf(z)) * dA;
+}
+
+}  // namespace sfp32

@@ -19,6 +19,7 @@
 // would give it, so Philox streams keyed by slot are reproducible.
 #pragma once
 #include "sfp_device.cuh"
+#include "sfp_device32.cuh"
 #include "sfp_run.cuh"
 
 #ifndef SFP_TILE
@@ -75,26 +76,49 @@ SFP_DEVICE_INLINE uint4 warp_sum_u4(uint4 v) {
 }
 
 // Decoupled look-back (Merrill & Garland, 2016) over the tiles of one
-// instance, run by warp 0.  Returns the exclusive per-channel prefix.
-// Every wait is bounded; on timeout the run's error word is set.
-SFP_DEVICE_INLINE uint4 lookback(const sfp_run_dev* R, long long tile, long long first_tile, uint4 agg,
-                                 unsigned int epoch) {
+// instance, run by warp 0.  A tile publishes its aggregate (AGG) as soon as
+// its events are known and its inclusive prefix (INCL) once the exclusive
+// prefix is known; look-backs sum predecessors' AGGs until an INCL.
+SFP_DEVICE_INLINE void publish(const sfp_run_dev* R, long long tile, uint4 v, unsigned int epoch, bool incl) {
+    if ((threadIdx.x & 31) == 0) {
+        st_cg_u4((incl ? R->tile_incl : R->tile_agg) + tile, v);
+        st_release_u32(R->tile_flag + tile, (epoch << 2) | (incl ? SFP_FLAG_INCL : SFP_FLAG_AGG));
+    }
+}
+
+// one window of 32 predecessors without waiting: true (and the exclusive
+// prefix) when an INCL is reached through ready tiles only
+SFP_DEVICE_INLINE bool lookback_try(const sfp_run_dev* R, long long tile, long long first_tile, unsigned int epoch,
+                                    uint4& excl) {
+    const int lane = threadIdx.x & 31;
+    const long long p = tile - 1 - lane;
+    const bool valid = p >= first_tile;
+    unsigned int status = 0;
+    if (valid) {
+        const unsigned int f = ld_acquire_u32(R->tile_flag + p);
+        if ((f >> 2) == epoch) status = f & 3u;
+    }
+    const unsigned int incl_mask = __ballot_sync(0xffffffffu, valid && status == SFP_FLAG_INCL);
+    const unsigned int ready_mask = __ballot_sync(0xffffffffu, valid && status != 0u);
+    if (!incl_mask) return false;
+    const int k = __ffs(incl_mask) - 1;
+    const unsigned int need = (k == 31) ? 0xffffffffu : ((1u << (k + 1)) - 1u);
+    if ((ready_mask & need) != need) return false;
+    uint4 v{0u, 0u, 0u, 0u};
+    if (lane < k) v = ld_cg_u4(R->tile_agg + p);
+    else if (lane == k) v = ld_cg_u4(R->tile_incl + p);
+    excl = warp_sum_u4(v);
+    return true;
+}
+
+// blocking look-back; every wait is bounded, and on timeout the run's error
+// word is set and the tile still publishes so that no successor waits on it
+SFP_DEVICE_INLINE uint4 lookback_wait(const sfp_run_dev* R, long long tile, long long first_tile, unsigned int epoch) {
     const int lane = threadIdx.x & 31;
     uint4 excl{0u, 0u, 0u, 0u};
-    if (tile == first_tile) {
-        if (lane == 0) {
-            st_cg_u4(R->tile_incl + tile, agg);
-            st_release_u32(R->tile_flag + tile, (epoch << 2) | SFP_FLAG_INCL);
-        }
-        return excl;
-    }
-    if (lane == 0) {
-        st_cg_u4(R->tile_agg + tile, agg);
-        st_release_u32(R->tile_flag + tile, (epoch << 2) | SFP_FLAG_AGG);
-    }
     long long base = tile - 1;
     bool failed = false;
-    while (true) {
+    while (base >= first_tile) {
         const long long p = base - lane;
         const bool valid = p >= first_tile;
         unsigned int status = 0;
@@ -115,12 +139,7 @@ SFP_DEVICE_INLINE uint4 lookback(const sfp_run_dev* R, long long tile, long long
             }
         }
         if (__any_sync(0xffffffffu, failed)) {
-            // give up: flag the run and still publish, so no successor waits on this tile
-            if (lane == 0) {
-                atomicExch(&R->st->error, SFP_DEV_LOOKBACK_TIMEOUT);
-                st_cg_u4(R->tile_incl + tile, agg);
-                st_release_u32(R->tile_flag + tile, (epoch << 2) | SFP_FLAG_INCL);
-            }
+            if (lane == 0) atomicExch(&R->st->error, SFP_DEV_LOOKBACK_TIMEOUT);
             return uint4{0u, 0u, 0u, 0u};
         }
         const unsigned int incl_mask = __ballot_sync(0xffffffffu, valid && status == SFP_FLAG_INCL);
@@ -135,11 +154,6 @@ SFP_DEVICE_INLINE uint4 lookback(const sfp_run_dev* R, long long tile, long long
         if (valid) v = ld_cg_u4(R->tile_agg + p);
         excl = u4_add(excl, warp_sum_u4(v));
         base -= 32;
-        if (base < first_tile) break;  // unreachable: the first tile publishes INCL
-    }
-    if (lane == 0) {
-        st_cg_u4(R->tile_incl + tile, u4_add(excl, agg));
-        st_release_u32(R->tile_flag + tile, (epoch << 2) | SFP_FLAG_INCL);
     }
     return excl;
 }
@@ -168,6 +182,82 @@ SFP_DEVICE_INLINE void push_photon(double& x, double& y, double& z, double ux, d
     const double ig = inv_gamma_photon(ux, uy, uz);
     push_position(x, y, z, ux, uy, uz, ig, 0.5 * dt);
     push_position(x, y, z, ux, uy, uz, ig, 0.5 * dt);
+}
+
+// float32 form of push_massive: float32 increments, float64 accumulation.
+SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& ux, double& uy, double& uz,
+                                      double& sx, double& sy, double& sz, const sfp_segment& S,
+                                      const double* __restrict__ P, double t, double dt) {
+    const float hc = (float)(0.5 * kC * dt);
+    float g = sfp32::gamma_of(ux, uy, uz, false);
+    float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    float a = hc / g;
+    x += (double)(a * fx);
+    y += (double)(a * fy);
+    z += (double)(a * fz);
+    float F[6];
+    sfp_field_program32(x, y, z, t + 0.5 * dt, P, F);
+    const float eps = (float)((S.q * dt) / ((2.0 * kMe) * kC));
+    const float bq = (float)((S.q * dt) / (2.0 * kMe));
+    const float ex = eps * F[0], ey = eps * F[1], ez = eps * F[2];
+    const float umx = fx + ex, umy = fy + ey, umz = fz + ez;
+    float gm;
+    if (g < (float)sfp32::kGammaSplit) {
+        gm = sqrtf(1.0f + umx * umx + umy * umy + umz * umz);
+    } else {
+        const double dx = ux + (double)ex, dy = uy + (double)ey, dz = uz + (double)ez;
+        gm = (float)sqrt(((1.0 + dx * dx) + dy * dy) + dz * dz);
+    }
+    const float igm = 1.0f / gm;
+    if (S.spin) {  // inline.py:39-70: spin rotation with B_eff(u-), as an increment
+        const float ae = (float)S.ae;
+        const float uB = umx * F[3] + umy * F[4] + umz * F[5];
+        const float a1 = ae + igm, a2 = ae * gm / (gm + 1.0f), a3 = ae + 1.0f / (gm + 1.0f);
+        const float bex = a1 * F[3] - a2 * uB * umx - a3 * (umy * F[2] - umz * F[1]);
+        const float bey = a1 * F[4] - a2 * uB * umy - a3 * (umz * F[0] - umx * F[2]);
+        const float bez = a1 * F[5] - a2 * uB * umz - a3 * (umx * F[1] - umy * F[0]);
+        const float Tx = bq * bex, Ty = bq * bey, Tz = bq * bez;
+        const float f2 = 2.0f / (1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
+        const float s0x = (float)sx, s0y = (float)sy, s0z = (float)sz;
+        const float spx = s0x + (s0y * Tz - s0z * Ty), spy = s0y + (s0z * Tx - s0x * Tz), spz = s0z + (s0x * Ty - s0y * Tx);
+        sx += (double)(f2 * (spy * Tz - spz * Ty));
+        sy += (double)(f2 * (spz * Tx - spx * Tz));
+        sz += (double)(f2 * (spx * Ty - spy * Tx));
+    }
+    // Boris (inline.py:4-36) as u += 2 eps E + u' x S
+    const float Tx = bq * F[3] * igm, Ty = bq * F[4] * igm, Tz = bq * F[5] * igm;
+    const float upx = umx + (umy * Tz - umz * Ty), upy = umy + (umz * Tx - umx * Tz), upz = umz + (umx * Ty - umy * Tx);
+    const float f2 = 2.0f / (1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
+    ux += (double)(2.0f * ex + f2 * (upy * Tz - upz * Ty));
+    uy += (double)(2.0f * ey + f2 * (upz * Tx - upx * Tz));
+    uz += (double)(2.0f * ez + f2 * (upx * Ty - upy * Tx));
+    g = sfp32::gamma_of(ux, uy, uz, false);
+    if (S.rr == SFP_RR_LL || (S.rr == SFP_RR_CLL && !S.spin)) {  // inline.py:104-123
+        fx = (float)ux; fy = (float)uy; fz = (float)uz;
+        const float chi = sfp32::chi_of(F, fx, fy, fz, g);
+        float factor = (float)ll_factor(dt);
+        if (S.rr == SFP_RR_CLL) {
+            const float q = 1.0f + 4.8f * (1.0f + chi) * __logf(1.0f + 1.7f * chi) + 2.44f * chi * chi;
+            factor *= exp2f(-0.66666667f * __log2f(q));
+        }
+        const float c = factor * chi * chi / g;
+        ux += (double)(c * fx);
+        uy += (double)(c * fy);
+        uz += (double)(c * fz);
+        g = sfp32::gamma_of(ux, uy, uz, false);
+    }
+    a = hc / g;
+    x += (double)(a * (float)ux);
+    y += (double)(a * (float)uy);
+    z += (double)(a * (float)uz);
+}
+
+SFP_DEVICE_INLINE void push_photon32(double& x, double& y, double& z, double ux, double uy, double uz, double dt) {
+    const float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    const float a = (float)(kC * dt) * rsqrtf(fx * fx + fy * fy + fz * fz);
+    x += (double)(a * fx);
+    y += (double)(a * fy);
+    z += (double)(a * fz);
 }
 
 }  // namespace sfp
@@ -248,15 +338,23 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
 }
 
 // ---------------------------------------------------------------------------
-// The fused step, float64 form.  Persistent grid; tiles handed out in order.
+// The fused step.  Persistent grid; tiles of SFP_TILE * ITEMS particles are
+// handed out in order; item k of thread j covers particle k*SFP_TILE + j of
+// the tile, so the ordered append scans items k-major.
+//
+// Per tile:  load -> QED events -> publish the tile's append count (and try
+// a non-blocking look-back) -> recoil + push every parent (registers) ->
+// finish the look-back -> write children (from the parent's stored,
+// not yet overwritten state) -> store the parents.  The look-back wait is
+// thus taken after the expensive push, when the predecessors are done.
 // ---------------------------------------------------------------------------
-template <int QED>
-__device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R) {
+template <int FORM, int QED, int ITEMS>
+__device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
     extern __shared__ double s_tab[];
     __shared__ long long s_tile;
     __shared__ int s_seg;
-    __shared__ unsigned int s_warp[SFP_TILE / 32];
+    __shared__ unsigned int s_warp[ITEMS][SFP_TILE / 32];
     __shared__ uint4 s_excl;
 
     sfp_step_state* st = R->st;
@@ -267,9 +365,11 @@ __device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R)
     const unsigned int step = (unsigned int)st->step;
     const unsigned int epoch = st->epoch;
 
-    // tables into shared memory
+    // QED tables into shared memory (float64 or float32 copies)
     const double* iAt = s_tab;
     const double* dAt = s_tab;
+    const float* iAf = reinterpret_cast<const float*>(s_tab);
+    const float* dAf = iAf;
     const double* od_rate_ph = s_tab;
     const double* od_rate_pa = s_tab;
     int zN = 0;
@@ -277,17 +377,34 @@ __device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R)
     if (QED == SFP_QED_REJECTION) {
         zN = R->rs.z_N;
         zmax = R->rs.z_max;
-        for (int i = threadIdx.x; i < zN; i += blockDim.x) {
-            s_tab[i] = R->rs.int_Ai[i];
-            s_tab[zN + i] = R->rs.Aip[i];
+        if (FORM == SFP_FORM_FP64) {
+            for (int i = threadIdx.x; i < zN; i += blockDim.x) {
+                s_tab[i] = R->rs.int_Ai[i];
+                s_tab[zN + i] = R->rs.Aip[i];
+            }
+            dAt = s_tab + zN;
+        } else {
+            float* f = reinterpret_cast<float*>(s_tab);
+            for (int i = threadIdx.x; i < zN; i += blockDim.x) {
+                f[i] = (float)R->rs.int_Ai[i];
+                f[zN + i] = (float)R->rs.Aip[i];
+            }
+            dAf = f + zN;
         }
-        dAt = s_tab + zN;
     } else {
         const int n1 = R->od_photon.chi_N, n2 = R->od_pair.chi_N;
         for (int i = threadIdx.x; i < n1; i += blockDim.x) s_tab[i] = R->od_photon.rate_total[i];
         for (int i = threadIdx.x; i < n2; i += blockDim.x) s_tab[n1 + i] = R->od_pair.rate_total[i];
         od_rate_pa = s_tab + n1;
     }
+    const float inv_dzf = (float)((double)(zN - 1) / zmax);
+    const float base_maxf = (float)(zmax * sqrt(zmax));
+    // pair creation needs z_min = (4/chi)^(2/3) <= z_max (the rate is 0 above
+    // the table): below this chi no pair event can happen, exactly
+    const double chi_pair_min = QED == SFP_QED_REJECTION ? 4.0 / (zmax * sqrt(zmax)) * (1.0 - 1e-6) : 0.0;
+    const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);  // alpha m c^2 / hbar
+    const float thrf = (float)R->photon_threshold;
+    const bool any_appends = R->any_appends != 0;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     while (true) {
@@ -296,7 +413,7 @@ __device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R)
             const long long tk = (long long)atomicAdd(&st->ticket, 1);
             s_tile = tk;
             int s = 0;
-            if (tk < n_tiles) {  // largest s with tile_start[s] <= tk < tile_start[s+1]
+            if (tk < n_tiles) {  // largest s with tile_start[s] <= tk
                 int lo = 0, hi = R->n_seg - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
@@ -316,50 +433,102 @@ __device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R)
         const double* __restrict__ P = I.field_params;
         const long long N = R->n_buf_step[si];
         const long long first_tile = R->tile_start[I.first_seg];
-        const long long i = (tile - R->tile_start[si]) * (long long)SFP_TILE + threadIdx.x;
+        const long long i0 = (tile - R->tile_start[si]) * (long long)(SFP_TILE * ITEMS) + threadIdx.x;
+        const bool qed_seg = S.radiating || S.bw;
 
-        const bool alive = (i < N) && (S.pruned[i] == 0);
-        double x = 0, y = 0, z = 0, ux = 0, uy = 0, uz = 0, sx = 0, sy = 0, sz = 0, tau = 0;
-        if (alive) {
-            x = S.x[i]; y = S.y[i]; z = S.z[i];
-            ux = S.ux[i]; uy = S.uy[i]; uz = S.uz[i];
-            if (S.spin) { sx = S.sx[i]; sy = S.sy[i]; sz = S.sz[i]; }
-            if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau = S.tau[i];
+        bool alive[ITEMS], ev[ITEMS];
+        double x[ITEMS], y[ITEMS], z[ITEMS], ux[ITEMS], uy[ITEMS], uz[ITEMS], tau[ITEMS], delta[ITEMS];
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const long long i = i0 + (long long)k * SFP_TILE;
+            alive[k] = (i < N) && (S.pruned[i] == 0);
+            ev[k] = false;
+            delta[k] = 0.0;
+            x[k] = y[k] = z[k] = ux[k] = uy[k] = uz[k] = tau[k] = 0.0;
+            if (alive[k]) {
+                x[k] = S.x[i]; y[k] = S.y[i]; z[k] = S.z[i];
+                ux[k] = S.ux[i]; uy[k] = S.uy[i]; uz[k] = S.uz[i];
+                if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau[k] = S.tau[i];
+            }
         }
 
         // --- QED events at t (fields at t only for pushed species) ---------
-        bool ev = false;
-        double delta = 0.0;
-        if (alive && (S.radiating || S.bw)) {
-            double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (S.push) sfp_field_program(x, y, z, t, P, F);
-            const double ig = S.massless ? inv_gamma_photon(ux, uy, uz) : inv_gamma_massive(ux, uy, uz);
-            const double chi = chi_of(F, ux, uy, uz, ig);
-            if (QED == SFP_QED_REJECTION) {
-                if (chi != 0.0) {
-                    double r1, r2;
-                    uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
-                    if (S.bw)
-                        ev = pair_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, delta);
-                    else
-                        ev = photon_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, delta);
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            if (!(alive[k] && qed_seg)) continue;
+            const long long i = i0 + (long long)k * SFP_TILE;
+            if (FORM == SFP_FORM_FP64) {
+                double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (S.push) sfp_field_program(x[k], y[k], z[k], t, P, F);
+                const double ig = S.massless ? inv_gamma_photon(ux[k], uy[k], uz[k])
+                                             : inv_gamma_massive(ux[k], uy[k], uz[k]);
+                const double chi = chi_of(F, ux[k], uy[k], uz[k], ig);
+                double d = 0.0;
+                if (QED == SFP_QED_REJECTION) {
+                    if (chi != 0.0 && !(S.bw && chi < chi_pair_min)) {
+                        double r1, r2;
+                        uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
+                        ev[k] = S.bw ? pair_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, d)
+                                     : photon_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, d);
+                    }
+                } else {
+                    ev[k] = S.bw ? od_event(chi, ig, dt, tau[k], R->od_pair, od_rate_pa, I.seed, S.stream, step, i, d)
+                                 : od_event(chi, ig, dt, tau[k], R->od_photon, od_rate_ph, I.seed, S.stream, step, i, d);
                 }
+                if (ev[k] && S.radiating && d / ig < R->photon_threshold) ev[k] = false;  // cpu.py:226-231
+                delta[k] = d;
             } else {
-                if (S.bw)
-                    ev = od_event(chi, ig, dt, tau, R->od_pair, od_rate_pa, I.seed, S.stream, step, i, delta);
-                else
-                    ev = od_event(chi, ig, dt, tau, R->od_photon, od_rate_ph, I.seed, S.stream, step, i, delta);
+                float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (S.push) sfp_field_program32(x[k], y[k], z[k], t, P, F);
+                const float g = sfp32::gamma_of(ux[k], uy[k], uz[k], S.massless != 0);
+                const float chi = sfp32::chi_of(F, (float)ux[k], (float)uy[k], (float)uz[k], g);
+                double d = 0.0;
+                if (QED == SFP_QED_REJECTION) {
+                    if (chi > 0.0f && !(S.bw && (double)chi < chi_pair_min)) {
+                        float r1, r2;
+                        sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+                        const float dtau = (float)dt / g;
+                        if (S.bw) {  // qed/rejection_sampling.py:92-107, delta = r1
+                            const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
+                            const float W = kRate * sfp32::rate_core(chi, base, iAf, dAf, inv_dzf, zN, base_maxf, -1.0f);
+                            ev[k] = r2 < W * dtau;
+                            d = (double)r1;
+                        } else {  // qed/rejection_sampling.py:73-89, delta = r1^3
+                            const float dl = r1 * r1 * r1;
+                            const float base = dl / ((1.0f - dl) * chi);
+                            const float W = -kRate * sfp32::rate_core(dl * chi, base, iAf, dAf, inv_dzf, zN, base_maxf, 1.0f);
+                            ev[k] = r2 < 3.0f * r1 * r1 * W * dtau;
+                            d = (double)dl;
+                            if (ev[k] && dl * g < thrf) ev[k] = false;
+                        }
+                    }
+                } else {
+                    const double igd = 1.0 / (double)g;
+                    ev[k] = S.bw ? od_event((double)chi, igd, dt, tau[k], R->od_pair, od_rate_pa, I.seed, S.stream, step,
+                                            i, d)
+                                 : od_event((double)chi, igd, dt, tau[k], R->od_photon, od_rate_ph, I.seed, S.stream,
+                                            step, i, d);
+                    if (ev[k] && S.radiating && d * (double)g < R->photon_threshold) ev[k] = false;
+                }
+                if (!ev[k]) d = 0.0;
+                delta[k] = d;
             }
-            if (ev && S.radiating && delta / ig < R->photon_threshold) ev = false;  // cpu.py:226-231
         }
 
-        // --- ordered slots: block scan + look-back -------------------------
-        const unsigned int bal = __ballot_sync(0xffffffffu, ev);
-        const unsigned int wpre = __popc(bal & ((1u << lane) - 1u));
-        if (lane == 0) s_warp[warp] = __popc(bal);
+        // --- tile count: block scan (k-major); publish, try the look-back ---
+        unsigned int wpre[ITEMS];
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const unsigned int bal = __ballot_sync(0xffffffffu, ev[k]);
+            wpre[k] = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0) s_warp[k][warp] = __popc(bal);
+        }
         __syncthreads();
-        if (warp == 0 && R->any_appends) {
-            unsigned int v = (lane < SFP_TILE / 32) ? s_warp[lane] : 0u;
+        uint4 agg{0u, 0u, 0u, 0u};
+        bool have_excl = true;
+        if (warp == 0 && any_appends) {
+            constexpr int NW = SFP_TILE / 32;
+            const unsigned int v = (lane < ITEMS * NW) ? s_warp[lane / NW][lane % NW] : 0u;
             unsigned int inc = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -367,95 +536,135 @@ __device__ __forceinline__ void sfp_step_fp64(const sfp_run_dev* __restrict__ R)
                 if (lane >= o) inc += n2;
             }
             const unsigned int total = __shfl_sync(0xffffffffu, inc, 31);
-            if (lane < SFP_TILE / 32) s_warp[lane] = inc - v;
-            const bool appends = S.radiating || S.bw;
-            uint4 ex{0u, 0u, 0u, 0u};
-            if (appends) {
-                ex = lookback(R, tile, first_tile, u4_one(S.channel, total), epoch);
-                if (lane == 0 && total) {
-                    if (S.radiating) atomicAdd(&R->appended[S.photon_dest], (unsigned long long)total);
-                    if (S.bw) {
-                        atomicAdd(&R->appended[S.ele_dest], (unsigned long long)total);
-                        atomicAdd(&R->appended[S.pos_dest], (unsigned long long)total);
-                    }
+            if (lane < ITEMS * NW) s_warp[lane / NW][lane % NW] = inc - v;
+            if (qed_seg) agg = u4_one(S.channel, total);
+            if (lane == 0 && total) {
+                if (S.radiating) atomicAdd(&R->appended[S.photon_dest], (unsigned long long)total);
+                if (S.bw) {
+                    atomicAdd(&R->appended[S.ele_dest], (unsigned long long)total);
+                    atomicAdd(&R->appended[S.pos_dest], (unsigned long long)total);
                 }
+            }
+            uint4 ex{0u, 0u, 0u, 0u};
+            if (tile == first_tile) {
+                publish(R, tile, agg, epoch, true);
             } else {
-                ex = lookback(R, tile, first_tile, uint4{0u, 0u, 0u, 0u}, epoch);
+                publish(R, tile, agg, epoch, false);
+                have_excl = lookback_try(R, tile, first_tile, epoch, ex);
+                if (have_excl) publish(R, tile, u4_add(ex, agg), epoch, true);
             }
             if (lane == 0) s_excl = ex;
         }
-        __syncthreads();
-        const long long off =
-            R->any_appends ? (long long)u4_get(s_excl, S.channel) + s_warp[warp] + wpre : 0ll;
 
-        // --- appends, recoil and pushes -------------------------------------
-        bool converted = false;
-        int n_items = 0;
-        if (ev && S.radiating) {
-            const sfp_segment& D = R->seg[S.photon_dest];
-            const long long slot = R->n_buf_step[S.photon_dest] + off;
-            double cx = x, cy = y, cz = z;
-            const double cux = delta * ux, cuy = delta * uy, cuz = delta * uz;
-            if (D.push) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
-            D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
-            D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
-            if (D.tau) D.tau[slot] = 0.0;
-            D.pruned[slot] = 0;
-            if (S.rr == SFP_RR_PHOTON) {  // cpu.py:76-87
-                const double f = 1.0 - delta;
-                ux = ux * f; uy = uy * f; uz = uz * f;
+        // --- recoil and push of every parent, in registers ------------------
+        bool conv[ITEMS];
+        double sx[ITEMS], sy[ITEMS], sz[ITEMS];
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const long long i = i0 + (long long)k * SFP_TILE;
+            conv[k] = ev[k] && S.bw;  // converted photons are pruned, not pushed (cpu.py:190)
+            sx[k] = sy[k] = sz[k] = 0.0;
+            if (ev[k] && S.radiating && S.rr == SFP_RR_PHOTON) {  // recoil, cpu.py:76-87
+                const double f = 1.0 - delta[k];
+                ux[k] = ux[k] * f; uy[k] = uy[k] * f; uz[k] = uz[k] * f;
             }
-        }
-        if (ev && S.bw) {
-            converted = true;
-            S.pruned[i] = 1;
-            n_items = 2;
-        }
-        const bool parent_massive = alive && !converted && S.push && !S.massless;
-        if (parent_massive) n_items = 1;
-
-        // massive pushes: the parent (e+- species) or the two pair children
-        for (int w = 0; w < 2; ++w) {
-            if (w >= n_items) break;
-            if (parent_massive) {
-                push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            if (!(alive[k] && !conv[k] && S.push)) continue;
+            if (S.massless) {
+                if (FORM == SFP_FORM_FP64) push_photon(x[k], y[k], z[k], ux[k], uy[k], uz[k], dt);
+                else push_photon32(x[k], y[k], z[k], ux[k], uy[k], uz[k], dt);
             } else {
-                const int di = (w == 0) ? S.ele_dest : S.pos_dest;
-                const sfp_segment& D = R->seg[di];
-                const double d = (w == 0) ? delta : 1.0 - delta;  // cpu.py:175-182
-                double cx = x, cy = y, cz = z, cux = d * ux, cuy = d * uy, cuz = d * uz;
-                double csx = 0.0, csy = 0.0, csz = 0.0;
-                if (D.push) push_massive(cx, cy, cz, cux, cuy, cuz, csx, csy, csz, D, P, t, dt);
-                const long long slot = R->n_buf_step[di] + off;
-                D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
-                D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
-                if (D.spin) { D.sx[slot] = csx; D.sy[slot] = csy; D.sz[slot] = csz; }
-                if (D.tau) D.tau[slot] = 0.0;
-                D.pruned[slot] = 0;
+                if (S.spin) { sx[k] = S.sx[i]; sy[k] = S.sy[i]; sz[k] = S.sz[i]; }
+                if (FORM == SFP_FORM_FP64) push_massive(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
+                else push_massive32(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
             }
         }
-        if (alive && !converted && S.push && S.massless) push_photon(x, y, z, ux, uy, uz, dt);
 
-        if (alive && !converted) {
-            if (S.push) { S.x[i] = x; S.y[i] = y; S.z[i] = z; }
-            if (!S.massless && (S.push || (ev && S.rr == SFP_RR_PHOTON))) {
-                S.ux[i] = ux; S.uy[i] = uy; S.uz[i] = uz;
-            }
-            if (S.spin && S.push) { S.sx[i] = sx; S.sy[i] = sy; S.sz[i] = sz; }
+        // --- finish the look-back -------------------------------------------
+        if (warp == 0 && any_appends && !__all_sync(0xffffffffu, have_excl)) {
+            const uint4 ex = lookback_wait(R, tile, first_tile, epoch);
+            publish(R, tile, u4_add(ex, agg), epoch, true);
+            if (lane == 0) s_excl = ex;
         }
-        if (QED == SFP_QED_OPTICAL_DEPTH && alive && S.tau && (S.radiating || S.bw)) S.tau[i] = tau;
+        __syncthreads();
+        const long long ch_base = any_appends ? (long long)u4_get(s_excl, S.channel) : 0ll;
+
+        // --- children, then the parents' state ------------------------------
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const long long i = i0 + (long long)k * SFP_TILE;
+            if (ev[k]) {
+                const long long off = ch_base + s_warp[k][warp] + wpre[k];
+                if (S.radiating) {  // photon at the parent's pre-push position, u = delta * u (cpu.py:89-116)
+                    const sfp_segment& D = R->seg[S.photon_dest];
+                    const long long slot = R->n_buf_step[S.photon_dest] + off;
+                    double cx = S.x[i], cy = S.y[i], cz = S.z[i];
+                    const double cux = delta[k] * S.ux[i], cuy = delta[k] * S.uy[i], cuz = delta[k] * S.uz[i];
+                    if (D.push) {
+                        if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
+                        else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
+                    }
+                    D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
+                    D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
+                    if (D.tau) D.tau[slot] = 0.0;
+                    D.pruned[slot] = 0;
+                } else {  // e- and e+ from the (unpushed) photon (cpu.py:119-189)
+                    for (int w = 0; w < 2; ++w) {
+                        const int di = (w == 0) ? S.ele_dest : S.pos_dest;
+                        const sfp_segment& D = R->seg[di];
+                        const double d = (w == 0) ? delta[k] : 1.0 - delta[k];
+                        double cx = x[k], cy = y[k], cz = z[k], cux = d * ux[k], cuy = d * uy[k], cuz = d * uz[k];
+                        double csx = 0.0, csy = 0.0, csz = 0.0;
+                        if (D.push) {
+                            if (FORM == SFP_FORM_FP64) push_massive(cx, cy, cz, cux, cuy, cuz, csx, csy, csz, D, P, t, dt);
+                            else push_massive32(cx, cy, cz, cux, cuy, cuz, csx, csy, csz, D, P, t, dt);
+                        }
+                        const long long slot = R->n_buf_step[di] + off;
+                        D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
+                        D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
+                        if (D.spin) { D.sx[slot] = csx; D.sy[slot] = csy; D.sz[slot] = csz; }
+                        if (D.tau) D.tau[slot] = 0.0;
+                        D.pruned[slot] = 0;
+                    }
+                    S.pruned[i] = 1;
+                }
+            }
+            if (alive[k] && !conv[k]) {
+                if (S.push) { S.x[i] = x[k]; S.y[i] = y[k]; S.z[i] = z[k]; }
+                if (!S.massless && (S.push || (ev[k] && S.rr == SFP_RR_PHOTON))) {
+                    S.ux[i] = ux[k]; S.uy[i] = uy[k]; S.uz[i] = uz[k];
+                }
+                if (S.spin && S.push && !S.massless) { S.sx[i] = sx[k]; S.sy[i] = sy[k]; S.sz[i] = sz[k]; }
+            }
+            if (QED == SFP_QED_OPTICAL_DEPTH && alive[k] && S.tau && qed_seg) S.tau[i] = tau[k];
+        }
     }
 }
 
+// kernels: <form>_<qed>_i<items per thread>_b<min resident blocks per SM>
+#define SFP_STEP_KERNEL(NAME, FORM, QED, ITEMS, MINB)                                                      \
+    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB) NAME(const sfp_run_dev* __restrict__ R) { \
+        sfp_step_body<FORM, QED, ITEMS>(R);                                                                \
+    }
+
 #if defined(SFP_STEP_FORM_FP64) && defined(SFP_STEP_QED_RS)
-extern "C" __global__ void __launch_bounds__(SFP_TILE) sfp_step_fp64_rs(const sfp_run_dev* __restrict__ R) {
-    sfp_step_fp64<SFP_QED_REJECTION>(R);
-}
+SFP_STEP_KERNEL(sfp_step_fp64_rs_i1_b2, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 2)
+SFP_STEP_KERNEL(sfp_step_fp64_rs_i1_b3, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 3)
+SFP_STEP_KERNEL(sfp_step_fp64_rs_i2_b2, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
 #endif
 #if defined(SFP_STEP_FORM_FP64) && defined(SFP_STEP_QED_OD)
-extern "C" __global__ void __launch_bounds__(SFP_TILE) sfp_step_fp64_od(const sfp_run_dev* __restrict__ R) {
-    sfp_step_fp64<SFP_QED_OPTICAL_DEPTH>(R);
-}
+SFP_STEP_KERNEL(sfp_step_fp64_od_i1_b2, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 2)
+SFP_STEP_KERNEL(sfp_step_fp64_od_i2_b2, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
+#endif
+#if defined(SFP_STEP_FORM_FP32) && defined(SFP_STEP_QED_RS)
+SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b2, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 2)
+SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b3, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 3)
+SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b4, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
+SFP_STEP_KERNEL(sfp_step_fp32_rs_i2_b2, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 2)
+SFP_STEP_KERNEL(sfp_step_fp32_rs_i2_b3, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+#endif
+#if defined(SFP_STEP_FORM_FP32) && defined(SFP_STEP_QED_OD)
+SFP_STEP_KERNEL(sfp_step_fp32_od_i1_b3, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 3)
+SFP_STEP_KERNEL(sfp_step_fp32_od_i2_b2, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 2)
 #endif
 #endif  // SFP_WANT_STEP
 

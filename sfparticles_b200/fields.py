@@ -27,6 +27,8 @@ from .constants import C, E_CHARGE, M_E, PI
 KIND_STATIC, KIND_SIMPLE, KIND_GAUSSIAN, KIND_FOCUSED, KIND_USER = "static", "simple", "gaussian", "focused", "user"
 _DEVICE_FN = {KIND_STATIC: "sfp::field_static", KIND_SIMPLE: "sfp::field_simple",
               KIND_GAUSSIAN: "sfp::field_gaussian", KIND_FOCUSED: "sfp::field_focused"}
+_DEVICE_FN32 = {KIND_STATIC: "sfp32::field_static", KIND_SIMPLE: "sfp32::field_simple",
+                KIND_GAUSSIAN: "sfp32::field_gaussian", KIND_FOCUSED: "sfp32::field_focused"}
 N_PARAMS = 16
 
 
@@ -88,42 +90,55 @@ class Fields:
         return walk(self._tree)
 
     def cuda_source(self) -> str:
-        """CUDA C++ of ``sfp_field_program`` for this structure."""
+        """CUDA C++ of ``sfp_field_program`` (float64) and
+        ``sfp_field_program32`` (float32 result) for this structure."""
         helpers = []
-        lines = []
-        counter = [0, 0]
+        user_fn = {}
 
-        def emit(n) -> str:
-            if isinstance(n, _Term):
-                k = counter[0]
-                counter[0] += 1
+        def program(real: str, fns) -> str:
+            lines = []
+            counter = [0, 0]
+
+            def emit(n) -> str:
+                if isinstance(n, _Term):
+                    k = counter[0]
+                    counter[0] += 1
+                    v = f"T{counter[1]}"
+                    counter[1] += 1
+                    if n.kind == KIND_USER:
+                        if id(n) not in user_fn:
+                            user_fn[id(n)] = f"sfp_user_field_{len(helpers)}"
+                            helpers.append(n.user_code.replace("__SFP_USER_FN__", user_fn[id(n)]))
+                        fname = user_fn[id(n)]
+                        if real == "double":
+                            lines.append(f"    double {v}[6]; {fname}(x, y, z, t, P + {k * N_PARAMS}, {v});")
+                        else:
+                            lines.append(f"    float {v}[6]; {{ double D[6]; {fname}(x, y, z, t, P + {k * N_PARAMS}, D);"
+                                         f" for (int i = 0; i < 6; ++i) {v}[i] = (float)D[i]; }}")
+                    elif n.kind == KIND_STATIC:
+                        lines.append(f"    {real} {v}[6]; {fns[n.kind]}(P + {k * N_PARAMS}, {v});")
+                    else:
+                        lines.append(f"    {real} {v}[6]; {fns[n.kind]}(P + {k * N_PARAMS}, x, y, z, t, {v});")
+                    return v
+                a = emit(n[1])
+                b = emit(n[2])
                 v = f"T{counter[1]}"
                 counter[1] += 1
-                if n.kind == KIND_USER:
-                    fname = f"sfp_user_field_{len(helpers)}"
-                    helpers.append(n.user_code.replace("__SFP_USER_FN__", fname))
-                    lines.append(f"    double {v}[6]; {fname}(x, y, z, t, P + {k * N_PARAMS}, {v});")
-                elif n.kind == KIND_STATIC:
-                    lines.append(f"    double {v}[6]; {_DEVICE_FN[n.kind]}(P + {k * N_PARAMS}, {v});")
-                else:
-                    lines.append(f"    double {v}[6]; {_DEVICE_FN[n.kind]}(P + {k * N_PARAMS}, x, y, z, t, {v});")
+                lines.append(f"    {real} {v}[6];")
+                lines.append(f"    for (int k = 0; k < 6; ++k) {v}[k] = {a}[k] + {b}[k];")
                 return v
-            a = emit(n[1])
-            b = emit(n[2])
-            v = f"T{counter[1]}"
-            counter[1] += 1
-            lines.append(f"    double {v}[6];")
-            lines.append(f"    for (int k = 0; k < 6; ++k) {v}[k] = {a}[k] + {b}[k];")
-            return v
 
-        res = emit(self._tree)
-        body = "\n".join(lines)
-        return ("\n".join(helpers) + "\n"
-                "SFP_DEVICE_INLINE void sfp_field_program(double x, double y, double z, double t,\n"
-                "                                         const double* __restrict__ P, double F[6]) {\n"
-                f"{body}\n"
-                f"    for (int k = 0; k < 6; ++k) F[k] = {res}[k];\n"
-                "}\n")
+            res = emit(self._tree)
+            name = "sfp_field_program" if real == "double" else "sfp_field_program32"
+            return (f"SFP_DEVICE_INLINE void {name}(double x, double y, double z, double t,\n"
+                    f"                                  const double* __restrict__ P, {real} F[6]) {{\n"
+                    + "\n".join(lines) + "\n"
+                    f"    for (int k = 0; k < 6; ++k) F[k] = {res}[k];\n"
+                    "}\n")
+
+        p64 = program("double", _DEVICE_FN)
+        p32 = program("float", _DEVICE_FN32)
+        return "\n".join(helpers) + "\n" + p64 + p32
 
     def params_device(self, device=None):
         """Parameter array on the CUDA device (cached per device)."""

@@ -173,12 +173,39 @@ class Particles(object):
 
     def _materialize(self, name):
         n = self.buffer_size
+        if name == "inv_gamma":  # derived from u (particles.py:118-123)
+            self._arr[name] = self._inv_gamma_from_u()
+            return
         if self._gpu:
             import torch
             dt = torch.uint8 if name in _BOOL_ATTRS else torch.float64
             self._arr[name] = torch.zeros(n, dtype=dt, device=_device())
         else:
             self._arr[name] = np.zeros(n, dtype=bool) if name in _BOOL_ATTRS else np.zeros(n)
+
+    def _inv_gamma_from_u(self):
+        if self._gpu:
+            import torch
+            ig = torch.empty(self.buffer_size, dtype=torch.float64, device=_device())
+            if self.buffer_size:
+                _lib.call("sfp_inv_gamma", ctypes.c_void_p(self._arr["ux"].data_ptr()),
+                          ctypes.c_void_p(self._arr["uy"].data_ptr()), ctypes.c_void_p(self._arr["uz"].data_ptr()),
+                          ctypes.c_void_p(ig.data_ptr()), self.buffer_size, 1 if self.m == 0 else 0, _stream_ptr())
+            return ig
+        ux, uy, uz = self._arr["ux"], self._arr["uy"], self._arr["uz"]
+        with np.errstate(divide="ignore"):
+            if self.m > 0:
+                return 1. / np.sqrt(1 + ux ** 2 + uy ** 2 + uz ** 2)
+            return 1. / np.sqrt(ux ** 2 + uy ** 2 + uz ** 2)
+
+    _SCRATCH = ("inv_gamma", "chi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "event", "photon_delta", "pair_delta")
+
+    def _drop_scratch(self):
+        """Free the per-step scratch arrays and the stored 1/gamma; the fused
+        step keeps neither (1/gamma is recomputed from u on access)."""
+        for k in self._SCRATCH:
+            self._arr.pop(k, None)
+        self._touch()
 
     def _d(self, name):
         """Device tensor of an attribute (species must be on the device)."""
@@ -414,14 +441,18 @@ class Particles(object):
 
     def _resize(self, new: int):
         old = self.buffer_size
+        freed = 0
         for k, v in list(self._arr.items()):
             if self._gpu:
                 import torch
-                t = torch.zeros(new, dtype=v.dtype, device=v.device)
-                t[: min(old, new)] = v[: min(old, new)]
-                if k == "_to_be_pruned" and new > old:
-                    t[old:] = 1
+                t = torch.empty(new, dtype=v.dtype, device=v.device)
+                m = min(old, new)
+                t[:m] = v[:m]
+                if new > old:
+                    t[old:] = 1 if k == "_to_be_pruned" else 0
+                freed += v.numel() * v.element_size()
                 self._arr[k] = t
+                del v
             else:
                 a = np.zeros(new, dtype=v.dtype)
                 a[: min(old, new)] = v[: min(old, new)]
@@ -430,6 +461,10 @@ class Particles(object):
                 self._arr[k] = a
         self.buffer_size = new
         self._touch()
+        if self._gpu and freed > (256 << 20):
+            # outgrown blocks are never reused by this buffer: return them
+            import torch
+            torch.cuda.empty_cache()
 
     def _prune(self) -> None:
         """Remove pruned particles and compact every array (particles.py:503-516)."""
@@ -445,14 +480,6 @@ class Particles(object):
             N = int(keep.sum())
         self.buffer_size = N
         self.N_buffered = N
-        self._touch()
-
-    def _refresh_inv_gamma(self):
-        """Recompute the stored 1/gamma from u after fused steps."""
-        if not self._gpu or self.buffer_size == 0:
-            return
-        _lib.call("sfp_inv_gamma", self._p("ux"), self._p("uy"), self._p("uz"), self._p("inv_gamma"),
-                  self.N_buffered, 1 if self.m == 0 else 0, _stream_ptr())
         self._touch()
 
 

@@ -50,7 +50,7 @@ def _inline(text: str, seen: set) -> str:
 
 def module_source(field_src: str, form, qed) -> str:
     seen = set()
-    head = _inline('#include "sfp_types.h"\n#include "sfp_device.cuh"\n', seen)
+    head = _inline('#include "sfp_types.h"\n#include "sfp_device.cuh"\n#include "sfp_device32.cuh"\n', seen)
     parts = [head, "// ---- field program ----\n", field_src]
     if form is None:
         parts.append("#define SFP_WANT_FIELD_EVAL 1\n")

@@ -20,7 +20,9 @@ and continues.
 Extra keyword arguments (no reference counterpart):
   seed        -- 64-bit key of the Philox streams (default: random);
   form        -- 'fp64' (plain float64, the reference arithmetic) or 'fp32';
-  graph_chunk -- steps per captured CUDA graph (0 disables graphs).
+  graph_chunk -- steps per captured CUDA graph (0 disables graphs);
+  items, min_blocks -- step-kernel variant: particles per thread per tile
+                 and minimum resident blocks per SM (see autotune.py).
 """
 from __future__ import annotations
 
@@ -43,7 +45,8 @@ except Exception:  # pragma: no cover
 
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
-                 photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64) -> None:
+                 photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
+                 items: int = 0, min_blocks: int = 0) -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -60,6 +63,8 @@ class Simulation(object):
             raise ValueError("form must be 'fp64' or 'fp32'")
         self.form = form
         self.graph_chunk = int(graph_chunk)
+        self.items = int(items)  # particles per thread per tile (0: the form's default)
+        self.min_blocks = int(min_blocks)  # kernel variant: resident blocks per SM (0: default)
         self.particle_steps = 0  # sum over executed steps of all species' N_buffered
         self.kernel_launches = 0  # libsfp kernels launched by start()/run_on_device()
         self._run = None
@@ -78,6 +83,9 @@ class Simulation(object):
         if len(ods) > 1:
             raise ValueError("all QED species of a simulation must use the same event method")
         self.qed_method = "od" if ods == {True} else "rs"
+        if self.items <= 0 or self.min_blocks <= 0:
+            from .autotune import DEFAULT
+            self.items, self.min_blocks = DEFAULT[(self.form, self.qed_method)]
 
     # ------------------------------------------------------------------
     def _index(self, p):
@@ -158,6 +166,8 @@ class Simulation(object):
         cfg.step0 = self.step
         cfg.qed = _lib.SFP_QED_OPTICAL_DEPTH if self.qed_method == "od" else _lib.SFP_QED_REJECTION
         cfg.form = _lib.SFP_FORM_FP32 if self.form == "fp32" else _lib.SFP_FORM_FP64
+        cfg.items = self.items
+        cfg.min_blocks = self.min_blocks
         if self.qed_method == "od":
             cfg.od_photon, cfg.od_pair = device_tables.od_tables(dev)
         else:
@@ -186,6 +196,7 @@ class Simulation(object):
         """Move species to the device and create the fused-step run."""
         for p in self.all_particles:
             p._to_gpu()
+            p._drop_scratch()
         self._ensure_headroom()
         mod = program.get_module(self.fields, form=self.form, qed=self.qed_method)
         params = self.fields.params_device(_device())
@@ -212,6 +223,13 @@ class Simulation(object):
         self._run = None
         self._keep = None
 
+    def set_kernel(self, items: int, min_blocks: int):
+        """Switch the step-kernel variant of a device-resident run."""
+        self.items, self.min_blocks = int(items), int(min_blocks)
+        if getattr(self, "_run", None) is not None:
+            self._end()
+            self._begin()
+
     def run_on_device(self, nstep: int):
         """Advance `nstep` steps keeping every species on the device (no
         prune, no host copies); call finish() to end like start()."""
@@ -232,29 +250,28 @@ class Simulation(object):
         stream they run on), with the buffered counts before and after."""
         if getattr(self, "_run", None) is None:
             self._begin()
-        if self._ensure_headroom():
-            self._update_run(self._run)
-        need = self._worst_case_need()
-        for p in self.all_particles:  # room for nstep worst-case steps
-            if need[id(p)]:
-                p._extend(need[id(p)] * nstep)
-        self._update_run(self._run)
         before = [p.N_buffered for p in self.all_particles]
-        ms = (ctypes.c_float * int(nstep))()
-        _lib.check(_lib.load().sfp_run_steps_timed(self._run, nstep, ms, _stream_ptr()), "sfp_run_steps_timed")
+        out = []
+        L = _lib.load()
         st = _lib.RunState()
         nbuf = (ctypes.c_int64 * len(self.all_particles))()
-        _lib.check(_lib.load().sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
-        if st.error or st.halted:
-            raise _lib.SFPError("timed steps did not complete")
-        for i, p in enumerate(self.all_particles):
-            p.N_buffered = int(nbuf[i])
-            p._touch()
-        self.kernel_launches += 2 * int(nstep) + 1
+        for _ in range(int(nstep)):
+            if self._ensure_headroom():
+                self._update_run(self._run)
+            ms = (ctypes.c_float * 1)()
+            _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
+            _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
+            if st.error or st.halted:
+                raise _lib.SFPError("timed step did not complete")
+            for i, p in enumerate(self.all_particles):
+                p.N_buffered = int(nbuf[i])
+                p._touch()
+            self.kernel_launches += 3
+            out.append(float(ms[0]))
         self.particle_steps = self._ps_base + int(st.particle_steps)
         self.step = int(st.step)
         self.t = float(st.t)
-        return list(ms), before, [p.N_buffered for p in self.all_particles]
+        return out, before, [p.N_buffered for p in self.all_particles]
 
     def _loop(self, run, nstep, call_back):
         L = _lib.load()
@@ -283,9 +300,7 @@ class Simulation(object):
             self.particle_steps = self._ps_base + int(st.particle_steps)
             if done > 0:
                 for p in self.all_particles:
-                    p._refresh_inv_gamma()
                     p._touch()
-                self.kernel_launches += len(self.all_particles)
             self.step = int(st.step)
             self.t = float(st.t)
             remaining -= done

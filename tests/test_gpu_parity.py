@@ -10,6 +10,7 @@ event decisions are compared exactly.
 import ctypes
 import json
 import math
+import os
 
 import numpy as np
 import pytest
@@ -308,3 +309,46 @@ def test_repeated_start_continues_the_run():
     for p, q in zip(a, b):
         assert p.N_buffered == q.N_buffered
         np.testing.assert_array_equal(np.stack([p.x, p.ux]), np.stack([q.x, q.ux]))
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_kernel_variants_give_identical_results(form):
+    """Every step-kernel variant (items per thread, register budget) computes
+    the same arithmetic in the same append order: identical results."""
+    cuda_or_skip()
+    import sfparticles_b200 as S
+    from sfparticles_b200.autotune import VARIANTS
+    g = golden("ref_sim_cascade.npz")
+    case = json.loads(str(g["case"]))
+    ref = None
+    for items, minb in VARIANTS[(form, "rs")]:
+        species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
+        sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
+                           photon_threshold=case["thr"], seed=case["seed"], form=form, items=items, min_blocks=minb)
+        sim.start(case["steps"])
+        got = [np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")]) for p in species]
+        if ref is None:
+            ref = got
+        else:
+            for a, b in zip(got, ref):
+                np.testing.assert_array_equal(a, b)
+
+
+def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
+    cuda_or_skip()
+    import sfparticles_b200 as S
+    from sfparticles_b200 import autotune, program
+    monkeypatch.setattr(program, "CACHE", str(tmp_path))
+    g = golden("ref_sim_cascade.npz")
+    case = json.loads(str(g["case"]))
+    species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
+    sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
+                       photon_threshold=case["thr"], seed=case["seed"], form="fp32")
+    sim.run_on_device(100)
+    step, t = sim.step, sim.t
+    best, times = autotune.tune(sim, sample=10_000, steps=2)
+    assert best in autotune.VARIANTS[("fp32", "rs")] and len(times) == len(autotune.VARIANTS[("fp32", "rs")])
+    assert (sim.step, sim.t) == (step, t)  # tuning ran on a copy
+    assert os.path.exists(os.path.join(str(tmp_path), "autotune.json"))
+    sim.run_on_device(10)
+    sim.finish()

@@ -1,0 +1,181 @@
+"""The reference's own tests (tests/test_qed.py, tests/test_pusher.py of
+xsgeng/sfparticles), run on the GPU implementation through the same public
+and private API the reference tests call.  Expected values come from the
+analytic rate integrals (sfparticles_b200.qed.tables restates the
+reference's scipy integrals), with the reference's 3-sigma bounds.
+Population sizes are those of the reference (1e7 electrons, 1e6 photons)."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from gpu_helpers import cuda_or_skip  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def S():
+    cuda_or_skip()
+    import sfparticles_b200
+    return sfparticles_b200
+
+
+def bfield_from_chi(S, chi, ux):
+    from sfparticles_b200.constants import C, E_CHARGE, HBAR, M_E
+    from sfparticles_b200.fields import static_field
+    return static_field(Bz=chi * M_E ** 2 * C ** 2 / E_CHARGE / HBAR / ux)
+
+
+def electrons(S, n, gamma):
+    ux = math.sqrt(gamma ** 2 - 1)
+    return S.Particles('ele', -1, 1, N=n, props=(np.zeros(n), np.zeros(n), np.zeros(n), np.full(n, ux),
+                                                 np.zeros(n), np.zeros(n)),
+                       RR=S.RadiationReactionType.NONE), ux
+
+
+def photons(S, n, gamma):
+    ux = math.sqrt(gamma ** 2 - 1)
+    return S.Particles('pho', 0, 0, N=n, props=(np.zeros(n), np.zeros(n), np.zeros(n), np.full(n, ux),
+                                                np.zeros(n), np.zeros(n))), ux
+
+
+# ---- tests/test_qed.py: TestPhotonNumber -----------------------------------
+
+def test_photon_creation_bookkeeping(S):
+    ele, ux = electrons(S, 10_000_000, 10000)
+    pho = S.Particles('pho', 0, 0)
+    ele.set_photon(pho)
+    ele._eval_field(bfield_from_chi(S, 1, ux), 0)
+    ele._calculate_chi()
+    ele._photon_event(1e-17)
+    ele._create_photon(pho)
+    ele._photon_event(1e-17)
+    ele._create_photon(pho)
+    assert pho.N_buffered == pho.Npart > 0
+
+
+def test_hard_photon(S):
+    ele, ux = electrons(S, 10_000_000, 10000)
+    pho = S.Particles('pho', 0, 0)
+    ele.set_photon(pho)
+    ele._eval_field(bfield_from_chi(S, 1, ux), 0)
+    ele._calculate_chi()
+    ele._photon_event(1e-17)
+    ele._pick_hard_photon(2.0)
+    ele._create_photon(pho)
+    assert pho.N_buffered > 0 and (pho.gamma > 2.0).all()
+
+
+def test_photon_number(S):
+    from sfparticles_b200.qed import tables
+    gamma = 10000
+    N = 10_000_000
+    ele, ux = electrons(S, N, gamma)
+    for chi_e in [0.1, 0.5, 1.0, 2.0, 5.0]:
+        interval = 1e-17 / chi_e
+        tau = interval / gamma
+        pho = S.Particles('pho', 0, 0)
+        ele.set_photon(pho)
+        ele._eval_field(bfield_from_chi(S, chi_e, ux), 0)
+        ele._calculate_chi()
+        ele._photon_event(interval)
+        ele._create_photon(pho)
+        n_photon = pho.Npart
+        p_tot = tables.photon_rate_total(chi_e) * tau
+        expected = p_tot * N
+        tol = 3 * math.sqrt(expected * (1 - p_tot))
+        assert abs(n_photon - expected) < tol, (chi_e, n_photon, expected)
+        for delta in [0.01, 0.1]:
+            n_bin = np.histogram(pho.ux / gamma, bins=[delta, delta * 1.1])[0][0]
+            p_bin = (tables.photon_rate_delta(chi_e, delta) + tables.photon_rate_delta(chi_e, delta * 1.1)) \
+                * (delta * 0.1) / 2 * tau
+            exp_bin = p_bin * N
+            assert abs(n_bin - exp_bin) < 3 * math.sqrt(exp_bin * (1 - p_bin)), (chi_e, delta, n_bin, exp_bin)
+
+
+# ---- tests/test_qed.py: TestPairNumber -------------------------------------
+
+def _pair_setup(S):
+    pho, ux = photons(S, 1_000_000, 10000)
+    ele = S.Particles('ele', -1, 1)
+    pos = S.Particles('pos', 1, 1)
+    pho.set_pair(ele, pos)
+    return pho, ele, pos, ux
+
+
+def test_pair_creation_bookkeeping(S):
+    pho, ele, pos, ux = _pair_setup(S)
+    pho._eval_field(bfield_from_chi(S, 1, ux), 0)
+    pho._calculate_chi()
+    pho._pair_event(1e-17)
+    pho._create_pair(ele, pos)
+    pho._pair_event(1e-17)
+    pho._create_pair(ele, pos)
+    assert pos.N_buffered == pos.Npart
+    assert ele.N_buffered == ele.Npart
+    assert pos.N_buffered == ele.Npart
+    assert 1_000_000 - pho.Npart == pos.Npart > 0
+
+
+def test_pair_momentum_conservation(S):
+    pho, ele, pos, ux = _pair_setup(S)
+    pho._eval_field(bfield_from_chi(S, 1, ux), 0)
+    pho._calculate_chi()
+    pho._pair_event(1e-17)
+    ev = pho.event
+    ux_pho, uy_pho, uz_pho = pho.ux[ev], pho.uy[ev], pho.uz[ev]
+    pho._create_pair(ele, pos)
+    assert ev.sum() > 0
+    assert (abs(ele.ux + pos.ux - ux_pho) < 1e-10).all()
+    assert (abs(ele.uy + pos.uy - uy_pho) < 1e-10).all()
+    assert (abs(ele.uz + pos.uz - uz_pho) < 1e-10).all()
+
+
+def test_pair_number(S):
+    from sfparticles_b200.qed import tables
+    gamma = 10000
+    interval = 1e-17
+    tau = interval / gamma
+    for chi_g in [1.0, 2.0, 5.0]:
+        pho, ele, pos, ux = _pair_setup(S)
+        pho._eval_field(bfield_from_chi(S, chi_g, ux), 0)
+        pho._calculate_chi()
+        pho._pair_event(interval)
+        pho._create_pair(ele, pos)
+        n_pair = pos.Npart
+        p_tot = tables.pair_rate_total(chi_g) * tau
+        expected = p_tot * 1_000_000
+        assert abs(n_pair - expected) < 3 * math.sqrt(expected * (1 - p_tot)), (chi_g, n_pair, expected)
+
+
+# ---- tests/test_pusher.py ---------------------------------------------------
+
+def test_boris_gyration_conserves_momentum(S):
+    import ctypes
+    from sfparticles_b200 import _lib
+    from sfparticles_b200.constants import C, E_CHARGE, M_E, PI
+    r = 1e-6
+    ux0, uz0 = 100, 10
+    u0 = math.sqrt(ux0 ** 2 + uz0 ** 2)
+    v = ux0 / math.sqrt(1 + ux0 ** 2) * C
+    T = 2 * PI * r / v
+    bz = M_E * C / E_CHARGE * ux0 / r
+    p = S.Particles('e', -1, 1, N=1, props=[0.0, 0.0, 0.0, float(ux0), 0.0, float(uz0)])
+    p.Bz = np.array([bz])
+    for _ in range(20):
+        p._push_momentum(T / 20)
+    assert abs(math.sqrt(p.ux[0] ** 2 + p.uy[0] ** 2 + p.uz[0] ** 2) - u0) / u0 < 1e-10
+
+
+def test_LL_ten_percent_loss(S):
+    ux0 = 1000.0
+    p = S.Particles('e', -1, 1, N=1, props=[0.0, 0.0, 0.0, ux0, 0.0, 0.0], RR=S.RadiationReactionType.LL)
+    p.chi = np.array([1.0])
+    from sfparticles_b200 import _lib
+    from sfparticles_b200.particles import _stream_ptr
+    _lib.call("sfp_LL_push", p._p("ux"), p._p("uy"), p._p("uz"), p._p("inv_gamma"), p._p("chi"), 1,
+              p._p("_to_be_pruned"), 2.67e-17, _stream_ptr())
+    p._touch()
+    assert p.ux[0] < ux0
+    assert round((ux0 - p.ux[0]) / ux0, 2) == 0.1

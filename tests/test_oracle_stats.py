@@ -1,0 +1,146 @@
+"""Pin the oracle's optical-depth pieces and its Monte-Carlo statistics
+against the reference.
+
+* the optical-depth table generator of sfparticles_b200.qed.tables vs rows
+  produced by the reference's own generators (qed/optical_depth_tables.py);
+* the oracle's rate interpolation and inverse-CDF sampler vs the reference's
+  _linear_interp1d / _bisect_interp bodies fed the same uniform draws;
+* Monte-Carlo observables of the oracle (keyed Philox draws) vs un-injected
+  reference runs (Numba's own generator): photon numbers, spectra and mean
+  energy agree within 3 standard deviations of the combined spread.
+"""
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import GOLDEN, golden
+
+
+def test_od_table_generator_matches_reference_rows():
+    from sfparticles_b200.qed import tables
+    g = golden("ref_od.npz")
+    rows = [0, 5, 11, 17]  # a subset of the fixture's rows keeps this test short
+    for k in rows:
+        chi = float(g["chi_rows"][k])
+        np.testing.assert_allclose(tables.photon_rate_total(chi), g["photon_total"][k], rtol=1e-12)
+        np.testing.assert_allclose(tables.pair_rate_total(chi), g["pair_total"][k], rtol=1e-12, atol=1e-300)
+    k = 9
+    chi = float(g["chi_rows"][k])
+    np.testing.assert_allclose(tables.photon_cumulative(chi), g["photon_cum"][k], rtol=1e-12)
+    np.testing.assert_allclose(tables.pair_cumulative(chi), g["pair_cum"][k], rtol=1e-12, atol=1e-300)
+
+
+def test_product_od_table_contains_reference_grid():
+    """The shipped table's first 256 rows are the reference grid log10 chi in [-3, 2]."""
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    g = golden("ref_od.npz")
+    chi = d["chi"]
+    assert chi.size == 307 and abs(math.log10(chi[-1]) - 3.0) < 1e-9
+    np.testing.assert_array_equal(chi[g["rows"]], g["chi_rows"])
+    np.testing.assert_allclose(d["photon_rate_total"][g["rows"]], g["photon_total"], rtol=1e-12)
+    np.testing.assert_allclose(d["photon_cumulative"][g["rows"]], g["photon_cum"], rtol=1e-12)
+
+
+def test_oracle_od_sampling_matches_reference_with_same_draws():
+    g = golden("ref_od.npz")
+    tab = orc.make_od_table(g["photon_total"], g["photon_cum"], float(g["sub_log_chi_min"]),
+                            float(g["sub_log_chi_delta"]), float(g["log_delta_min"]), float(g["log_delta_delta"]))
+    L = orc.lib()
+    interp = np.array([L.orc_od_interp1d(c, ctypes.byref(tab)) for c in g["q_chi"]])
+    np.testing.assert_allclose(interp, g["q_interp"], rtol=1e-14)
+    bis = np.array([L.orc_od_bisect(c, r, ctypes.byref(tab)) for c, r in zip(g["q_chi"], g["q_r"])])
+    np.testing.assert_allclose(bis, g["q_bisect"], rtol=1e-13)
+
+
+def _stats():
+    with open(os.path.join(GOLDEN, "ref_stats.json")) as f:
+        return json.load(f)
+
+
+def static_field_photons(n, chi_e, seed, gamma=10000):
+    """tests/test_qed.py:18-34 setup on the oracle: n electrons at gamma in a
+    static B_z giving chi_e; one step of dt = 1e-17 / chi_e."""
+    from sfparticles_b200.qed import tables
+    ux = math.sqrt(gamma ** 2 - 1)
+    props = [np.zeros(n), np.zeros(n), np.zeros(n), np.full(n, ux), np.zeros(n), np.zeros(n)]
+    ele = orc.Species("ele", -1, 1, N=n, props=props, RR=orc.RR_NONE)
+    pho = orc.Species("pho", 0, 0)
+    ele.set_photon(pho)
+    Bz = chi_e * orc.M_E ** 2 * orc.C ** 2 / orc.E_CHARGE / orc.HBAR / ux
+    terms = orc.static_field(Bz=Bz)
+    iA, dA, _, _ = tables.rs_tables()
+    sim = orc.OracleSim([ele, pho], 1e-17 / chi_e, terms, ("rs", iA, dA), seed=seed, photon_threshold=0.0)
+    ele.eval_field(terms, 0.0)
+    ele.calc_chi()
+    sim._events(ele, photon=True)
+    sim._create_photon(ele)
+    pho.prune()
+    return pho.N_buffered, np.histogram(pho.ux / gamma, bins=[0.01, 0.011])[0][0], \
+        np.histogram(pho.ux / gamma, bins=[0.1, 0.11])[0][0]
+
+
+@pytest.mark.parametrize("chi_e", ["0.5", "2.0"])
+def test_oracle_photon_statistics_match_reference(chi_e):
+    s = _stats()["static_photon"]
+    ref = np.array(s["counts"][chi_e], dtype=float)  # reps x (count, bin 0.01, bin 0.1)
+    got = np.array([static_field_photons(s["N"], float(chi_e), seed) for seed in range(3)], dtype=float)
+    for j in range(3):
+        m_ref, m_got = ref[:, j].mean(), got[:, j].mean()
+        # Poisson spread of each mean
+        sigma = math.sqrt(m_ref / len(ref) + m_got / len(got))
+        assert abs(m_got - m_ref) < 3 * sigma + 1e-9, (chi_e, j, m_got, m_ref, sigma)
+
+
+def c1_small_oracle(seed, spec):
+    from sfparticles_b200.qed import tables
+    rng = np.random.default_rng(seed)
+    n = spec["n"]
+    L = spec["L"]
+    g = 2000 * (1 + 0.01 * rng.normal(size=n))
+    props = [rng.normal(-L, 5e-6, n), rng.normal(0, 1e-6, n), rng.normal(0, 1e-6, n), np.sqrt(g ** 2 - 1),
+             np.zeros(n), np.zeros(n)]
+    ele = orc.Species("ele", -1, 1, N=n, props=props)
+    pho = orc.Species("pho", 0, 0)
+    pos = orc.Species("pos", 1, 1)
+    ele.set_photon(pho)
+    pos.set_photon(pho)
+    pho.set_pair(ele, pos)
+    terms = orc.gaussian_laser_pulse(spec["a0"], 3e-6, spec["ctau"], direction=-1, x0=L)
+    iA, dA, _, _ = tables.rs_tables()
+    T0 = 0.8e-6 / orc.C
+    sim = orc.OracleSim([ele, pos, pho], T0 / 50, terms, ("rs", iA, dA), seed=seed)
+    sim.run(spec["steps"])
+    for p in (ele, pos, pho):
+        p.prune()
+    eph = 1.0 / pho.inv_gamma
+    hist = np.histogram(np.log10(eph), bins=spec["bins"], range=tuple(spec["hist_range"]))[0]
+    return dict(n_photon=pho.N_buffered, n_pos=pos.N_buffered, mean_gamma_e=float(np.mean(1 / ele.inv_gamma)),
+                hist=hist)
+
+
+def test_oracle_c1_cascade_statistics_match_reference():
+    """1000 electrons of the config-1 beam against the a0=50 pulse, 1500
+    steps: photon number, photon spectrum (16 log bins) and mean electron
+    energy of the oracle vs the reference's own runs."""
+    spec = _stats()["c1_small"]
+    ref = spec["runs"]
+    got = [c1_small_oracle(100 + s, spec) for s in range(4)]
+    for key in ("n_photon", "mean_gamma_e"):
+        r = np.array([x[key] for x in ref], dtype=float)
+        o = np.array([x[key] for x in got], dtype=float)
+        sigma = math.sqrt(r.var(ddof=1) / r.size + o.var(ddof=1) / o.size)
+        assert abs(r.mean() - o.mean()) < 3 * sigma, (key, r.mean(), o.mean(), sigma)
+    rh = np.array([x["hist"] for x in ref], dtype=float)
+    oh = np.array([x["hist"] for x in got], dtype=float)
+    sigma = np.sqrt(rh.var(0, ddof=1) / len(rh) + oh.var(0, ddof=1) / len(oh) + 1.0)
+    z = np.abs(rh.mean(0) - oh.mean(0)) / sigma
+    assert (z < 3.5).all(), z
+    # spectrum-level agreement: relative L1 of the mean spectra
+    l1 = np.abs(rh.mean(0) - oh.mean(0)).sum() / rh.mean(0).sum()
+    assert l1 < 0.03, l1
