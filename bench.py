@@ -38,10 +38,12 @@ W0 = 3e-6
 GAMMA0 = 2000.0
 STEPS_FULL = 3000
 DT = T0 / 100
-# algorithmic bytes per particle-step (float64 state read once + written once)
-BYTES_EPM = 97   # x,y,z,ux,uy,uz read+write + alive flag
-BYTES_PHOTON = 73  # x,y,z,ux,uy,uz read + alive flag + position write
-BYTES_APPEND = 49  # appended particle: state + flag written
+# algorithmic bytes per unit of work (float64 state in HBM, each byte moved once)
+BYTES_EPM = 97      # pushed e+-: x,y,z,ux,uy,uz read + written (96) + alive flag read
+BYTES_PHOTON = 73   # pushed photon: x,y,z,ux,uy,uz read (48) + flag (1) + x,y,z written (24)
+BYTES_DEAD = 1      # pruned slot: flag read
+BYTES_APPEND = 49   # appended particle: x,y,z,ux,uy,uz + flag written
+BYTES_CHILD = 96    # pair child pushed by the children kernel: x,y,z,ux,uy,uz read + written
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
@@ -57,7 +59,7 @@ def beam(n, seed, steps=STEPS_FULL):
     return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
 
 
-def make_sim(n, seed, form="fp64", items=0, min_blocks=0):
+def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64):
     import sfparticles_b200 as S
     from sfparticles_b200.fields import gaussian_laser_pulse
     props, L = beam(n, seed)
@@ -68,8 +70,9 @@ def make_sim(n, seed, form="fp64", items=0, min_blocks=0):
     pos.set_photon(pho)
     pho.set_pair(ele, pos)
     fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
-    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form, items=items,
-                       min_blocks=min_blocks)
+    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form,
+                       items=massive[0], min_blocks=massive[1], p_unroll=photon[0], p_min_blocks=photon[1],
+                       graph_chunk=graph_chunk)
     return sim
 
 
@@ -177,7 +180,8 @@ def run_ours(args, rank, world):
     wsim.run_on_device(args.warmup)
     wsim.finish()
     del wsim
-    sim = make_sim(args.electrons, seed, args.form, args.items, args.min_blocks)
+    sim = make_sim(args.electrons, seed, args.form, (args.items, args.min_blocks), (args.p_unroll, args.p_min_blocks),
+                   graph_chunk=0 if args.no_graphs else 64)
     sim._begin()
     torch.cuda.synchronize()
     if world > 1:
@@ -194,19 +198,39 @@ def run_ours(args, rank, world):
     launches = sim.kernel_launches - launches0
     ps = sim.particle_steps
     counts = {p.name: p.N_buffered for p in sim.all_particles}
-    # roofline of the step kernel at the final state: CUDA events around each launch
+    # roofline of each step kernel at the final state: CUDA events around every launch
     from sfparticles_b200 import autotune
-    variant_ms = {}
+    tm, tp = {}, {}
     if not args.no_variants:
-        variant_ms = autotune.measure(sim, steps=2)
-        sim.set_kernel(*min(variant_ms, key=variant_ms.get))
+        tm, tp = autotune.measure(sim, steps=2)
+        sim.set_kernel(massive=min(tm, key=tm.get), photon=min(tp, key=tp.get))
     alive = {p.name: p.Npart for p in sim.all_particles}
+    buffered = {p.name: p.N_buffered for p in sim.all_particles}
     kms, before, after = sim.time_step_kernel(args.roofline_steps)
-    k_avg_ms = float(np.mean(kms))
-    appended = (sum(after) - sum(before)) / args.roofline_steps
-    alg_bytes = ((alive["electron"] + alive["positron"]) * BYTES_EPM + alive["photon"] * BYTES_PHOTON
-                 + appended * BYTES_APPEND)
-    sim_items, sim_minb = sim.items, sim.min_blocks
+    k_ms = [float(np.mean([k[j] for k in kms])) for j in range(3)]
+    n_ph_app = (after[2] - before[2]) / args.roofline_steps  # photons appended per step
+    n_pairs = (after[1] - before[1]) / args.roofline_steps    # pairs per step
+    n_epm = alive["electron"] + alive["positron"]
+    dead_m = buffered["electron"] + buffered["positron"] - n_epm
+    alg = {
+        "massive": n_epm * BYTES_EPM + dead_m * BYTES_DEAD + n_ph_app * BYTES_APPEND,
+        "photon": alive["photon"] * BYTES_PHOTON + (buffered["photon"] - alive["photon"]) * BYTES_DEAD
+        + 2 * n_pairs * BYTES_APPEND,
+        "children": 2 * n_pairs * BYTES_CHILD,
+    }
+    names = {
+        "massive": f"sfp_massive_{args.form}_rs_i{sim.items}_b{sim.min_blocks}",
+        "photon": f"sfp_photon_{args.form}_rs_u{sim.p_unroll}_b{sim.p_min_blocks}",
+        "children": f"sfp_children_{args.form}",
+    }
+    per_kernel = {}
+    for j, k in enumerate(("massive", "photon", "children")):
+        gbs = alg[k] / (k_ms[j] * 1e-3) / 1e9 if k_ms[j] > 0 else 0.0
+        per_kernel[k] = {"kernel": names[k], "avg_ms": k_ms[j], "alg_bytes_per_launch": alg[k],
+                         "achieved_gbs": gbs}
+    dominant = max(per_kernel, key=lambda k: per_kernel[k]["avg_ms"])
+    step_units = {"electrons+positrons_alive": n_epm, "photons_alive": alive["photon"],
+                  "photons_appended_per_step": n_ph_app, "pairs_per_step": n_pairs}
     sim.finish()
     del sim
     torch.cuda.empty_cache()
@@ -273,14 +297,17 @@ def run_ours(args, rank, world):
         torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
         tot_ps = float(w.item())
     peak, peak_kind = measured_peak_hbm()
-    achieved = alg_bytes / (k_avg_ms * 1e-3) / 1e9
+    dk = per_kernel[dominant]
+    for v in per_kernel.values():
+        v["frac"] = v["achieved_gbs"] / peak
     return dict(ms=ms, particle_steps=tot_ps, counts=counts, launches=launches, clocks=clk.summary(),
-                roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                          "kernel": f"sfp_step_{args.form}_rs_i{sim_items}_b{sim_minb}",
-                          "variants_ms": {f"i{a}_b{b}": v for (a, b), v in variant_ms.items()},
-                          "kernel_avg_ms": k_avg_ms,
-                          "alg_bytes_per_launch": alg_bytes, "launches_timed": args.roofline_steps},
+                roofline={"bound": "hbm", "achieved": dk["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                          "frac": dk["achieved_gbs"] / peak, "traffic": None, "peak_kind": peak_kind,
+                          "kernel": dk["kernel"], "kernel_avg_ms": dk["avg_ms"],
+                          "alg_bytes_per_launch": dk["alg_bytes_per_launch"], "launches_timed": args.roofline_steps,
+                          "units_at_final_state": step_units, "per_kernel": per_kernel,
+                          "variants_ms": {**{f"massive_i{a}_b{b}": v for (a, b), v in tm.items()},
+                                          **{f"photon_u{a}_b{b}": v for (a, b), v in tp.items()}}},
                 e2e=e2e, compare=compare)
 
 
@@ -297,6 +324,9 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--items", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0)
+    ap.add_argument("--p-unroll", type=int, default=0)
+    ap.add_argument("--p-min-blocks", type=int, default=0)
+    ap.add_argument("--no-graphs", action="store_true", help="one eager launch per kernel (for profilers)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--roofline-steps", type=int, default=8)

@@ -138,8 +138,10 @@ typedef struct sfp_run_config {
     int64_t step0;           /* steps already taken (Philox step key)     */
     int32_t qed;             /* SFP_QED_*                                  */
     int32_t form;            /* SFP_FORM_*                                 */
-    int32_t items;           /* particles per thread per tile (0 = default)              */
-    int32_t min_blocks;      /* kernel variant: min resident blocks per SM (0 = default) */
+    int32_t items;           /* massive kernel: particles per thread per tile (0 = default) */
+    int32_t min_blocks;      /* massive kernel: min resident blocks per SM (0 = default)    */
+    int32_t p_unroll;        /* photon kernel: sub-tiles in flight per thread (0 = default) */
+    int32_t p_min_blocks;    /* photon kernel: min resident blocks per SM (0 = default)     */
     sfp_rs_table rs;
     sfp_od_table od_photon;
     sfp_od_table od_pair;
@@ -153,9 +155,11 @@ int sfp_run_update(sfp_run *r, int n_seg, const sfp_segment *seg, const int64_t 
  * lacks the worst-case headroom); graph_chunk > 0 replays CUDA graphs of
  * that many steps.  Asynchronous on `stream`. */
 int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
-/* like sfp_run_steps without graphs, with CUDA events recorded around every
- * step-kernel launch on the run's stream; synchronous.  kernel_ms[i] is the
- * duration of launch i (n_steps entries). */
+/* like sfp_run_steps without graphs, with CUDA events recorded around each
+ * of the three kernels of every step on the run's stream; synchronous.
+ * kernel_ms[3*i + k] is the duration of step i's massive (k=0), photon (k=1)
+ * and pair-children (k=2) kernel; 0 for a kernel the run does not launch
+ * (3*nsteps entries). */
 int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stream);
 /* synchronous: state and per-segment buffered counts (n_seg entries) */
 int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);

@@ -57,7 +57,8 @@ class RunState(ctypes.Structure):
 
 class RunConfig(ctypes.Structure):
     _fields_ = [("dt", c_d), ("photon_threshold", c_d), ("t0", c_d), ("step0", c_i64), ("qed", c_i32), ("form", c_i32),
-                ("items", c_i32), ("min_blocks", c_i32), ("rs", RSTable), ("od_photon", ODTable),
+                ("items", c_i32), ("min_blocks", c_i32), ("p_unroll", c_i32), ("p_min_blocks", c_i32),
+                ("rs", RSTable), ("od_photon", ODTable),
                 ("od_pair", ODTable)]
 
 

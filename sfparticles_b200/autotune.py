@@ -1,16 +1,23 @@
-"""Autotuner of the fused step kernel.
+"""Autotuner of the step kernels.
 
-Every NVRTC step module holds several variants of the step kernel, named
-``sfp_step_<form>_<qed>_i<items>_b<blocks>``: ``items`` particles per thread
-per tile (a tile is 256 * items particles) and a register budget that keeps
-at least ``blocks`` blocks of 256 threads resident per SM.  Which variant is
-fastest depends on the particle mix (pushed e+- vs photons), the field
-program and the form, so ``tune`` measures them: it builds a sample of the
-simulation's current state (up to ``sample`` particles per species, copied,
-so the user's run is not advanced), times a few steps of each variant with
-CUDA events on the launching stream, and selects the fastest.  Results are
-cached per (GPU, form, QED method, field structure, population bucket) in
-``autotune.json`` beside the NVRTC module cache.
+Every NVRTC step module holds several variants of the two persistent step
+kernels:
+
+* ``sfp_massive_<form>_<qed>_i<items>_b<blocks>`` -- e+- tiles of
+  256 * ``items`` particles (``items`` particles per thread);
+* ``sfp_photon_<form>_<qed>_u<unroll>_b<blocks>`` -- photon tiles of
+  8 * 256 photons streamed ``unroll`` sub-tiles at a time per thread;
+
+``blocks`` is the register budget: at least that many blocks of 256 threads
+stay resident per SM.  Which variant is fastest depends on the particle mix,
+the field program and the form, so ``tune`` measures them: it builds a sample
+of the simulation's current state (up to ``sample`` particles per species,
+copied, so the user's run is not advanced), times a few steps of each
+variant with CUDA events on the launching stream, and selects the fastest
+of each kernel (the two kernels run one after the other and touch disjoint
+memory, so they are tuned independently).  Results are cached per (GPU,
+form, QED method, field structure, population bucket) in ``autotune.json``
+beside the NVRTC module cache.
 """
 from __future__ import annotations
 
@@ -23,13 +30,20 @@ import numpy as np
 
 from . import program
 
+# (massive variants (items, blocks), photon variants (unroll, blocks)); the
+# NVRTC step module compiles exactly these
 VARIANTS = {
-    ("fp64", "rs"): [(1, 2), (1, 3), (2, 2)],
-    ("fp64", "od"): [(1, 2), (2, 2)],
-    ("fp32", "rs"): [(1, 2), (1, 3), (1, 4), (2, 2), (2, 3)],
-    ("fp32", "od"): [(1, 3), (2, 2)],
+    ("fp64", "rs"): ([(1, 2), (2, 2)], [(1, 3), (2, 2)]),
+    ("fp64", "od"): ([(1, 2), (2, 2)], [(1, 3), (2, 2)]),
+    ("fp32", "rs"): ([(1, 3), (1, 4), (2, 2), (2, 3)], [(1, 4), (2, 4), (2, 3), (4, 3)]),
+    ("fp32", "od"): ([(1, 3), (2, 2)], [(1, 4), (2, 3)]),
 }
-DEFAULT = {("fp64", "rs"): (1, 2), ("fp64", "od"): (1, 2), ("fp32", "rs"): (1, 3), ("fp32", "od"): (1, 3)}
+DEFAULT = {
+    ("fp64", "rs"): ((1, 2), (1, 3)),
+    ("fp64", "od"): ((1, 2), (1, 3)),
+    ("fp32", "rs"): ((2, 3), (1, 4)),
+    ("fp32", "od"): ((1, 3), (1, 4)),
+}
 
 _lock = threading.Lock()
 
@@ -98,36 +112,47 @@ def _sample_sim(sim, sample):
 
 
 def measure(sim, variants=None, steps: int = 3):
-    """Median step-kernel time [ms] of each variant on `sim`'s current state.
-    Advances `sim` by len(variants) * steps steps."""
-    variants = variants or VARIANTS[(sim.form, sim.qed_method)]
-    out = {}
-    for items, minb in variants:
-        sim.set_kernel(items, minb)
+    """Median kernel times [ms] on `sim`'s current state: ({massive variant:
+    ms}, {photon variant: ms}).  Advances `sim` by
+    (len(massive) + len(photon)) * steps steps."""
+    mv, pv = variants or VARIANTS[(sim.form, sim.qed_method)]
+    tm, tp = {}, {}
+    m0, p0 = (sim.items, sim.min_blocks), (sim.p_unroll, sim.p_min_blocks)
+    for v in mv:
+        sim.set_kernel(massive=v, photon=p0)
         ms, _, _ = sim.time_step_kernel(steps)
-        out[(items, minb)] = float(np.median(ms))
-    return out
+        tm[tuple(v)] = float(np.median([m[0] for m in ms]))
+    for v in pv:
+        sim.set_kernel(massive=m0, photon=v)
+        ms, _, _ = sim.time_step_kernel(steps)
+        tp[tuple(v)] = float(np.median([m[1] for m in ms]))
+    return tm, tp
 
 
 def tune(sim, sample: int = 2_000_000, steps: int = 3, use_cache: bool = True):
-    """Select the fastest step-kernel variant for `sim` (see module doc)."""
+    """Select the fastest massive- and photon-kernel variants for `sim` (see
+    the module doc).  Returns ((massive, photon), times), times a dict
+    'm<items>_b<blocks>' / 'p<unroll>_b<blocks>' -> ms."""
     key = cache_key(sim)
     with _lock:
         cache = _load() if use_cache else {}
-        if key in cache:
-            items, minb = cache[key]["best"]
-            sim.set_kernel(items, minb)
-            return (items, minb), cache[key].get("ms", {})
+        if key in cache and "best" in cache[key] and len(cache[key]["best"]) == 2:
+            m, p = (tuple(v) for v in cache[key]["best"])
+            sim.set_kernel(massive=m, photon=p)
+            return (m, p), cache[key].get("ms", {})
     s = _sample_sim(sim, sample)
     try:
-        times = measure(s, steps=steps)
+        tm, tp = measure(s, steps=steps)
     finally:
         s.finish()
-    best = min(times, key=times.get)
-    sim.set_kernel(*best)
+    # a kernel with no work (0 ms everywhere) keeps the default
+    m = min(tm, key=tm.get) if any(tm.values()) else (sim.items, sim.min_blocks)
+    p = min(tp, key=tp.get) if any(tp.values()) else (sim.p_unroll, sim.p_min_blocks)
+    sim.set_kernel(massive=m, photon=p)
+    times = {**{f"m{a}_b{b}": v for (a, b), v in tm.items()}, **{f"p{a}_b{b}": v for (a, b), v in tp.items()}}
     if use_cache:
         with _lock:
             cache = _load()
-            cache[key] = {"best": list(best), "ms": {f"i{a}_b{b}": v for (a, b), v in times.items()}}
+            cache[key] = {"best": [list(m), list(p)], "ms": times}
             _store(cache)
-    return best, times
+    return (m, p), times

@@ -3,7 +3,8 @@
 //   * per-op kernels that replace the reference's Numba kernels one for one
 //     (the plugin boundary, sfparticles/particles.py:14-25);
 //   * NVRTC compilation / loading of field-specialised step modules;
-//   * fused-step runs: device bookkeeping, persistent launches, CUDA graphs.
+//   * step runs: device bookkeeping, persistent launches of the massive /
+//     photon / pair-children kernels, CUDA graphs.
 //
 // Device memory of particle buffers belongs to the caller; a run allocates
 // only its own bookkeeping (segment tables, tile look-back flags, counters).
@@ -637,11 +638,18 @@ int sfp_inv_gamma(const double* ux, const double* uy, const double* uz, double* 
 }  // extern "C"
 
 // ================================ runs =======================================
+//
+// One step = book(prepare) + massive + photon + children launches on the
+// run's stream.  The massive and photon kernels are persistent grids that
+// take tiles by ticket; the children kernel is a grid-stride push.
+
+// photon-group tile: SFP_PHOTON_SUB_HOST sub-tiles of SFP_TILE_HOST photons
+#define SFP_PHOTON_SUB_HOST 8
 
 struct sfp_run {
     sfp_module* mod = nullptr;
-    cudaKernel_t k_step = nullptr, k_book = nullptr;
-    int grid = 0;
+    cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_children = nullptr, k_book = nullptr;
+    int grid_m = 0, grid_p = 0, grid_c = 0;
     size_t smem = 0;
     cudaStream_t s = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -650,12 +658,15 @@ struct sfp_run {
     sfp_run_dev* d = nullptr;
     std::map<int, cudaGraphExec_t> graphs;
     std::vector<sfp_segment> segs;
+    std::vector<int> mseg, pseg, cseg;
 };
 
-static long long tiles_for(const std::vector<sfp_segment>& segs, int tile) {
+// look-back flags needed: tiles of both groups at full capacity, plus slack
+static long long tiles_for(const sfp_run* r) {
     long long t = 0;
-    for (auto& s : segs) t += (s.capacity + tile - 1) / tile;
-    return t + (long long)segs.size() + 1;
+    for (int s : r->mseg) t += (r->segs[s].capacity + r->h.mtile - 1) / r->h.mtile;
+    for (int s : r->pseg) t += (r->segs[s].capacity + r->h.ptile - 1) / r->h.ptile;
+    return t + (long long)r->segs.size() + 1;
 }
 
 static int run_alloc_tiles(sfp_run* r, long long need) {
@@ -693,6 +704,9 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
         if (S.capacity > 0 && S.spin && (!S.sx || !S.sy || !S.sz))
             return fail(SFP_EINVAL, "spin segment without spin arrays");
         if (S.channel < 0 || S.channel >= SFP_MAX_CHANNELS) return fail(SFP_EINVAL, "append channel out of range");
+        // the massive kernel handles emission, the photon kernel pair creation
+        if (S.massless && S.radiating) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": a photon cannot radiate");
+        if (!S.massless && S.bw) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": only photons create pairs");
         const sfp_instance& I = inst[S.instance];
         auto in_inst = [&](int d) { return d >= I.first_seg && d < I.first_seg + I.n_seg; };
         if (S.radiating && (!in_inst(S.photon_dest) || !seg[S.photon_dest].massless))
@@ -700,6 +714,8 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
         if (S.bw && (!in_inst(S.ele_dest) || !in_inst(S.pos_dest) || seg[S.ele_dest].massless ||
                      seg[S.pos_dest].massless))
             return fail(SFP_EINVAL, "pair-creating segment needs massive destinations in its instance");
+        if (S.bw && S.ele_dest == S.pos_dest)
+            return fail(SFP_EINVAL, "pair-creating segment: electron and positron destinations must differ");
     }
     return SFP_OK;
 }
@@ -714,6 +730,17 @@ static int run_upload(sfp_run* r, const sfp_instance* inst, const int64_t* n_buf
     return SFP_OK;
 }
 
+// persistent grid of one kernel: resident blocks per SM x SMs
+static int persistent_grid(cudaKernel_t k, size_t smem, int fallback_per_sm) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, SFP_TILE_HOST, smem) != cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = fallback_per_sm;
+    }
+    return sm_count() * per_sm;
+}
+
 extern "C" {
 
 int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const sfp_instance* inst, int n_seg,
@@ -724,21 +751,32 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if (!m) return fail(SFP_EINVAL, "sfp_run_create: NULL module");
     if (cfg->qed != SFP_QED_REJECTION && cfg->qed != SFP_QED_OPTICAL_DEPTH) return fail(SFP_EINVAL, "unknown QED method");
     if (cfg->form != SFP_FORM_FP64 && cfg->form != SFP_FORM_FP32) return fail(SFP_EINVAL, "unknown arithmetic form");
+    const bool f64 = cfg->form == SFP_FORM_FP64;
+    const int items = cfg->items > 0 ? cfg->items : (f64 ? 1 : 1);
+    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (f64 ? 2 : 3);
+    const int unr = cfg->p_unroll > 0 ? cfg->p_unroll : (f64 ? 1 : 2);
+    const int pminb = cfg->p_min_blocks > 0 ? cfg->p_min_blocks : (f64 ? 3 : 4);
+    if (items < 1 || items > 4 || minb < 1 || minb > 8 || unr < 1 || unr > SFP_PHOTON_SUB_HOST ||
+        SFP_PHOTON_SUB_HOST % unr != 0 || pminb < 1 || pminb > 8)
+        return fail(SFP_EINVAL, "kernel variant out of range");
     auto* r = new sfp_run();
     r->mod = m;
     r->n_seg = n_seg;
     r->n_inst = n_inst;
     r->segs.assign(seg, seg + n_seg);
-    const int items = cfg->items > 0 ? cfg->items : 1;
-    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (cfg->form == SFP_FORM_FP64 ? 2 : 3);
-    if (items < 1 || items > 4 || minb < 1 || minb > 8) {
-        delete r;
-        return fail(SFP_EINVAL, "kernel variant out of range");
+    for (int s = 0; s < n_seg; ++s) {
+        (seg[s].massless ? r->pseg : r->mseg).push_back(s);
+        bool dest = false;
+        for (int q = 0; q < n_seg; ++q)
+            if (seg[q].bw && (seg[q].ele_dest == s || seg[q].pos_dest == s)) dest = true;
+        if (dest) r->cseg.push_back(s);
     }
-    std::string kname = std::string("sfp_step_") + (cfg->form == SFP_FORM_FP64 ? "fp64_" : "fp32_") +
-                        (cfg->qed == SFP_QED_REJECTION ? "rs" : "od") + "_i" + std::to_string(items) + "_b" +
-                        std::to_string(minb);
-    if ((rc = module_kernel(m, kname.c_str(), &r->k_step)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
+    const std::string fq = std::string(f64 ? "fp64_" : "fp32_") + (cfg->qed == SFP_QED_REJECTION ? "rs" : "od");
+    const std::string km = "sfp_massive_" + fq + "_i" + std::to_string(items) + "_b" + std::to_string(minb);
+    const std::string kp = "sfp_photon_" + fq + "_u" + std::to_string(unr) + "_b" + std::to_string(pminb);
+    const std::string kc = f64 ? "sfp_children_fp64" : "sfp_children_fp32";
+    if ((rc = module_kernel(m, km.c_str(), &r->k_massive)) || (rc = module_kernel(m, kp.c_str(), &r->k_photon)) ||
+        (rc = module_kernel(m, kc.c_str(), &r->k_children)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
         delete r;
         return rc;
     }
@@ -756,9 +794,13 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     h.dt = cfg->dt;
     h.photon_threshold = cfg->photon_threshold;
     h.qed = cfg->qed;
-    h.tile = SFP_TILE_HOST * items;
+    h.mtile = SFP_TILE_HOST * items;
+    h.ptile = SFP_TILE_HOST * SFP_PHOTON_SUB_HOST;
     h.any_appends = 0;
     for (int s = 0; s < n_seg; ++s) h.any_appends |= (seg[s].radiating || seg[s].bw) ? 1 : 0;
+    h.n_mseg = (int)r->mseg.size();
+    h.n_pseg = (int)r->pseg.size();
+    h.n_cseg = (int)r->cseg.size();
     h.rs = cfg->rs;
     h.od_photon = cfg->od_photon;
     h.od_pair = cfg->od_pair;
@@ -766,45 +808,62 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) return cleanup(fail(SFP_ENOMEM, "cudaMalloc " #ptr))
     sfp_segment* dseg;
     sfp_instance* dinst;
+    int *dm, *dp, *dc;
     ALLOC(dseg, n_seg * sizeof(sfp_segment));
     ALLOC(dinst, n_inst * sizeof(sfp_instance));
     h.seg = dseg;
     h.inst = dinst;
+    ALLOC(dm, (r->mseg.size() + 1) * sizeof(int));
+    ALLOC(dp, (r->pseg.size() + 1) * sizeof(int));
+    ALLOC(dc, (r->cseg.size() + 1) * sizeof(int));
+    h.mseg = dm;
+    h.pseg = dp;
+    h.cseg = dc;
     ALLOC(h.n_buffered, n_seg * sizeof(long long));
     ALLOC(h.appended, n_seg * sizeof(unsigned long long));
     ALLOC(h.n_buf_step, n_seg * sizeof(long long));
-    ALLOC(h.tile_start, (n_seg + 1) * sizeof(long long));
+    ALLOC(h.mtile_start, (r->mseg.size() + 1) * sizeof(long long));
+    ALLOC(h.ptile_start, (r->pseg.size() + 1) * sizeof(long long));
+    ALLOC(h.chain_first, n_seg * sizeof(long long));
     ALLOC(h.st, sizeof(sfp_step_state));
     ALLOC(r->d, sizeof(sfp_run_dev));
 #undef ALLOC
-    if (cudaMemsetAsync(h.appended, 0, n_seg * sizeof(unsigned long long), r->s) != cudaSuccess)
-        return cleanup(fail(SFP_ECUDA, "memset"));
+    if ((!r->mseg.empty() &&
+         cudaMemcpyAsync(dm, r->mseg.data(), r->mseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        (!r->pseg.empty() &&
+         cudaMemcpyAsync(dp, r->pseg.data(), r->pseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        (!r->cseg.empty() &&
+         cudaMemcpyAsync(dc, r->cseg.data(), r->cseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        cudaMemsetAsync(h.appended, 0, n_seg * sizeof(unsigned long long), r->s) != cudaSuccess ||
+        cudaMemsetAsync(h.chain_first, 0, n_seg * sizeof(long long), r->s) != cudaSuccess)
+        return cleanup(fail(SFP_ECUDA, "segment lists upload"));
     sfp_step_state st0{};
     st0.t = cfg->t0;
     st0.step = cfg->step0;
     st0.skip = 1;
     if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "state upload"));
-    if ((rc = run_alloc_tiles(r, tiles_for(r->segs, h.tile)))) return cleanup(rc);
+    if ((rc = run_alloc_tiles(r, tiles_for(r)))) return cleanup(rc);
     if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
-    // shared memory for the tables, persistent grid size
+    // shared memory for the tables, persistent grid sizes
     if (cfg->qed == SFP_QED_REJECTION)
-        r->smem = 2 * (size_t)cfg->rs.z_N * (cfg->form == SFP_FORM_FP64 ? sizeof(double) : sizeof(float));
+        r->smem = 2 * (size_t)cfg->rs.z_N * (f64 ? sizeof(double) : sizeof(float));
     else
         r->smem = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
-    if (r->smem > 48 * 1024) {
-        if (cudaFuncSetAttribute((const void*)r->k_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem) !=
-            cudaSuccess)
-            return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory for the table"));
+    if (r->smem > 16 * 1024) {
+        // the photon kernel's event lists take ~20 KB static shared memory:
+        // allow the table beside it
+        const int cap = 64 * 1024;
+        if (r->smem > (size_t)cap) return cleanup(fail(SFP_EINVAL, "QED tables exceed 64 KB of shared memory"));
+        if (cudaFuncSetAttribute((const void*)r->k_massive, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute((const void*)r->k_photon, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) !=
+                cudaSuccess)
+            return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory for the tables"));
     }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)r->k_step, SFP_TILE_HOST, r->smem) !=
-            cudaSuccess ||
-        per_sm <= 0) {
-        cudaGetLastError();
-        per_sm = 2;
-    }
-    r->grid = sm_count() * per_sm;
+    r->grid_m = persistent_grid(r->k_massive, r->smem, minb);
+    r->grid_p = persistent_grid(r->k_photon, r->smem, pminb);
+    r->grid_c = persistent_grid(r->k_children, 0, 2);
     *out = r;
     return SFP_OK;
 }
@@ -812,18 +871,43 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
 int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t* n_buffered) {
     if (!r || !seg) return fail(SFP_EINVAL, "sfp_run_update: NULL argument");
     if (n_seg != r->n_seg) return fail(SFP_EINVAL, "sfp_run_update: segment count changed");
+    for (int s = 0; s < n_seg; ++s)
+        if (seg[s].massless != r->segs[s].massless || seg[s].radiating != r->segs[s].radiating ||
+            seg[s].bw != r->segs[s].bw || seg[s].ele_dest != r->segs[s].ele_dest ||
+            seg[s].pos_dest != r->segs[s].pos_dest)
+            return fail(SFP_EINVAL, "sfp_run_update: segment roles changed");
     r->segs.assign(seg, seg + n_seg);
-    int rc = run_alloc_tiles(r, tiles_for(r->segs, r->h.tile));
+    int rc = run_alloc_tiles(r, tiles_for(r));
     if (rc) return rc;
     return run_upload(r, nullptr, n_buffered);
 }
 
-static int launch_unit(sfp_run* r, cudaStream_t s) {
+// one step: book(prepare), massive, photon, children; ev (6 events) brackets
+// the three step kernels when given
+static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev) {
     int prep = 1;
     void* a_book[] = {&r->d, &prep};
+    void* a[] = {&r->d};
     SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, s));
-    void* a_step[] = {&r->d};
-    SFP_CUDA(cudaLaunchKernel((const void*)r->k_step, dim3(r->grid), dim3(SFP_TILE_HOST), a_step, r->smem, s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[0], s));
+    if (!r->mseg.empty())
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem, s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[1], s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[2], s));
+    if (!r->pseg.empty())
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem, s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[3], s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[4], s));
+    if (!r->cseg.empty())
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_children, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, s));
+    if (ev) SFP_CUDA(cudaEventRecord(ev[5], s));
+    return SFP_OK;
+}
+
+static int launch_fold(sfp_run* r) {
+    int prep = 0;
+    void* a_book[] = {&r->d, &prep};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s));
     return SFP_OK;
 }
 
@@ -840,7 +924,7 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
             cudaGraph_t g;
             SFP_CUDA(cudaStreamBeginCapture(r->s, cudaStreamCaptureModeThreadLocal));
             int rc = SFP_OK;
-            for (int k = 0; k < graph_chunk && rc == SFP_OK; ++k) rc = launch_unit(r, r->s);
+            for (int k = 0; k < graph_chunk && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, nullptr);
             cudaError_t e = cudaStreamEndCapture(r->s, &g);
             if (rc) return rc;
             if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -853,12 +937,11 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
         for (; done + graph_chunk <= nsteps; done += graph_chunk) SFP_CUDA(cudaGraphLaunch(it->second, r->s));
     }
     for (; done < nsteps; ++done) {
-        int rc = launch_unit(r, r->s);
+        int rc = launch_unit(r, r->s, nullptr);
         if (rc) return rc;
     }
-    int prep = 0;
-    void* a_book[] = {&r->d, &prep};
-    SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s));
+    int rc = launch_fold(r);
+    if (rc) return rc;
     SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
     SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
     return SFP_OK;
@@ -870,30 +953,21 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     cudaStream_t cs = as_stream(stream);
     SFP_CUDA(cudaEventRecord(r->ev_in, cs));
     SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
-    std::vector<cudaEvent_t> ev(2 * nsteps, nullptr);
+    std::vector<cudaEvent_t> ev(6 * nsteps, nullptr);
     int rc = SFP_OK;
     for (auto& e : ev)
         if (cudaEventCreate(&e) != cudaSuccess) rc = fail(SFP_ECUDA, "cudaEventCreate");
-    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) {
-        int prep = 1;
-        void* a_book[] = {&r->d, &prep};
-        void* a_step[] = {&r->d};
-        if (cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s) != cudaSuccess ||
-            cudaEventRecord(ev[2 * k], r->s) != cudaSuccess ||
-            cudaLaunchKernel((const void*)r->k_step, dim3(r->grid), dim3(SFP_TILE_HOST), a_step, r->smem, r->s) !=
-                cudaSuccess ||
-            cudaEventRecord(ev[2 * k + 1], r->s) != cudaSuccess)
-            rc = fail(SFP_ECUDA, std::string("timed launch: ") + cudaGetErrorString(cudaGetLastError()));
-    }
-    if (rc == SFP_OK) {
-        int prep = 0;
-        void* a_book[] = {&r->d, &prep};
-        if (cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, r->s) != cudaSuccess)
-            rc = fail(SFP_ECUDA, "fold launch");
-    }
+    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, &ev[6 * k]);
+    if (rc == SFP_OK) rc = launch_fold(r);
     if (rc == SFP_OK && cudaStreamSynchronize(r->s) != cudaSuccess) rc = fail(SFP_ECUDA, "synchronize");
+    const bool has[3] = {!r->mseg.empty(), !r->pseg.empty(), !r->cseg.empty()};
     for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k)
-        if (cudaEventElapsedTime(&kernel_ms[k], ev[2 * k], ev[2 * k + 1]) != cudaSuccess) rc = fail(SFP_ECUDA, "elapsed");
+        for (int j = 0; j < 3 && rc == SFP_OK; ++j) {
+            kernel_ms[3 * k + j] = 0.0f;
+            if (has[j] && cudaEventElapsedTime(&kernel_ms[3 * k + j], ev[6 * k + 2 * j], ev[6 * k + 2 * j + 1]) !=
+                              cudaSuccess)
+                rc = fail(SFP_ECUDA, "elapsed");
+        }
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (rc) return rc;
@@ -937,10 +1011,15 @@ int sfp_run_destroy(sfp_run* r) {
     for (auto& kv : r->graphs) cudaGraphExecDestroy(kv.second);
     cudaFree((void*)r->h.seg);
     cudaFree((void*)r->h.inst);
+    cudaFree((void*)r->h.mseg);
+    cudaFree((void*)r->h.pseg);
+    cudaFree((void*)r->h.cseg);
     cudaFree(r->h.n_buffered);
     cudaFree(r->h.appended);
     cudaFree(r->h.n_buf_step);
-    cudaFree(r->h.tile_start);
+    cudaFree(r->h.mtile_start);
+    cudaFree(r->h.ptile_start);
+    cudaFree(r->h.chain_first);
     cudaFree(r->h.tile_flag);
     cudaFree(r->h.tile_agg);
     cudaFree(r->h.tile_incl);

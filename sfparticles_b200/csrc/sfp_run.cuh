@@ -1,19 +1,31 @@
 // sfp_run.cuh -- device-side layout of a fused-step run, shared by the host
 // C-ABI (nvcc) and the NVRTC-compiled step modules.
+//
+// A step runs three kernels over two tile groups:
+//   massive group -- tiles over the e+- (massive) segments: QED photon
+//                    emission, recoil, Boris push, photon children;
+//   photon group  -- tiles over the photon segments: pair creation, photon
+//                    push, pair children written unpushed;
+//   children      -- the pair children of this step, pushed.
+// Each group numbers its tiles from 0; the look-back flags of the photon
+// group follow those of the massive group in one flag array.
 #pragma once
 #include "sfp_types.h"
 
 struct sfp_step_state {
-    double t;            // time of the prepared / running step
-    long long step;      // steps completed
-    long long n_tiles;   // tiles of the prepared step
-    int ticket;          // next tile to hand out
-    int skip;            // 1: the prepared step must not run
-    int halted;          // sticky: capacity guard tripped (host regrows, resets)
-    int error;           // sticky device error (SFP_DEV_*)
-    unsigned int epoch;  // look-back flag epoch of the prepared step
-    int pending;         // a prepared step awaits folding
-    long long particle_steps;  // sum over executed steps of all N_buffered
+    double t;                   // time of the prepared / running step
+    long long step;             // steps completed
+    long long n_mtiles;         // massive-group tiles of the prepared step
+    long long n_ptiles;         // photon-group tiles
+    int mticket;                // next massive tile to hand out
+    int pticket;                // next photon tile to hand out
+    int skip;                   // 1: the prepared step must not run
+    int halted;                 // sticky: capacity guard tripped (host regrows, resets)
+    int error;                  // sticky device error (SFP_DEV_*)
+    unsigned int epoch;         // look-back flag epoch of the prepared step
+    int pending;                // a prepared step awaits folding
+    int pad;
+    long long particle_steps;   // sum over executed steps of all N_buffered
 };
 
 struct sfp_run_dev {
@@ -23,17 +35,26 @@ struct sfp_run_dev {
     int n_inst;
     double dt;
     double photon_threshold;
-    int qed;              // SFP_QED_*
-    int tile;             // particles per tile (= block size)
-    int any_appends;      // some segment radiates or creates pairs
+    int qed;                    // SFP_QED_*
+    int mtile;                  // particles per massive tile (256 * items)
+    int ptile;                  // particles per photon tile
+    int any_appends;            // some segment radiates or creates pairs
+    int n_mseg;                 // massive segments (instance order)
+    int n_pseg;                 // photon segments
+    int n_cseg;                 // segments receiving pair children
     int pad;
+    const int* mseg;            // [n_mseg] segment indices
+    const int* pseg;            // [n_pseg]
+    const int* cseg;            // [n_cseg]
     sfp_rs_table rs;
     sfp_od_table od_photon;
     sfp_od_table od_pair;
     long long* n_buffered;        // [n_seg] authoritative buffered counts
     unsigned long long* appended; // [n_seg] children appended by the running step
     long long* n_buf_step;        // [n_seg] counts at the start of the running step
-    long long* tile_start;        // [n_seg + 1]
+    long long* mtile_start;       // [n_mseg + 1]
+    long long* ptile_start;       // [n_pseg + 1]
+    long long* chain_first;       // [n_seg] flag index of the first tile of the segment's chain
     long long max_tiles;
     unsigned int* tile_flag;      // [max_tiles] (epoch << 2) | status
     uint4* tile_agg;              // [max_tiles] per-channel tile counts

@@ -14,9 +14,14 @@
 //   5. pairs appended, converted photons pruned,
 //   6. every pushed particle -- children included -- pushed from t to t+dt:
 //      half position, fields at t+dt/2, Boris / Boris-TBMT (+LL/CLL), half position.
-// Appends are ordered: a block-wide scan plus a decoupled look-back across
-// tiles gives each child the slot the reference's find_event_index + create_*
-// would give it, so Philox streams keyed by slot are reproducible.
+// A step is three kernels (after the bookkeeping kernel): the massive group
+// (e+- tiles: 3, 4, recoil, 6), the photon group (photon tiles: 2, 5, 6 for
+// photons) and the pair children's push (6 for this step's pairs).  The two
+// groups touch disjoint memory: each writes its children past the start-of-
+// step count of the other group's buffers.  Appends are ordered: a block
+// scan plus a decoupled look-back across the tiles of a group gives each
+// child the slot that the reference's find_event_index + create_* would give
+// it, so Philox streams keyed by slot are reproducible.
 #pragma once
 #include "sfp_device.cuh"
 #include "sfp_device32.cuh"
@@ -263,9 +268,180 @@ SFP_DEVICE_INLINE void push_photon32(double& x, double& y, double& z, double ux,
 }  // namespace sfp
 
 #if defined(SFP_WANT_STEP)
+
 // ---------------------------------------------------------------------------
-// Bookkeeping: fold the appends of the step that ran, advance t, then (mode 1)
-// prepare the next step: capacity guard, tile map, ticket, epoch.
+// QED tables staged in shared memory (float64, or float32 copies for FP32)
+// ---------------------------------------------------------------------------
+struct sfp_qed_smem {
+    const double* iAt;
+    const double* dAt;
+    const float* iAf;
+    const float* dAf;
+    const double* od_ph;
+    const double* od_pa;
+    int zN;
+    double zmax;
+    float inv_dzf;
+    float base_maxf;
+    double chi_pair_min;  // below: no pair event is possible (z_min > z_max)
+};
+
+template <int FORM, int QED>
+__device__ __forceinline__ sfp_qed_smem sfp_stage_tables(const sfp_run_dev* __restrict__ R, double* s_tab) {
+    sfp_qed_smem T;
+    T.iAt = T.dAt = s_tab;
+    T.iAf = T.dAf = reinterpret_cast<const float*>(s_tab);
+    T.od_ph = T.od_pa = s_tab;
+    T.zN = 0;
+    T.zmax = 0.0;
+    if (QED == SFP_QED_REJECTION) {
+        T.zN = R->rs.z_N;
+        T.zmax = R->rs.z_max;
+        if (FORM == SFP_FORM_FP64) {
+            for (int i = threadIdx.x; i < T.zN; i += blockDim.x) {
+                s_tab[i] = R->rs.int_Ai[i];
+                s_tab[T.zN + i] = R->rs.Aip[i];
+            }
+            T.dAt = s_tab + T.zN;
+        } else {
+            float* f = reinterpret_cast<float*>(s_tab);
+            for (int i = threadIdx.x; i < T.zN; i += blockDim.x) {
+                f[i] = (float)R->rs.int_Ai[i];
+                f[T.zN + i] = (float)R->rs.Aip[i];
+            }
+            T.dAf = f + T.zN;
+        }
+    } else {
+        const int n1 = R->od_photon.chi_N, n2 = R->od_pair.chi_N;
+        for (int i = threadIdx.x; i < n1; i += blockDim.x) s_tab[i] = R->od_photon.rate_total[i];
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) s_tab[n1 + i] = R->od_pair.rate_total[i];
+        T.od_pa = s_tab + n1;
+    }
+    T.inv_dzf = (float)((double)(T.zN - 1) / T.zmax);
+    T.base_maxf = (float)(T.zmax * sqrt(T.zmax));
+    // pair creation needs z_min = (4/chi)^(2/3) <= z_max: exact cut with margin
+    T.chi_pair_min = QED == SFP_QED_REJECTION ? 4.0 / (T.zmax * sqrt(T.zmax)) * (1.0 - 1e-6) : 0.0;
+    return T;
+}
+
+// photon emission by a massive particle at t (qed/rejection_sampling.py:73-89,
+// optical_depth.py:15-62, hard-photon filter cpu.py:226-231)
+template <int FORM, int QED>
+__device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
+                                                 const sfp_segment& S, const sfp_instance& I,
+                                                 const double* __restrict__ P, double x, double y, double z, double ux,
+                                                 double uy, double uz, double t, unsigned int step, long long i,
+                                                 double& tau, double& delta) {
+    using namespace sfp;
+    const double dt = R->dt;
+    bool ev = false;
+    double d = 0.0;
+    if (FORM == SFP_FORM_FP64) {
+        double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (S.push) sfp_field_program(x, y, z, t, P, F);
+        const double ig = inv_gamma_massive(ux, uy, uz);
+        const double chi = chi_of(F, ux, uy, uz, ig);
+        if (QED == SFP_QED_REJECTION) {
+            if (chi != 0.0) {
+                double r1, r2;
+                uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
+                ev = photon_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
+            }
+        } else {
+            ev = od_event(chi, ig, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+        }
+        if (ev && d / ig < R->photon_threshold) ev = false;
+    } else {
+        float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (S.push) sfp_field_program32(x, y, z, t, P, F);
+        const float g = sfp32::gamma_of(ux, uy, uz, false);
+        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+        if (QED == SFP_QED_REJECTION) {
+            if (chi > 0.0f) {
+                float r1, r2;
+                sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+                const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
+                const float dl = r1 * r1 * r1;
+                const float base = dl / ((1.0f - dl) * chi);
+                const float W = -kRate * sfp32::rate_core(dl * chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, 1.0f);
+                ev = r2 < 3.0f * r1 * r1 * W * ((float)dt / g);
+                d = (double)dl;
+                if (ev && dl * g < (float)R->photon_threshold) ev = false;
+            }
+        } else {
+            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+            if (ev && d * (double)g < R->photon_threshold) ev = false;
+        }
+        if (!ev) d = 0.0;
+    }
+    delta = d;
+    return ev;
+}
+
+// pair creation by a photon at t (qed/rejection_sampling.py:92-107,
+// optical_depth.py:64-111)
+template <int FORM, int QED>
+__device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
+                                               const sfp_segment& S, const sfp_instance& I,
+                                               const double* __restrict__ P, double x, double y, double z, double ux,
+                                               double uy, double uz, double t, unsigned int step, long long i,
+                                               double& tau, double& delta) {
+    using namespace sfp;
+    const double dt = R->dt;
+    bool ev = false;
+    double d = 0.0;
+    if (FORM == SFP_FORM_FP64) {
+        double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (S.push) sfp_field_program(x, y, z, t, P, F);
+        const double ig = inv_gamma_photon(ux, uy, uz);
+        const double chi = chi_of(F, ux, uy, uz, ig);
+        if (QED == SFP_QED_REJECTION) {
+            if (chi != 0.0 && !(chi < T.chi_pair_min)) {
+                double r1, r2;
+                uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
+                ev = pair_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
+            }
+        } else {
+            ev = od_event(chi, ig, dt, tau, R->od_pair, T.od_pa, I.seed, S.stream, step, i, d);
+        }
+    } else {
+        float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (S.push) sfp_field_program32(x, y, z, t, P, F);
+        const float g = sfp32::gamma_of(ux, uy, uz, true);
+        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+        if (QED == SFP_QED_REJECTION) {
+            if (chi > 0.0f && !((double)chi < T.chi_pair_min)) {
+                float r1, r2;
+                sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+                const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
+                const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
+                const float W = kRate * sfp32::rate_core(chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, -1.0f);
+                ev = r2 < W * ((float)dt / g);
+                d = (double)r1;
+            }
+        } else {
+            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_pair, T.od_pa, I.seed, S.stream, step, i, d);
+        }
+        if (!ev) d = 0.0;
+    }
+    delta = d;
+    return ev;
+}
+
+// largest j with start[j] <= tk (binary search over a group's tile starts)
+__device__ __forceinline__ int sfp_find_group_pos(const long long* __restrict__ start, int n, long long tk) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= tk) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Bookkeeping: fold the appends of the step that ran, advance t; then
+// (prepare) the capacity guard, the tile maps of both groups, tickets, epoch.
 // One block of 256 threads.
 // ---------------------------------------------------------------------------
 extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_dev* __restrict__ R, int prepare) {
@@ -313,22 +489,48 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
         return;
     }
     if (threadIdx.x == 0) {
-        long long acc = 0, ps = 0;
-        const long long T = R->tile;
+        long long ps = 0;
         for (int s = 0; s < n; ++s) {
-            R->tile_start[s] = acc;
             R->n_buf_step[s] = R->n_buffered[s];
-            acc += (R->n_buffered[s] + T - 1) / T;
             ps += R->n_buffered[s];
         }
-        R->tile_start[n] = acc;
-        if (acc > R->max_tiles) {
+        long long acc = 0;
+        int prev_inst = -1;
+        long long chain = 0;
+        for (int j = 0; j < R->n_mseg; ++j) {
+            const int s = R->mseg[j];
+            R->mtile_start[j] = acc;
+            if (R->seg[s].instance != prev_inst) {
+                prev_inst = R->seg[s].instance;
+                chain = acc;
+            }
+            R->chain_first[s] = chain;
+            acc += (R->n_buffered[s] + R->mtile - 1) / R->mtile;
+        }
+        R->mtile_start[R->n_mseg] = acc;
+        const long long m_tiles = acc;
+        acc = 0;
+        prev_inst = -1;
+        for (int j = 0; j < R->n_pseg; ++j) {
+            const int s = R->pseg[j];
+            R->ptile_start[j] = acc;
+            if (R->seg[s].instance != prev_inst) {
+                prev_inst = R->seg[s].instance;
+                chain = m_tiles + acc;
+            }
+            R->chain_first[s] = chain;
+            acc += (R->n_buffered[s] + R->ptile - 1) / R->ptile;
+        }
+        R->ptile_start[R->n_pseg] = acc;
+        if (m_tiles + acc > R->max_tiles) {
             st->error = SFP_DEV_CAPACITY;
             st->skip = 1;
             return;
         }
-        st->n_tiles = acc;
-        st->ticket = 0;
+        st->n_mtiles = m_tiles;
+        st->n_ptiles = acc;
+        st->mticket = 0;
+        st->pticket = 0;
         st->epoch = (unsigned int)((st->step + 1) & 0x3FFFFFFFll);
         if (st->epoch == 0u) st->epoch = 1u;
         st->skip = 0;
@@ -338,103 +540,49 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
 }
 
 // ---------------------------------------------------------------------------
-// The fused step.  Persistent grid; tiles of SFP_TILE * ITEMS particles are
-// handed out in order; item k of thread j covers particle k*SFP_TILE + j of
-// the tile, so the ordered append scans items k-major.
-//
-// Per tile:  load -> QED events -> publish the tile's append count (and try
-// a non-blocking look-back) -> recoil + push every parent (registers) ->
-// finish the look-back -> write children (from the parent's stored,
-// not yet overwritten state) -> store the parents.  The look-back wait is
-// thus taken after the expensive push, when the predecessors are done.
+// Massive group.  Tiles of 256 * ITEMS particles; item k of thread j is
+// particle k*256 + j of the tile (so the ordered append scans items
+// k-major).  Per tile: load -> photon events at t -> publish the count, try
+// the look-back -> recoil + push (registers) -> finish the look-back ->
+// photon children from the parents' stored (pre-push) state -> store.
 // ---------------------------------------------------------------------------
 template <int FORM, int QED, int ITEMS>
-__device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R) {
+__device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
     extern __shared__ double s_tab[];
     __shared__ long long s_tile;
-    __shared__ int s_seg;
+    __shared__ int s_pos;
     __shared__ unsigned int s_warp[ITEMS][SFP_TILE / 32];
     __shared__ uint4 s_excl;
-
     sfp_step_state* st = R->st;
-    if (st->skip) return;
-    const long long n_tiles = st->n_tiles;
+    if (st->skip || st->n_mtiles == 0) return;
+    const long long n_tiles = st->n_mtiles;
     const double t = st->t;
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
     const unsigned int epoch = st->epoch;
-
-    // QED tables into shared memory (float64 or float32 copies)
-    const double* iAt = s_tab;
-    const double* dAt = s_tab;
-    const float* iAf = reinterpret_cast<const float*>(s_tab);
-    const float* dAf = iAf;
-    const double* od_rate_ph = s_tab;
-    const double* od_rate_pa = s_tab;
-    int zN = 0;
-    double zmax = 0.0;
-    if (QED == SFP_QED_REJECTION) {
-        zN = R->rs.z_N;
-        zmax = R->rs.z_max;
-        if (FORM == SFP_FORM_FP64) {
-            for (int i = threadIdx.x; i < zN; i += blockDim.x) {
-                s_tab[i] = R->rs.int_Ai[i];
-                s_tab[zN + i] = R->rs.Aip[i];
-            }
-            dAt = s_tab + zN;
-        } else {
-            float* f = reinterpret_cast<float*>(s_tab);
-            for (int i = threadIdx.x; i < zN; i += blockDim.x) {
-                f[i] = (float)R->rs.int_Ai[i];
-                f[zN + i] = (float)R->rs.Aip[i];
-            }
-            dAf = f + zN;
-        }
-    } else {
-        const int n1 = R->od_photon.chi_N, n2 = R->od_pair.chi_N;
-        for (int i = threadIdx.x; i < n1; i += blockDim.x) s_tab[i] = R->od_photon.rate_total[i];
-        for (int i = threadIdx.x; i < n2; i += blockDim.x) s_tab[n1 + i] = R->od_pair.rate_total[i];
-        od_rate_pa = s_tab + n1;
-    }
-    const float inv_dzf = (float)((double)(zN - 1) / zmax);
-    const float base_maxf = (float)(zmax * sqrt(zmax));
-    // pair creation needs z_min = (4/chi)^(2/3) <= z_max (the rate is 0 above
-    // the table): below this chi no pair event can happen, exactly
-    const double chi_pair_min = QED == SFP_QED_REJECTION ? 4.0 / (zmax * sqrt(zmax)) * (1.0 - 1e-6) : 0.0;
-    const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);  // alpha m c^2 / hbar
-    const float thrf = (float)R->photon_threshold;
+    const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
     const bool any_appends = R->any_appends != 0;
-
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) {
-            const long long tk = (long long)atomicAdd(&st->ticket, 1);
+            const long long tk = (long long)atomicAdd(&st->mticket, 1);
             s_tile = tk;
-            int s = 0;
-            if (tk < n_tiles) {  // largest s with tile_start[s] <= tk
-                int lo = 0, hi = R->n_seg - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (R->tile_start[mid] <= tk) lo = mid;
-                    else hi = mid - 1;
-                }
-                s = lo;
-            }
-            s_seg = s;
+            s_pos = tk < n_tiles ? sfp_find_group_pos(R->mtile_start, R->n_mseg, tk) : 0;
         }
         __syncthreads();
         const long long tile = s_tile;
         if (tile >= n_tiles) break;
-        const int si = s_seg;
+        const int pos = s_pos;
+        const int si = R->mseg[pos];
         const sfp_segment& S = R->seg[si];
         const sfp_instance& I = R->inst[S.instance];
         const double* __restrict__ P = I.field_params;
         const long long N = R->n_buf_step[si];
-        const long long first_tile = R->tile_start[I.first_seg];
-        const long long i0 = (tile - R->tile_start[si]) * (long long)(SFP_TILE * ITEMS) + threadIdx.x;
-        const bool qed_seg = S.radiating || S.bw;
+        const long long first_tile = R->chain_first[si];
+        const long long i0 = (tile - R->mtile_start[pos]) * (long long)(SFP_TILE * ITEMS) + threadIdx.x;
 
         bool alive[ITEMS], ev[ITEMS];
         double x[ITEMS], y[ITEMS], z[ITEMS], ux[ITEMS], uy[ITEMS], uz[ITEMS], tau[ITEMS], delta[ITEMS];
@@ -451,71 +599,15 @@ __device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R)
                 if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau[k] = S.tau[i];
             }
         }
-
-        // --- QED events at t (fields at t only for pushed species) ---------
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
-            if (!(alive[k] && qed_seg)) continue;
-            const long long i = i0 + (long long)k * SFP_TILE;
-            if (FORM == SFP_FORM_FP64) {
-                double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                if (S.push) sfp_field_program(x[k], y[k], z[k], t, P, F);
-                const double ig = S.massless ? inv_gamma_photon(ux[k], uy[k], uz[k])
-                                             : inv_gamma_massive(ux[k], uy[k], uz[k]);
-                const double chi = chi_of(F, ux[k], uy[k], uz[k], ig);
-                double d = 0.0;
-                if (QED == SFP_QED_REJECTION) {
-                    if (chi != 0.0 && !(S.bw && chi < chi_pair_min)) {
-                        double r1, r2;
-                        uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
-                        ev[k] = S.bw ? pair_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, d)
-                                     : photon_event_rs(chi, ig, dt, r1, r2, iAt, dAt, zN, zmax, d);
-                    }
-                } else {
-                    ev[k] = S.bw ? od_event(chi, ig, dt, tau[k], R->od_pair, od_rate_pa, I.seed, S.stream, step, i, d)
-                                 : od_event(chi, ig, dt, tau[k], R->od_photon, od_rate_ph, I.seed, S.stream, step, i, d);
-                }
-                if (ev[k] && S.radiating && d / ig < R->photon_threshold) ev[k] = false;  // cpu.py:226-231
-                delta[k] = d;
-            } else {
-                float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (S.push) sfp_field_program32(x[k], y[k], z[k], t, P, F);
-                const float g = sfp32::gamma_of(ux[k], uy[k], uz[k], S.massless != 0);
-                const float chi = sfp32::chi_of(F, (float)ux[k], (float)uy[k], (float)uz[k], g);
-                double d = 0.0;
-                if (QED == SFP_QED_REJECTION) {
-                    if (chi > 0.0f && !(S.bw && (double)chi < chi_pair_min)) {
-                        float r1, r2;
-                        sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
-                        const float dtau = (float)dt / g;
-                        if (S.bw) {  // qed/rejection_sampling.py:92-107, delta = r1
-                            const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
-                            const float W = kRate * sfp32::rate_core(chi, base, iAf, dAf, inv_dzf, zN, base_maxf, -1.0f);
-                            ev[k] = r2 < W * dtau;
-                            d = (double)r1;
-                        } else {  // qed/rejection_sampling.py:73-89, delta = r1^3
-                            const float dl = r1 * r1 * r1;
-                            const float base = dl / ((1.0f - dl) * chi);
-                            const float W = -kRate * sfp32::rate_core(dl * chi, base, iAf, dAf, inv_dzf, zN, base_maxf, 1.0f);
-                            ev[k] = r2 < 3.0f * r1 * r1 * W * dtau;
-                            d = (double)dl;
-                            if (ev[k] && dl * g < thrf) ev[k] = false;
-                        }
-                    }
-                } else {
-                    const double igd = 1.0 / (double)g;
-                    ev[k] = S.bw ? od_event((double)chi, igd, dt, tau[k], R->od_pair, od_rate_pa, I.seed, S.stream, step,
-                                            i, d)
-                                 : od_event((double)chi, igd, dt, tau[k], R->od_photon, od_rate_ph, I.seed, S.stream,
-                                            step, i, d);
-                    if (ev[k] && S.radiating && d * (double)g < R->photon_threshold) ev[k] = false;
-                }
-                if (!ev[k]) d = 0.0;
-                delta[k] = d;
+            if (alive[k] && S.radiating) {
+                const long long i = i0 + (long long)k * SFP_TILE;
+                ev[k] = sfp_photon_event<FORM, QED>(R, T, S, I, P, x[k], y[k], z[k], ux[k], uy[k], uz[k], t, step, i,
+                                                    tau[k], delta[k]);
             }
         }
-
-        // --- tile count: block scan (k-major); publish, try the look-back ---
+        // tile count (k-major block scan); publish and try the look-back
         unsigned int wpre[ITEMS];
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
@@ -537,14 +629,8 @@ __device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R)
             }
             const unsigned int total = __shfl_sync(0xffffffffu, inc, 31);
             if (lane < ITEMS * NW) s_warp[lane / NW][lane % NW] = inc - v;
-            if (qed_seg) agg = u4_one(S.channel, total);
-            if (lane == 0 && total) {
-                if (S.radiating) atomicAdd(&R->appended[S.photon_dest], (unsigned long long)total);
-                if (S.bw) {
-                    atomicAdd(&R->appended[S.ele_dest], (unsigned long long)total);
-                    atomicAdd(&R->appended[S.pos_dest], (unsigned long long)total);
-                }
-            }
+            if (S.radiating) agg = u4_one(S.channel, total);
+            if (lane == 0 && total) atomicAdd(&R->appended[S.photon_dest], (unsigned long long)total);
             uint4 ex{0u, 0u, 0u, 0u};
             if (tile == first_tile) {
                 publish(R, tile, agg, epoch, true);
@@ -555,31 +641,21 @@ __device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R)
             }
             if (lane == 0) s_excl = ex;
         }
-
-        // --- recoil and push of every parent, in registers ------------------
-        bool conv[ITEMS];
+        // recoil and push, in registers
         double sx[ITEMS], sy[ITEMS], sz[ITEMS];
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
             const long long i = i0 + (long long)k * SFP_TILE;
-            conv[k] = ev[k] && S.bw;  // converted photons are pruned, not pushed (cpu.py:190)
             sx[k] = sy[k] = sz[k] = 0.0;
-            if (ev[k] && S.radiating && S.rr == SFP_RR_PHOTON) {  // recoil, cpu.py:76-87
+            if (ev[k] && S.rr == SFP_RR_PHOTON) {  // recoil, cpu.py:76-87
                 const double f = 1.0 - delta[k];
                 ux[k] = ux[k] * f; uy[k] = uy[k] * f; uz[k] = uz[k] * f;
             }
-            if (!(alive[k] && !conv[k] && S.push)) continue;
-            if (S.massless) {
-                if (FORM == SFP_FORM_FP64) push_photon(x[k], y[k], z[k], ux[k], uy[k], uz[k], dt);
-                else push_photon32(x[k], y[k], z[k], ux[k], uy[k], uz[k], dt);
-            } else {
-                if (S.spin) { sx[k] = S.sx[i]; sy[k] = S.sy[i]; sz[k] = S.sz[i]; }
-                if (FORM == SFP_FORM_FP64) push_massive(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
-                else push_massive32(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
-            }
+            if (!(alive[k] && S.push)) continue;
+            if (S.spin) { sx[k] = S.sx[i]; sy[k] = S.sy[i]; sz[k] = S.sz[i]; }
+            if (FORM == SFP_FORM_FP64) push_massive(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
+            else push_massive32(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
         }
-
-        // --- finish the look-back -------------------------------------------
         if (warp == 0 && any_appends && !__all_sync(0xffffffffu, have_excl)) {
             const uint4 ex = lookback_wait(R, tile, first_tile, epoch);
             publish(R, tile, u4_add(ex, agg), epoch, true);
@@ -587,84 +663,280 @@ __device__ __forceinline__ void sfp_step_body(const sfp_run_dev* __restrict__ R)
         }
         __syncthreads();
         const long long ch_base = any_appends ? (long long)u4_get(s_excl, S.channel) : 0ll;
-
-        // --- children, then the parents' state ------------------------------
+        // photon children (cpu.py:89-116) from the stored pre-push state, then the parents
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
             const long long i = i0 + (long long)k * SFP_TILE;
             if (ev[k]) {
-                const long long off = ch_base + s_warp[k][warp] + wpre[k];
-                if (S.radiating) {  // photon at the parent's pre-push position, u = delta * u (cpu.py:89-116)
-                    const sfp_segment& D = R->seg[S.photon_dest];
-                    const long long slot = R->n_buf_step[S.photon_dest] + off;
-                    double cx = S.x[i], cy = S.y[i], cz = S.z[i];
-                    const double cux = delta[k] * S.ux[i], cuy = delta[k] * S.uy[i], cuz = delta[k] * S.uz[i];
-                    if (D.push) {
-                        if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
-                        else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
-                    }
-                    D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
-                    D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
-                    if (D.tau) D.tau[slot] = 0.0;
-                    D.pruned[slot] = 0;
-                } else {  // e- and e+ from the (unpushed) photon (cpu.py:119-189)
-                    for (int w = 0; w < 2; ++w) {
-                        const int di = (w == 0) ? S.ele_dest : S.pos_dest;
-                        const sfp_segment& D = R->seg[di];
-                        const double d = (w == 0) ? delta[k] : 1.0 - delta[k];
-                        double cx = x[k], cy = y[k], cz = z[k], cux = d * ux[k], cuy = d * uy[k], cuz = d * uz[k];
-                        double csx = 0.0, csy = 0.0, csz = 0.0;
-                        if (D.push) {
-                            if (FORM == SFP_FORM_FP64) push_massive(cx, cy, cz, cux, cuy, cuz, csx, csy, csz, D, P, t, dt);
-                            else push_massive32(cx, cy, cz, cux, cuy, cuz, csx, csy, csz, D, P, t, dt);
-                        }
-                        const long long slot = R->n_buf_step[di] + off;
-                        D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
-                        D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
-                        if (D.spin) { D.sx[slot] = csx; D.sy[slot] = csy; D.sz[slot] = csz; }
-                        if (D.tau) D.tau[slot] = 0.0;
-                        D.pruned[slot] = 0;
-                    }
-                    S.pruned[i] = 1;
+                const sfp_segment& D = R->seg[S.photon_dest];
+                const long long slot = R->n_buf_step[S.photon_dest] + ch_base + s_warp[k][warp] + wpre[k];
+                double cx = S.x[i], cy = S.y[i], cz = S.z[i];
+                const double cux = delta[k] * S.ux[i], cuy = delta[k] * S.uy[i], cuz = delta[k] * S.uz[i];
+                if (D.push) {
+                    if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
+                    else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
                 }
+                D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
+                D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
+                if (D.tau) D.tau[slot] = 0.0;
+                D.pruned[slot] = 0;
             }
-            if (alive[k] && !conv[k]) {
-                if (S.push) { S.x[i] = x[k]; S.y[i] = y[k]; S.z[i] = z[k]; }
-                if (!S.massless && (S.push || (ev[k] && S.rr == SFP_RR_PHOTON))) {
-                    S.ux[i] = ux[k]; S.uy[i] = uy[k]; S.uz[i] = uz[k];
+            if (alive[k]) {
+                if (S.push) {
+                    S.x[i] = x[k]; S.y[i] = y[k]; S.z[i] = z[k];
+                    if (S.spin) { S.sx[i] = sx[k]; S.sy[i] = sy[k]; S.sz[i] = sz[k]; }
                 }
-                if (S.spin && S.push && !S.massless) { S.sx[i] = sx[k]; S.sy[i] = sy[k]; S.sz[i] = sz[k]; }
+                if (S.push || (ev[k] && S.rr == SFP_RR_PHOTON)) { S.ux[i] = ux[k]; S.uy[i] = uy[k]; S.uz[i] = uz[k]; }
+                if (QED == SFP_QED_OPTICAL_DEPTH && S.tau && S.radiating) S.tau[i] = tau[k];
             }
-            if (QED == SFP_QED_OPTICAL_DEPTH && alive[k] && S.tau && qed_seg) S.tau[i] = tau[k];
         }
     }
 }
 
-// kernels: <form>_<qed>_i<items per thread>_b<min resident blocks per SM>
-#define SFP_STEP_KERNEL(NAME, FORM, QED, ITEMS, MINB)                                                      \
-    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB) NAME(const sfp_run_dev* __restrict__ R) { \
-        sfp_step_body<FORM, QED, ITEMS>(R);                                                                \
+// ---------------------------------------------------------------------------
+// Photon group.  Streaming tiles of SUB * 256 photons: each sub-step loads,
+// tests for pair creation, pushes and stores its photons at once; events go
+// into per-warp shared-memory lists (no block barrier while streaming); at
+// the end of the tile one look-back orders them and the e-/e+ children are
+// written, unpushed, from the converted photons' (unmoved) state.
+// ---------------------------------------------------------------------------
+template <int FORM, int QED, int SUB, int UNR>
+__device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ R) {
+    using namespace sfp;
+    constexpr int NW = SFP_TILE / 32;
+    static_assert(SUB * NW <= 64, "scan covers at most 64 (sub, warp) groups");
+    extern __shared__ double s_tab[];
+    __shared__ long long s_tile;
+    __shared__ int s_pos;
+    __shared__ unsigned int s_cnt[SUB][NW];
+    __shared__ uint4 s_excl;
+    __shared__ double s_evd[NW][32 * SUB];
+    __shared__ unsigned int s_evi[NW][32 * SUB];
+    sfp_step_state* st = R->st;
+    if (st->skip || st->n_ptiles == 0) return;
+    const long long n_tiles = st->n_ptiles;
+    const long long flag0 = st->n_mtiles;
+    const double t = st->t;
+    const double dt = R->dt;
+    const unsigned int step = (unsigned int)st->step;
+    const unsigned int epoch = st->epoch;
+    const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
+    const bool any_appends = R->any_appends != 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
+
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const long long tk = (long long)atomicAdd(&st->pticket, 1);
+            s_tile = tk;
+            s_pos = tk < n_tiles ? sfp_find_group_pos(R->ptile_start, R->n_pseg, tk) : 0;
+        }
+        __syncthreads();
+        const long long tile = s_tile;
+        if (tile >= n_tiles) break;
+        const int pos = s_pos;
+        const int si = R->pseg[pos];
+        const sfp_segment& S = R->seg[si];
+        const sfp_instance& I = R->inst[S.instance];
+        const double* __restrict__ P = I.field_params;
+        const long long N = R->n_buf_step[si];
+        const long long base = (tile - R->ptile_start[pos]) * (long long)(SFP_TILE * SUB);
+        unsigned int wn = 0;  // events recorded by this warp
+
+#pragma unroll 1
+        for (int sub = 0; sub < SUB; sub += UNR) {
+            bool alive[UNR], ev[UNR];
+            double x[UNR], y[UNR], z[UNR], ux[UNR], uy[UNR], uz[UNR], tau[UNR], delta[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const long long i = base + (long long)(sub + u) * SFP_TILE + threadIdx.x;
+                alive[u] = (i < N) && (S.pruned[i] == 0);
+                ev[u] = false;
+                delta[u] = tau[u] = 0.0;
+                x[u] = y[u] = z[u] = ux[u] = uy[u] = uz[u] = 0.0;
+                if (alive[u]) {
+                    x[u] = S.x[i]; y[u] = S.y[i]; z[u] = S.z[i];
+                    ux[u] = S.ux[i]; uy[u] = S.uy[i]; uz[u] = S.uz[i];
+                    if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau[u] = S.tau[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const long long i = base + (long long)(sub + u) * SFP_TILE + threadIdx.x;
+                if (alive[u] && S.bw)
+                    ev[u] = sfp_pair_event<FORM, QED>(R, T, S, I, P, x[u], y[u], z[u], ux[u], uy[u], uz[u], t, step, i,
+                                                      tau[u], delta[u]);
+                const unsigned int bal = __ballot_sync(0xffffffffu, ev[u]);
+                if (ev[u]) {
+                    const unsigned int r = __popc(bal & lt);
+                    s_evd[warp][wn + r] = delta[u];
+                    s_evi[warp][wn + r] = ((unsigned int)(sub + u) << 16) | (r << 5) | (unsigned int)lane;
+                    S.pruned[i] = 1;  // converted photons are pruned, not pushed (cpu.py:190)
+                } else if (alive[u]) {
+                    if (S.push) {
+                        if (FORM == SFP_FORM_FP64) push_photon(x[u], y[u], z[u], ux[u], uy[u], uz[u], dt);
+                        else push_photon32(x[u], y[u], z[u], ux[u], uy[u], uz[u], dt);
+                        S.x[i] = x[u]; S.y[i] = y[u]; S.z[i] = z[u];
+                    }
+                }
+                if (QED == SFP_QED_OPTICAL_DEPTH && alive[u] && S.tau && S.bw) S.tau[i] = tau[u];
+                if (lane == 0) s_cnt[sub + u][warp] = __popc(bal);
+                wn += __popc(bal);
+            }
+        }
+        if (!any_appends) continue;
+        __syncthreads();
+        if (warp == 0) {
+            // exclusive scan over the (sub, warp) groups in index order: two per lane
+            constexpr int G = SUB * NW;
+            unsigned int a = (2 * lane < G) ? s_cnt[(2 * lane) / NW][(2 * lane) % NW] : 0u;
+            unsigned int b = (2 * lane + 1 < G) ? s_cnt[(2 * lane + 1) / NW][(2 * lane + 1) % NW] : 0u;
+            const unsigned int pair = a + b;
+            unsigned int inc = pair;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int n2 = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += n2;
+            }
+            const unsigned int total = __shfl_sync(0xffffffffu, inc, 31);
+            const unsigned int ex0 = inc - pair;
+            if (2 * lane < G) s_cnt[(2 * lane) / NW][(2 * lane) % NW] = ex0;
+            if (2 * lane + 1 < G) s_cnt[(2 * lane + 1) / NW][(2 * lane + 1) % NW] = ex0 + a;
+            uint4 agg{0u, 0u, 0u, 0u};
+            if (S.bw) agg = u4_one(S.channel, total);
+            if (lane == 0 && total) {
+                atomicAdd(&R->appended[S.ele_dest], (unsigned long long)total);
+                atomicAdd(&R->appended[S.pos_dest], (unsigned long long)total);
+            }
+            const long long ft = flag0 + tile;
+            const long long first = R->chain_first[si];
+            uint4 ex{0u, 0u, 0u, 0u};
+            if (ft == first) {
+                publish(R, ft, agg, epoch, true);
+            } else {
+                publish(R, ft, agg, epoch, false);
+                if (!lookback_try(R, ft, first, epoch, ex)) ex = lookback_wait(R, ft, first, epoch);
+                publish(R, ft, u4_add(ex, agg), epoch, true);
+            }
+            if (lane == 0) s_excl = ex;
+        }
+        __syncthreads();
+        // e- (delta) and e+ (1 - delta) children (cpu.py:119-189), unpushed;
+        // the children kernel pushes them after this kernel
+        if (wn) {
+            const long long ch_base = (long long)u4_get(s_excl, S.channel);
+            const sfp_segment& De = R->seg[S.ele_dest];
+            const sfp_segment& Dp = R->seg[S.pos_dest];
+            const long long be = R->n_buf_step[S.ele_dest] + ch_base;
+            const long long bp = R->n_buf_step[S.pos_dest] + ch_base;
+            for (unsigned int e = lane; e < wn; e += 32) {
+                const unsigned int code = s_evi[warp][e];
+                const int sb = (int)(code >> 16), r = (int)((code >> 5) & 0x7FFu), ln = (int)(code & 31u);
+                const double d = s_evd[warp][e];
+                const long long i = base + (long long)sb * SFP_TILE + warp * 32 + ln;
+                const long long rank = (long long)s_cnt[sb][warp] + r;
+                const double px = S.x[i], py = S.y[i], pz = S.z[i], pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
+                const double d2 = 1.0 - d;
+                long long slot = be + rank;
+                De.x[slot] = px; De.y[slot] = py; De.z[slot] = pz;
+                De.ux[slot] = d * pux; De.uy[slot] = d * puy; De.uz[slot] = d * puz;
+                if (De.spin) { De.sx[slot] = 0.0; De.sy[slot] = 0.0; De.sz[slot] = 0.0; }
+                if (De.tau) De.tau[slot] = 0.0;
+                De.pruned[slot] = 0;
+                slot = bp + rank;
+                Dp.x[slot] = px; Dp.y[slot] = py; Dp.z[slot] = pz;
+                Dp.ux[slot] = d2 * pux; Dp.uy[slot] = d2 * puy; Dp.uz[slot] = d2 * puz;
+                if (Dp.spin) { Dp.sx[slot] = 0.0; Dp.sy[slot] = 0.0; Dp.sz[slot] = 0.0; }
+                if (Dp.tau) Dp.tau[slot] = 0.0;
+                Dp.pruned[slot] = 0;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pair children of this step, pushed from t to t+dt like every other pushed
+// particle (simulation.py:128-137).  They occupy [n_buf_step, n_buf_step +
+// appended) of each pair-destination segment.
+// ---------------------------------------------------------------------------
+template <int FORM>
+__device__ __forceinline__ void sfp_children_body(const sfp_run_dev* __restrict__ R) {
+    using namespace sfp;
+    sfp_step_state* st = R->st;
+    if (st->skip) return;
+    const double t = st->t;
+    const double dt = R->dt;
+    const long long gsize = (long long)gridDim.x * blockDim.x;
+    for (int c = 0; c < R->n_cseg; ++c) {
+        const int si = R->cseg[c];
+        const sfp_segment& S = R->seg[si];
+        if (!S.push) continue;
+        const long long cnt = (long long)R->appended[si];
+        const long long start = R->n_buf_step[si];
+        const double* __restrict__ P = R->inst[S.instance].field_params;
+        for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < cnt; j += gsize) {
+            const long long i = start + j;
+            double x = S.x[i], y = S.y[i], z = S.z[i], ux = S.ux[i], uy = S.uy[i], uz = S.uz[i];
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            S.x[i] = x; S.y[i] = y; S.z[i] = z;
+            S.ux[i] = ux; S.uy[i] = uy; S.uz[i] = uz;
+        }
+    }
+}
+
+// kernels: sfp_{massive,photon}_<form>_<qed>_<variant>, sfp_children_<form>
+#ifndef SFP_PHOTON_SUB
+#define SFP_PHOTON_SUB 8
+#endif
+#define SFP_MASSIVE_KERNEL(FORM_S, QED_S, FORM, QED, ITEMS, MINB)                                              \
+    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
+        sfp_massive_##FORM_S##_##QED_S##_i##ITEMS##_b##MINB(const sfp_run_dev* __restrict__ R) {              \
+        sfp_massive_body<FORM, QED, ITEMS>(R);                                                               \
+    }
+#define SFP_PHOTON_KERNEL(FORM_S, QED_S, FORM, QED, UNR, MINB)                                                 \
+    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
+        sfp_photon_##FORM_S##_##QED_S##_u##UNR##_b##MINB(const sfp_run_dev* __restrict__ R) {                 \
+        sfp_photon_body<FORM, QED, SFP_PHOTON_SUB, UNR>(R);                                                  \
     }
 
-#if defined(SFP_STEP_FORM_FP64) && defined(SFP_STEP_QED_RS)
-SFP_STEP_KERNEL(sfp_step_fp64_rs_i1_b2, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 2)
-SFP_STEP_KERNEL(sfp_step_fp64_rs_i1_b3, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 3)
-SFP_STEP_KERNEL(sfp_step_fp64_rs_i2_b2, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+#if defined(SFP_STEP_FORM_FP64)
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_children_fp64(const sfp_run_dev* __restrict__ R) {
+    sfp_children_body<SFP_FORM_FP64>(R);
+}
+#if defined(SFP_STEP_QED_RS)
+SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 2)
+SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 3)
+SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+#else
+SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 2)
+SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 3)
+SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
 #endif
-#if defined(SFP_STEP_FORM_FP64) && defined(SFP_STEP_QED_OD)
-SFP_STEP_KERNEL(sfp_step_fp64_od_i1_b2, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 2)
-SFP_STEP_KERNEL(sfp_step_fp64_od_i2_b2, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
 #endif
-#if defined(SFP_STEP_FORM_FP32) && defined(SFP_STEP_QED_RS)
-SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b2, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 2)
-SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b3, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 3)
-SFP_STEP_KERNEL(sfp_step_fp32_rs_i1_b4, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
-SFP_STEP_KERNEL(sfp_step_fp32_rs_i2_b2, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 2)
-SFP_STEP_KERNEL(sfp_step_fp32_rs_i2_b3, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+#if defined(SFP_STEP_FORM_FP32)
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_children_fp32(const sfp_run_dev* __restrict__ R) {
+    sfp_children_body<SFP_FORM_FP32>(R);
+}
+#if defined(SFP_STEP_QED_RS)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 3)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 2)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 3)
+#else
+SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 3)
+SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 4)
+SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 3)
 #endif
-#if defined(SFP_STEP_FORM_FP32) && defined(SFP_STEP_QED_OD)
-SFP_STEP_KERNEL(sfp_step_fp32_od_i1_b3, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 3)
-SFP_STEP_KERNEL(sfp_step_fp32_od_i2_b2, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 2)
 #endif
 #endif  // SFP_WANT_STEP
 

@@ -9,9 +9,11 @@ generates QED events, appends photons then pairs, and pushes every pushed
 particle (children included) from t to t+dt (simulation.py:102-144);
 ``start`` ends by pruning and returning host arrays (simulation.py:158-161).
 
-Each step is ONE launch of the fused kernel over all species (plus a
-one-block bookkeeping launch); steps between progress reports / callbacks
-run back to back on the device, replayed from CUDA graphs, with no host
+Each step is three persistent launches over all species -- the massive
+kernel (e+-: emission, recoil, push, photon children), the photon kernel
+(pair creation, photon push) and the pair-children push -- after a one-block
+bookkeeping launch; steps between progress reports / callbacks run back to
+back on the device, replayed from CUDA graphs, with no host
 synchronisation.  The kernel never overruns a buffer: a device-side guard
 skips the step when a destination lacks room for the worst case (every
 emitter emits), and the host then grows that buffer by the reference rule
@@ -21,8 +23,10 @@ Extra keyword arguments (no reference counterpart):
   seed        -- 64-bit key of the Philox streams (default: random);
   form        -- 'fp64' (plain float64, the reference arithmetic) or 'fp32';
   graph_chunk -- steps per captured CUDA graph (0 disables graphs);
-  items, min_blocks -- step-kernel variant: particles per thread per tile
-                 and minimum resident blocks per SM (see autotune.py).
+  items, min_blocks -- massive-kernel variant: particles per thread per
+                 tile and minimum resident blocks per SM (see autotune.py);
+  p_unroll, p_min_blocks -- photon-kernel variant: sub-tiles in flight per
+                 thread and minimum resident blocks per SM.
 """
 from __future__ import annotations
 
@@ -46,7 +50,7 @@ except Exception:  # pragma: no cover
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
-                 items: int = 0, min_blocks: int = 0) -> None:
+                 items: int = 0, min_blocks: int = 0, p_unroll: int = 0, p_min_blocks: int = 0) -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -63,8 +67,10 @@ class Simulation(object):
             raise ValueError("form must be 'fp64' or 'fp32'")
         self.form = form
         self.graph_chunk = int(graph_chunk)
-        self.items = int(items)  # particles per thread per tile (0: the form's default)
-        self.min_blocks = int(min_blocks)  # kernel variant: resident blocks per SM (0: default)
+        self.items = int(items)  # massive kernel: particles per thread per tile (0: the form's default)
+        self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
+        self.p_unroll = int(p_unroll)  # photon kernel: sub-tiles in flight per thread (0: default)
+        self.p_min_blocks = int(p_min_blocks)  # photon kernel: resident blocks per SM (0: default)
         self.particle_steps = 0  # sum over executed steps of all species' N_buffered
         self.kernel_launches = 0  # libsfp kernels launched by start()/run_on_device()
         self._run = None
@@ -83,9 +89,12 @@ class Simulation(object):
         if len(ods) > 1:
             raise ValueError("all QED species of a simulation must use the same event method")
         self.qed_method = "od" if ods == {True} else "rs"
+        from .autotune import DEFAULT
+        dm, dp = DEFAULT[(self.form, self.qed_method)]
         if self.items <= 0 or self.min_blocks <= 0:
-            from .autotune import DEFAULT
-            self.items, self.min_blocks = DEFAULT[(self.form, self.qed_method)]
+            self.items, self.min_blocks = dm
+        if self.p_unroll <= 0 or self.p_min_blocks <= 0:
+            self.p_unroll, self.p_min_blocks = dp
 
     # ------------------------------------------------------------------
     def _index(self, p):
@@ -168,6 +177,8 @@ class Simulation(object):
         cfg.form = _lib.SFP_FORM_FP32 if self.form == "fp32" else _lib.SFP_FORM_FP64
         cfg.items = self.items
         cfg.min_blocks = self.min_blocks
+        cfg.p_unroll = self.p_unroll
+        cfg.p_min_blocks = self.p_min_blocks
         if self.qed_method == "od":
             cfg.od_photon, cfg.od_pair = device_tables.od_tables(dev)
         else:
@@ -223,9 +234,14 @@ class Simulation(object):
         self._run = None
         self._keep = None
 
-    def set_kernel(self, items: int, min_blocks: int):
-        """Switch the step-kernel variant of a device-resident run."""
-        self.items, self.min_blocks = int(items), int(min_blocks)
+    def set_kernel(self, massive=None, photon=None):
+        """Switch the kernel variants of a device-resident run: `massive` =
+        (items, min_blocks), `photon` = (p_unroll, p_min_blocks); None keeps
+        the current one."""
+        if massive is not None:
+            self.items, self.min_blocks = int(massive[0]), int(massive[1])
+        if photon is not None:
+            self.p_unroll, self.p_min_blocks = int(photon[0]), int(photon[1])
         if getattr(self, "_run", None) is not None:
             self._end()
             self._begin()
@@ -245,9 +261,10 @@ class Simulation(object):
             p._to_host()
 
     def time_step_kernel(self, nstep: int):
-        """Advance `nstep` steps with one eager launch each and return the
-        CUDA-event durations [ms] of the step-kernel launches (recorded on the
-        stream they run on), with the buffered counts before and after."""
+        """Advance `nstep` steps with eager launches and return, per step, the
+        CUDA-event durations [ms] of its (massive, photon, pair-children)
+        kernels (recorded on the stream they run on; 0 for a kernel the run
+        does not launch), with the buffered counts before and after."""
         if getattr(self, "_run", None) is None:
             self._begin()
         before = [p.N_buffered for p in self.all_particles]
@@ -258,7 +275,7 @@ class Simulation(object):
         for _ in range(int(nstep)):
             if self._ensure_headroom():
                 self._update_run(self._run)
-            ms = (ctypes.c_float * 1)()
+            ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             if st.error or st.halted:
@@ -266,12 +283,19 @@ class Simulation(object):
             for i, p in enumerate(self.all_particles):
                 p.N_buffered = int(nbuf[i])
                 p._touch()
-            self.kernel_launches += 3
-            out.append(float(ms[0]))
+            self.kernel_launches += self._launches_per_step() + 1
+            out.append((float(ms[0]), float(ms[1]), float(ms[2])))
         self.particle_steps = self._ps_base + int(st.particle_steps)
         self.step = int(st.step)
         self.t = float(st.t)
         return out, before, [p.N_buffered for p in self.all_particles]
+
+    def _launches_per_step(self):
+        """libsfp kernels one step launches: bookkeeping + the massive,
+        photon and pair-children kernels that have species to work on."""
+        ps = self.all_particles
+        return (1 + any(p.m != 0 for p in ps) + any(p.m == 0 for p in ps)
+                + any(p.bw for p in ps))
 
     def _loop(self, run, nstep, call_back):
         L = _lib.load()
@@ -290,7 +314,7 @@ class Simulation(object):
                 self._update_run(run)
             _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
-            self.kernel_launches += 2 * chunk + 1
+            self.kernel_launches += self._launches_per_step() * chunk + 1
             _lib.check(L.sfp_run_read_state(run, ctypes.byref(st), nbuf, _stream_ptr()), "sfp_run_read_state")
             if st.error:
                 raise _lib.SFPError(f"device error in the step kernel: {_lib.DEV_ERRORS.get(st.error, st.error)}")

@@ -312,26 +312,38 @@ def test_repeated_start_continues_the_run():
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])
-def test_kernel_variants_give_identical_results(form):
-    """Every step-kernel variant (items per thread, register budget) computes
-    the same arithmetic in the same append order: identical results."""
+def test_kernel_variants_give_the_same_results(form):
+    """Every variant of the massive kernel (items per thread, register
+    budget) and of the photon kernel (sub-tiles in flight, register budget)
+    computes the same arithmetic in the same append order: the same event
+    counts and the same states up to the compiler's different FMA
+    contraction per variant (1e-10 relative in float64, 1e-4 in float32)."""
     cuda_or_skip()
+    import itertools
     import sfparticles_b200 as S
     from sfparticles_b200.autotune import VARIANTS
     g = golden("ref_sim_cascade.npz")
     case = json.loads(str(g["case"]))
+    mv, pv = VARIANTS[(form, "rs")]
+    bound = 1e-10 if form == "fp64" else 1e-4
     ref = None
-    for items, minb in VARIANTS[(form, "rs")]:
+    for m, p in itertools.zip_longest(mv, pv, fillvalue=None):
+        m = m or mv[0]
+        p = p or pv[0]
         species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
         sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
-                           photon_threshold=case["thr"], seed=case["seed"], form=form, items=items, min_blocks=minb)
+                           photon_threshold=case["thr"], seed=case["seed"], form=form, items=m[0], min_blocks=m[1],
+                           p_unroll=p[0], p_min_blocks=p[1])
         sim.start(case["steps"])
-        got = [np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")]) for p in species]
+        got = [np.stack([getattr(q, k) for k in ("x", "y", "z", "ux", "uy", "uz")]) for q in species]
         if ref is None:
             ref = got
-        else:
-            for a, b in zip(got, ref):
-                np.testing.assert_array_equal(a, b)
+            continue
+        for a, b in zip(got, ref):
+            assert a.shape == b.shape, (m, p, a.shape, b.shape)
+            err = _rel(a, b)
+            print(f"{form} massive {m} photon {p}: max rel diff {err:.2e}")
+            assert err < bound, (m, p, err)
 
 
 def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
@@ -347,7 +359,9 @@ def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
     sim.run_on_device(100)
     step, t = sim.step, sim.t
     best, times = autotune.tune(sim, sample=10_000, steps=2)
-    assert best in autotune.VARIANTS[("fp32", "rs")] and len(times) == len(autotune.VARIANTS[("fp32", "rs")])
+    mv, pv = autotune.VARIANTS[("fp32", "rs")]
+    assert tuple(best[0]) in mv and tuple(best[1]) in pv and len(times) == len(mv) + len(pv)
+    assert (sim.items, sim.min_blocks) == tuple(best[0]) and (sim.p_unroll, sim.p_min_blocks) == tuple(best[1])
     assert (sim.step, sim.t) == (step, t)  # tuning ran on a copy
     assert os.path.exists(os.path.join(str(tmp_path), "autotune.json"))
     sim.run_on_device(10)
