@@ -94,6 +94,19 @@ int sfp_bool_sum(const uint8_t *event, int64_t N, int64_t *count, void *stream);
 size_t sfp_find_event_index_workspace(int64_t N);
 int sfp_find_event_index(const uint8_t *event, int64_t N_event, int64_t N, int64_t *index, void *workspace,
                          size_t workspace_bytes, void *stream);
+/* find_event_index without a workspace and without any allocation.  No
+ * counterpart in the reference: for callers that cannot allocate device
+ * memory on demand (memory owned by a pool or caching allocator sized at
+ * start-up; code that must not stall, as cudaMalloc / cudaFree synchronise
+ * the device).  Same result as sfp_find_event_index.  Its scratch is a fixed
+ * 512 KiB array in the library's device image, held on every GPU that loads
+ * the library until exit, so N <= SFP_FEI_NOALLOC_MAX_N (2^28); larger N is
+ * rejected with SFP_EINVAL.  The first call with a device current looks up
+ * that device's scratch address (a call with N = 0 does only this); make it
+ * before any stream capture.  Calls in flight at once on one device (other
+ * streams or threads) share the scratch and race. */
+#define SFP_FEI_NOALLOC_MAX_N (1LL << 28)
+int sfp_find_event_index_noalloc(const uint8_t *event, int64_t N_event, int64_t N, int64_t *index, void *stream);
 /* create_photon, cpu.py:89-116 */
 int sfp_create_photon(const double *x_src, const double *y_src, const double *z_src, const double *ux_src,
                       const double *uy_src, const double *uz_src, double *x_dst, double *y_dst, double *z_dst,

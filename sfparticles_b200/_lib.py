@@ -87,6 +87,7 @@ _SIGS = {
     "sfp_bool_sum": ([P, c_i64, P, P], c_i32),
     "sfp_find_event_index_workspace": ([c_i64], c_sz),
     "sfp_find_event_index": ([P, c_i64, c_i64, P, P, c_sz, P], c_i32),
+    "sfp_find_event_index_noalloc": ([P, c_i64, c_i64, P, P], c_i32),
     "sfp_create_photon": ([P] * 16 + [c_i64, c_i64, P], c_i32),
     "sfp_create_pair": ([P] * 17 + [c_i64, c_i64, c_i32, P], c_i32),
     "sfp_photon_from_rejection_sampling": ([P, P, c_d, c_i64, P, P, P, P, c_u64, c_u32, c_u32, P], c_i32),

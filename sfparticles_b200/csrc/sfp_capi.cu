@@ -352,6 +352,52 @@ __global__ void k_inv_gamma(const double* __restrict__ ux, const double* __restr
 
 }  // namespace
 
+// ============== find_event_index without allocation (scratch) ===============
+//
+// sfp_find_event_index needs a scratch array of one count per 4096-entry
+// chunk of the event mask, and asks its caller for it.  Some callers cannot
+// provide device memory on demand: their device memory belongs to a pool or
+// a caching allocator sized at start-up (cudaMalloc beside it fails or
+// fragments the pool), or they must not stall, and cudaMalloc / cudaFree
+// synchronise the whole device.  For them the scratch is a fixed array in
+// the library's own device image instead: 65536 chunk counts (512 KiB), so
+// at most 65536 * 4096 = 2^28 entries per call.  Every GPU on which this
+// library's device code is loaded holds the 512 KiB until the process exits.
+#define SFP_FEI_NOALLOC_CHUNKS 65536
+static_assert((long long)SFP_FEI_NOALLOC_CHUNKS * kChunk == SFP_FEI_NOALLOC_MAX_N,
+              "scratch size and the declared maximum disagree");
+static __device__ __align__(256) long long g_fei_noalloc_scratch[SFP_FEI_NOALLOC_CHUNKS];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_fei_noalloc_mu;
+long long* g_fei_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch on the current device.  Looked up once per
+// device, by the first call made with that device current; later calls on
+// that device reuse the cached address.
+int fei_noalloc_scratch(long long** out) {
+    int dev = -1;
+    SFP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail(SFP_EINVAL, "sfp_find_event_index_noalloc: device index " + std::to_string(dev) +
+                                    " beyond the supported 64 devices");
+    std::lock_guard<std::mutex> g(g_fei_noalloc_mu);
+    if (!g_fei_noalloc_ptr[dev]) {
+        long long* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_fei_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(SFP_ECUDA, std::string("sfp_find_event_index_noalloc: cudaGetSymbolAddress of the scratch "
+                                               "failed: ") + cudaGetErrorString(e));
+        g_fei_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_fei_noalloc_ptr[dev];
+    return SFP_OK;
+}
+
+}  // namespace
+
 // ================================ C-ABI ======================================
 
 struct sfp_module {
@@ -560,6 +606,34 @@ int sfp_find_event_index(const uint8_t* ev, int64_t N_event, int64_t N, int64_t*
     if (!ws || ws_bytes < (size_t)nb * sizeof(long long))
         return fail(SFP_EINVAL, "sfp_find_event_index: workspace too small");
     long long* counts = static_cast<long long*>(ws);
+    cudaStream_t s = as_stream(stream);
+    k_fei_count<<<(unsigned int)nb, kBlock, 0, s>>>(ev, N, counts);
+    SFP_CHECK_LAUNCH();
+    k_fei_scan<<<1, 1024, 0, s>>>(counts, nb);
+    SFP_CHECK_LAUNCH();
+    k_fei_scatter<<<(unsigned int)nb, kBlock, 0, s>>>(ev, N, counts, reinterpret_cast<long long*>(index), N_event);
+    SFP_CHECK_LAUNCH();
+    return SFP_OK;
+}
+
+// Same three kernels as sfp_find_event_index, with the file-scope scratch in
+// place of the caller's workspace.  Allocates nothing.  Nothing in the
+// scratch has to start at zero: k_fei_count writes every chunk count that
+// k_fei_scan and k_fei_scatter then read.  The scratch is shared by all
+// calls on a device, so two calls in flight at once on one device (on
+// different streams, or from different host threads) race; calls queued on
+// one stream run one after the other and do not.
+int sfp_find_event_index_noalloc(const uint8_t* ev, int64_t N_event, int64_t N, int64_t* index, void* stream) {
+    if (N > SFP_FEI_NOALLOC_MAX_N)
+        return fail(SFP_EINVAL, "sfp_find_event_index_noalloc: N = " + std::to_string((long long)N) +
+                                    " exceeds the maximum of 268435456 (2^28) entries; use sfp_find_event_index "
+                                    "with a caller workspace");
+    // set-up first, so that a call with N = 0 performs only the set-up
+    long long* counts = nullptr;
+    const int rc = fei_noalloc_scratch(&counts);
+    if (rc) return rc;
+    if (N <= 0 || N_event <= 0) return SFP_OK;
+    const long long nb = (N + kChunk - 1) / kChunk;
     cudaStream_t s = as_stream(stream);
     k_fei_count<<<(unsigned int)nb, kBlock, 0, s>>>(ev, N, counts);
     SFP_CHECK_LAUNCH();
