@@ -153,7 +153,7 @@ typedef struct sfp_run_config {
     int32_t form;            /* SFP_FORM_*                                 */
     int32_t items;           /* massive kernel: particles per thread per tile (0 = default) */
     int32_t min_blocks;      /* massive kernel: min resident blocks per SM (0 = default)    */
-    int32_t p_unroll;        /* photon kernel: sub-tiles in flight per thread (0 = default) */
+    int32_t p_stages;        /* photon kernel: depth of the copy ring, 2..4 (0 = default)   */
     int32_t p_min_blocks;    /* photon kernel: min resident blocks per SM (0 = default)     */
     sfp_rs_table rs;
     sfp_od_table od_photon;
@@ -170,9 +170,9 @@ int sfp_run_update(sfp_run *r, int n_seg, const sfp_segment *seg, const int64_t 
 int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
 /* like sfp_run_steps without graphs, with CUDA events recorded around each
  * of the three kernels of every step on the run's stream; synchronous.
- * kernel_ms[3*i + k] is the duration of step i's massive (k=0), photon (k=1)
- * and pair-children (k=2) kernel; 0 for a kernel the run does not launch
- * (3*nsteps entries). */
+ * kernel_ms[3*i + k] is the duration of step i's massive (k=0) and photon
+ * (k=1) kernels and of its pair scan + pairs kernels (k=2); 0 for kernels
+ * the run does not launch (3*nsteps entries). */
 int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stream);
 /* synchronous: state and per-segment buffered counts (n_seg entries) */
 int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);

@@ -48,6 +48,8 @@ typedef struct sfp_segment {
     double *x, *y, *z, *ux, *uy, *uz;
     double *sx, *sy, *sz; /* NULL unless spin (SpinParticles)              */
     double *tau;          /* NULL unless the optical-depth method is used  */
+    double *delta;        /* pair-creating photons: pair_delta, the delta of
+                             this step's pair events (NULL otherwise)       */
     sfp_u8 *pruned;       /* _to_be_pruned                                 */
     sfp_i64 capacity;     /* buffer_size                                   */
     double q;             /* charge [C]                                    */

@@ -27,7 +27,7 @@ c_d, c_i64, c_i32, c_u32, c_u64, c_sz, P = (ctypes.c_double, ctypes.c_int64, cty
 class Segment(ctypes.Structure):
     _fields_ = [
         ("x", P), ("y", P), ("z", P), ("ux", P), ("uy", P), ("uz", P),
-        ("sx", P), ("sy", P), ("sz", P), ("tau", P), ("pruned", P),
+        ("sx", P), ("sy", P), ("sz", P), ("tau", P), ("delta", P), ("pruned", P),
         ("capacity", c_i64), ("q", c_d), ("ae", c_d),
         ("massless", c_i32), ("push", c_i32), ("rr", c_i32), ("spin", c_i32),
         ("radiating", c_i32), ("bw", c_i32), ("photon_dest", c_i32), ("ele_dest", c_i32), ("pos_dest", c_i32),
@@ -57,7 +57,7 @@ class RunState(ctypes.Structure):
 
 class RunConfig(ctypes.Structure):
     _fields_ = [("dt", c_d), ("photon_threshold", c_d), ("t0", c_d), ("step0", c_i64), ("qed", c_i32), ("form", c_i32),
-                ("items", c_i32), ("min_blocks", c_i32), ("p_unroll", c_i32), ("p_min_blocks", c_i32),
+                ("items", c_i32), ("min_blocks", c_i32), ("p_stages", c_i32), ("p_min_blocks", c_i32),
                 ("rs", RSTable), ("od_photon", ODTable),
                 ("od_pair", ODTable)]
 

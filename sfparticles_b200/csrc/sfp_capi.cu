@@ -713,18 +713,21 @@ int sfp_inv_gamma(const double* ux, const double* uy, const double* uz, double* 
 
 // ================================ runs =======================================
 //
-// One step = book(prepare) + massive + photon + children launches on the
-// run's stream.  The massive and photon kernels are persistent grids that
-// take tiles by ticket; the children kernel is a grid-stride push.
+// One step = book(prepare) + massive + photon [+ pair scan + pairs] launches
+// on the run's stream.  The massive and photon kernels are persistent grids
+// that take tiles by ticket; the pair scan is one block; the pairs kernel is
+// a grid over the photon-tile counters.
 
-// photon-group tile: SFP_PHOTON_SUB_HOST sub-tiles of SFP_TILE_HOST photons
-#define SFP_PHOTON_SUB_HOST 8
+// photon (warp) tile: SFP_PHOTON_WSUB_HOST sub-steps of 32 photons; the NVRTC
+// modules are built with SFP_PHOTON_WSUB equal to it
+#define SFP_PHOTON_WSUB_HOST 32
+#define SFP_SUPER_TILE_HOST 64
 
 struct sfp_run {
     sfp_module* mod = nullptr;
-    cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_children = nullptr, k_book = nullptr;
+    cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_pairs = nullptr, k_book = nullptr;
     int grid_m = 0, grid_p = 0, grid_c = 0;
-    size_t smem = 0;
+    size_t smem_m = 0, smem_p = 0;
     cudaStream_t s = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int n_seg = 0, n_inst = 0;
@@ -732,30 +735,54 @@ struct sfp_run {
     sfp_run_dev* d = nullptr;
     std::map<int, cudaGraphExec_t> graphs;
     std::vector<sfp_segment> segs;
+    std::vector<sfp_instance> insts;
     std::vector<int> mseg, pseg, cseg;
 };
 
-// look-back flags needed: tiles of both groups at full capacity, plus slack
-static long long tiles_for(const sfp_run* r) {
+// massive tiles (look-back flags) and photon tiles (event counters) at full
+// capacity, plus slack; photon segments start at multiples of a super-tile
+static long long mtiles_for(const sfp_run* r) {
     long long t = 0;
     for (int s : r->mseg) t += (r->segs[s].capacity + r->h.mtile - 1) / r->h.mtile;
-    for (int s : r->pseg) t += (r->segs[s].capacity + r->h.ptile - 1) / r->h.ptile;
     return t + (long long)r->segs.size() + 1;
 }
+static long long ptiles_for(const sfp_run* r) {
+    long long t = 0;
+    for (int s : r->pseg) t += (r->segs[s].capacity + r->h.ptile - 1) / r->h.ptile + SFP_SUPER_TILE_HOST;
+    return t + 1;
+}
 
-static int run_alloc_tiles(sfp_run* r, long long need) {
-    if (need <= r->h.max_tiles) return SFP_OK;
-    long long n = need + need / 4 + 64;
-    if (r->h.tile_flag) cudaFree(r->h.tile_flag);
-    if (r->h.tile_agg) cudaFree(r->h.tile_agg);
-    if (r->h.tile_incl) cudaFree(r->h.tile_incl);
-    r->h.tile_flag = nullptr;
-    r->h.tile_agg = r->h.tile_incl = nullptr;
-    SFP_CUDA(cudaMalloc(&r->h.tile_flag, n * sizeof(unsigned int)));
-    SFP_CUDA(cudaMalloc(&r->h.tile_agg, n * sizeof(uint4)));
-    SFP_CUDA(cudaMalloc(&r->h.tile_incl, n * sizeof(uint4)));
-    SFP_CUDA(cudaMemsetAsync(r->h.tile_flag, 0, n * sizeof(unsigned int), r->s));
-    r->h.max_tiles = n;
+static int run_alloc_tiles(sfp_run* r) {
+    const long long need_m = mtiles_for(r), need_p = ptiles_for(r);
+    if (need_m > r->h.max_tiles) {
+        const long long n = need_m + need_m / 4 + 64;
+        if (r->h.tile_flag) cudaFree(r->h.tile_flag);
+        if (r->h.tile_agg) cudaFree(r->h.tile_agg);
+        if (r->h.tile_incl) cudaFree(r->h.tile_incl);
+        r->h.tile_flag = nullptr;
+        r->h.tile_agg = r->h.tile_incl = nullptr;
+        r->h.max_tiles = 0;
+        SFP_CUDA(cudaMalloc(&r->h.tile_flag, n * sizeof(unsigned int)));
+        SFP_CUDA(cudaMalloc(&r->h.tile_agg, n * sizeof(uint4)));
+        SFP_CUDA(cudaMalloc(&r->h.tile_incl, n * sizeof(uint4)));
+        SFP_CUDA(cudaMemsetAsync(r->h.tile_flag, 0, n * sizeof(unsigned int), r->s));
+        r->h.max_tiles = n;
+    }
+    if (need_p > r->h.max_ptiles) {
+        const long long n = need_p + need_p / 4 + 64;
+        const long long ns = n / SFP_SUPER_TILE_HOST + 2;
+        if (r->h.ptile_cnt) cudaFree(r->h.ptile_cnt);
+        if (r->h.psuper_cnt) cudaFree(r->h.psuper_cnt);
+        if (r->h.psuper_pre) cudaFree(r->h.psuper_pre);
+        r->h.ptile_cnt = nullptr;
+        r->h.psuper_cnt = nullptr;
+        r->h.psuper_pre = nullptr;
+        r->h.max_ptiles = 0;
+        SFP_CUDA(cudaMalloc(&r->h.ptile_cnt, n * sizeof(unsigned int)));
+        SFP_CUDA(cudaMalloc(&r->h.psuper_cnt, ns * sizeof(unsigned int)));
+        SFP_CUDA(cudaMalloc(&r->h.psuper_pre, ns * sizeof(long long)));
+        r->h.max_ptiles = n;
+    }
     return SFP_OK;
 }
 
@@ -778,6 +805,15 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
         if (S.capacity > 0 && S.spin && (!S.sx || !S.sy || !S.sz))
             return fail(SFP_EINVAL, "spin segment without spin arrays");
         if (S.channel < 0 || S.channel >= SFP_MAX_CHANNELS) return fail(SFP_EINVAL, "append channel out of range");
+        // the photon kernel streams photon state with 16-byte asynchronous copies
+        if (S.massless && S.capacity > 0) {
+            const void* a[] = {S.x, S.y, S.z, S.ux, S.uy, S.uz, S.pruned, S.tau};
+            for (const void* p : a)
+                if (p && (reinterpret_cast<uintptr_t>(p) & 15u))
+                    return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": photon arrays must be 16-byte aligned");
+            if (S.bw && !S.delta)
+                return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": pair-creating photons need a delta array");
+        }
         // the massive kernel handles emission, the photon kernel pair creation
         if (S.massless && S.radiating) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": a photon cannot radiate");
         if (!S.massless && S.bw) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": only photons create pairs");
@@ -828,16 +864,16 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     const bool f64 = cfg->form == SFP_FORM_FP64;
     const int items = cfg->items > 0 ? cfg->items : (f64 ? 1 : 1);
     const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (f64 ? 2 : 3);
-    const int unr = cfg->p_unroll > 0 ? cfg->p_unroll : (f64 ? 1 : 2);
+    const int stages = cfg->p_stages > 0 ? cfg->p_stages : 3;
     const int pminb = cfg->p_min_blocks > 0 ? cfg->p_min_blocks : (f64 ? 3 : 4);
-    if (items < 1 || items > 4 || minb < 1 || minb > 8 || unr < 1 || unr > SFP_PHOTON_SUB_HOST ||
-        SFP_PHOTON_SUB_HOST % unr != 0 || pminb < 1 || pminb > 8)
+    if (items < 1 || items > 4 || minb < 1 || minb > 8 || stages < 2 || stages > 4 || pminb < 1 || pminb > 8)
         return fail(SFP_EINVAL, "kernel variant out of range");
     auto* r = new sfp_run();
     r->mod = m;
     r->n_seg = n_seg;
     r->n_inst = n_inst;
     r->segs.assign(seg, seg + n_seg);
+    r->insts.assign(inst, inst + n_inst);
     for (int s = 0; s < n_seg; ++s) {
         (seg[s].massless ? r->pseg : r->mseg).push_back(s);
         bool dest = false;
@@ -847,10 +883,12 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     }
     const std::string fq = std::string(f64 ? "fp64_" : "fp32_") + (cfg->qed == SFP_QED_REJECTION ? "rs" : "od");
     const std::string km = "sfp_massive_" + fq + "_i" + std::to_string(items) + "_b" + std::to_string(minb);
-    const std::string kp = "sfp_photon_" + fq + "_u" + std::to_string(unr) + "_b" + std::to_string(pminb);
-    const std::string kc = f64 ? "sfp_children_fp64" : "sfp_children_fp32";
+    const std::string kp = "sfp_photon_" + fq + "_s" + std::to_string(stages) + "_b" + std::to_string(pminb);
+    const std::string kc = f64 ? "sfp_pairs_fp64" : "sfp_pairs_fp32";
     if ((rc = module_kernel(m, km.c_str(), &r->k_massive)) || (rc = module_kernel(m, kp.c_str(), &r->k_photon)) ||
-        (rc = module_kernel(m, kc.c_str(), &r->k_children)) || (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
+        (rc = module_kernel(m, kc.c_str(), &r->k_pairs)) ||
+        (rc = module_kernel(m, "sfp_pair_scan_kernel", &r->k_scan)) ||
+        (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
         delete r;
         return rc;
     }
@@ -869,9 +907,9 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     h.photon_threshold = cfg->photon_threshold;
     h.qed = cfg->qed;
     h.mtile = SFP_TILE_HOST * items;
-    h.ptile = SFP_TILE_HOST * SFP_PHOTON_SUB_HOST;
+    h.ptile = 32 * SFP_PHOTON_WSUB_HOST;
     h.any_appends = 0;
-    for (int s = 0; s < n_seg; ++s) h.any_appends |= (seg[s].radiating || seg[s].bw) ? 1 : 0;
+    for (int s = 0; s < n_seg; ++s) h.any_appends |= seg[s].radiating ? 1 : 0;
     h.n_mseg = (int)r->mseg.size();
     h.n_pseg = (int)r->pseg.size();
     h.n_cseg = (int)r->cseg.size();
@@ -917,27 +955,31 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     st0.skip = 1;
     if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "state upload"));
-    if ((rc = run_alloc_tiles(r, tiles_for(r)))) return cleanup(rc);
-    if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
-    // shared memory for the tables, persistent grid sizes
+    // shared memory: the QED tables (both kernels), then the photon kernel's
+    // copy ring of `stages` stages per warp (photon state + flags)
+    size_t tab;
     if (cfg->qed == SFP_QED_REJECTION)
-        r->smem = 2 * (size_t)cfg->rs.z_N * (f64 ? sizeof(double) : sizeof(float));
+        tab = 2 * (size_t)cfg->rs.z_N * (f64 ? sizeof(double) : sizeof(float));
     else
-        r->smem = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
-    if (r->smem > 16 * 1024) {
-        // the photon kernel's event lists take ~20 KB static shared memory:
-        // allow the table beside it
-        const int cap = 64 * 1024;
-        if (r->smem > (size_t)cap) return cleanup(fail(SFP_EINVAL, "QED tables exceed 64 KB of shared memory"));
-        if (cudaFuncSetAttribute((const void*)r->k_massive, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) !=
-                cudaSuccess ||
-            cudaFuncSetAttribute((const void*)r->k_photon, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) !=
-                cudaSuccess)
-            return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory for the tables"));
-    }
-    r->grid_m = persistent_grid(r->k_massive, r->smem, minb);
-    r->grid_p = persistent_grid(r->k_photon, r->smem, pminb);
-    r->grid_c = persistent_grid(r->k_children, 0, 2);
+        tab = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
+    const size_t nc = cfg->qed == SFP_QED_OPTICAL_DEPTH ? 7 : 6;
+    r->smem_m = tab;
+    h.ring_off = (int)((tab + 127) / 128 * 128);
+    r->smem_p = (size_t)h.ring_off + (size_t)(SFP_TILE_HOST / 32) * stages * (nc * 32 * 8 + 32);
+    if ((rc = run_alloc_tiles(r))) return cleanup(rc);
+    if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
+    const size_t cap = 200 * 1024;
+    if (r->smem_m > cap || r->smem_p > cap) return cleanup(fail(SFP_EINVAL, "QED tables too large for shared memory"));
+    if ((r->smem_m > 48 * 1024 && cudaFuncSetAttribute((const void*)r->k_massive,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)r->smem_m) != cudaSuccess) ||
+        (r->smem_p > 48 * 1024 && cudaFuncSetAttribute((const void*)r->k_photon,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)r->smem_p) != cudaSuccess))
+        return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory"));
+    r->grid_m = persistent_grid(r->k_massive, r->smem_m, minb);
+    r->grid_p = persistent_grid(r->k_photon, r->smem_p, pminb);
+    r->grid_c = persistent_grid(r->k_pairs, 0, 2);
     *out = r;
     return SFP_OK;
 }
@@ -950,14 +992,16 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
             seg[s].bw != r->segs[s].bw || seg[s].ele_dest != r->segs[s].ele_dest ||
             seg[s].pos_dest != r->segs[s].pos_dest)
             return fail(SFP_EINVAL, "sfp_run_update: segment roles changed");
+    int rc = validate_segments(r->n_inst, r->insts.data(), n_seg, seg);
+    if (rc) return rc;
     r->segs.assign(seg, seg + n_seg);
-    int rc = run_alloc_tiles(r, tiles_for(r));
+    rc = run_alloc_tiles(r);
     if (rc) return rc;
     return run_upload(r, nullptr, n_buffered);
 }
 
-// one step: book(prepare), massive, photon, children; ev (6 events) brackets
-// the three step kernels when given
+// one step: book(prepare), massive, photon, pair scan + pairs; ev (6
+// events) brackets the massive, the photon and the two pair kernels when given
 static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev) {
     int prep = 1;
     void* a_book[] = {&r->d, &prep};
@@ -965,15 +1009,17 @@ static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev) {
     SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[0], s));
     if (!r->mseg.empty())
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem, s));
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem_m, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[1], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[2], s));
     if (!r->pseg.empty())
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem, s));
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem_p, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[3], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[4], s));
-    if (!r->cseg.empty())
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_children, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, s));
+    if (!r->cseg.empty()) {
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_scan, dim3(1), dim3(1024), a, 0, s));
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_pairs, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, s));
+    }
     if (ev) SFP_CUDA(cudaEventRecord(ev[5], s));
     return SFP_OK;
 }
@@ -1097,6 +1143,9 @@ int sfp_run_destroy(sfp_run* r) {
     cudaFree(r->h.tile_flag);
     cudaFree(r->h.tile_agg);
     cudaFree(r->h.tile_incl);
+    cudaFree(r->h.ptile_cnt);
+    cudaFree(r->h.psuper_cnt);
+    cudaFree(r->h.psuper_pre);
     cudaFree(r->h.st);
     cudaFree(r->d);
     if (r->ev_in) cudaEventDestroy(r->ev_in);

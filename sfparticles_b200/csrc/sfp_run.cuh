@@ -1,14 +1,17 @@
 // sfp_run.cuh -- device-side layout of a fused-step run, shared by the host
 // C-ABI (nvcc) and the NVRTC-compiled step modules.
 //
-// A step runs three kernels over two tile groups:
-//   massive group -- tiles over the e+- (massive) segments: QED photon
-//                    emission, recoil, Boris push, photon children;
-//   photon group  -- tiles over the photon segments: pair creation, photon
-//                    push, pair children written unpushed;
-//   children      -- the pair children of this step, pushed.
-// Each group numbers its tiles from 0; the look-back flags of the photon
-// group follow those of the massive group in one flag array.
+// A step runs four kernels after the bookkeeping kernel:
+//   massive   -- block tiles over the e+- (massive) segments: QED photon
+//                emission, recoil, Boris push, photon children (ordered by
+//                a decoupled look-back over the tiles);
+//   photon    -- warp tiles over the photon segments: pair creation (the
+//                converted photon is marked and its delta stored), photon
+//                push; per-tile event counts, summed per super-tile of 64;
+//   pair scan -- one block: exclusive scan of the super-tile counts;
+//   pairs     -- e-/e+ children of the marked photons, in index order, pushed.
+// Photon-segment tile ranges start at multiples of 64 tiles, so a
+// super-tile never spans two segments.
 #pragma once
 #include "sfp_types.h"
 
@@ -37,8 +40,8 @@ struct sfp_run_dev {
     double photon_threshold;
     int qed;                    // SFP_QED_*
     int mtile;                  // particles per massive tile (256 * items)
-    int ptile;                  // particles per photon tile
-    int any_appends;            // some segment radiates or creates pairs
+    int ptile;                  // photons per photon (warp) tile
+    int any_appends;            // some massive segment radiates (the massive look-back runs)
     int n_mseg;                 // massive segments (instance order)
     int n_pseg;                 // photon segments
     int n_cseg;                 // segments receiving pair children
@@ -54,7 +57,13 @@ struct sfp_run_dev {
     long long* n_buf_step;        // [n_seg] counts at the start of the running step
     long long* mtile_start;       // [n_mseg + 1]
     long long* ptile_start;       // [n_pseg + 1]
-    long long* chain_first;       // [n_seg] flag index of the first tile of the segment's chain
+    long long* chain_first;       // [n_seg] first massive tile of the segment's chain
+    long long max_ptiles;
+    unsigned int* ptile_cnt;      // [max_ptiles] pair events per photon tile
+    unsigned int* psuper_cnt;     // [max_ptiles / 64 + 1] pair events per super-tile
+    long long* psuper_pre;        // [max_ptiles / 64 + 1] exclusive prefix in its chain
+    int ring_off;                 // photon kernel: byte offset of the copy ring in dynamic smem
+    int pad2;
     long long max_tiles;
     unsigned int* tile_flag;      // [max_tiles] (epoch << 2) | status
     uint4* tile_agg;              // [max_tiles] per-channel tile counts

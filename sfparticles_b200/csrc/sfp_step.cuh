@@ -14,14 +14,15 @@
 //   5. pairs appended, converted photons pruned,
 //   6. every pushed particle -- children included -- pushed from t to t+dt:
 //      half position, fields at t+dt/2, Boris / Boris-TBMT (+LL/CLL), half position.
-// A step is three kernels (after the bookkeeping kernel): the massive group
-// (e+- tiles: 3, 4, recoil, 6), the photon group (photon tiles: 2, 5, 6 for
-// photons) and the pair children's push (6 for this step's pairs).  The two
-// groups touch disjoint memory: each writes its children past the start-of-
-// step count of the other group's buffers.  Appends are ordered: a block
-// scan plus a decoupled look-back across the tiles of a group gives each
-// child the slot that the reference's find_event_index + create_* would give
-// it, so Philox streams keyed by slot are reproducible.
+// After the bookkeeping kernel a step is: the massive kernel (e+- tiles:
+// 3, 4, recoil, 6), the photon kernel (photon tiles: 2, the marking of 5,
+// 6 for photons), the pair scan and the pairs kernel (5 and 6 for this
+// step's pairs).  The massive and photon kernels touch disjoint memory:
+// each writes past the start-of-step count of the other group's buffers.
+// Appends are ordered: a child gets the slot that the reference's
+// find_event_index + create_* would give it (photons: block scan plus a
+// decoupled look-back across the massive tiles; pairs: per-tile counts,
+// scanned), so Philox streams keyed by slot are reproducible.
 #pragma once
 #include "sfp_device.cuh"
 #include "sfp_device32.cuh"
@@ -30,6 +31,12 @@
 #ifndef SFP_TILE
 #define SFP_TILE 256
 #endif
+// photon (warp) tile: SFP_PHOTON_WSUB sub-steps of 32 photons
+#ifndef SFP_PHOTON_WSUB
+#define SFP_PHOTON_WSUB 32
+#endif
+// photon tiles per super-tile of the pair-event scan
+#define SFP_SUPER_TILE 64
 #define SFP_LOOKBACK_SPIN_LIMIT (1u << 24)
 
 #define SFP_FLAG_AGG 1u
@@ -78,6 +85,19 @@ SFP_DEVICE_INLINE uint4 warp_sum_u4(uint4 v) {
         v.w += __shfl_xor_sync(0xffffffffu, v.w, o);
     }
     return v;
+}
+
+// Asynchronous 16-byte global -> shared copies (cp.async, one per thread,
+// L2 only); `src_bytes` < 16 zero-fills the rest and reads only that many.
+SFP_DEVICE_INLINE void cp_async16(void* smem_dst, const void* gsrc, unsigned int src_bytes) {
+    const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
+    const unsigned long long g = (unsigned long long)__cvta_generic_to_global(gsrc);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(src_bytes) : "memory");
+}
+SFP_DEVICE_INLINE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+SFP_DEVICE_INLINE void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Decoupled look-back (Merrill & Garland, 2016) over the tiles of one
@@ -446,6 +466,7 @@ __device__ __forceinline__ int sfp_find_group_pos(const long long* __restrict__ 
 // ---------------------------------------------------------------------------
 extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_dev* __restrict__ R, int prepare) {
     __shared__ int s_bad;
+    __shared__ long long s_nsuper;
     sfp_step_state* st = R->st;
     const int n = R->n_seg;
     if (st->pending) {
@@ -462,7 +483,10 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
     }
     __syncthreads();
     if (!prepare) return;
-    if (threadIdx.x == 0) s_bad = 0;
+    if (threadIdx.x == 0) {
+        s_bad = 0;
+        s_nsuper = 0;
+    }
     __syncthreads();
     if (st->halted || st->error) {
         if (threadIdx.x == 0) st->skip = 1;
@@ -494,6 +518,7 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
             R->n_buf_step[s] = R->n_buffered[s];
             ps += R->n_buffered[s];
         }
+        // massive group: tiles in segment order; each instance's tiles form one look-back chain
         long long acc = 0;
         int prev_inst = -1;
         long long chain = 0;
@@ -509,34 +534,34 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
         }
         R->mtile_start[R->n_mseg] = acc;
         const long long m_tiles = acc;
+        // photon group: each segment starts at a multiple of SFP_SUPER_TILE tiles
         acc = 0;
-        prev_inst = -1;
         for (int j = 0; j < R->n_pseg; ++j) {
             const int s = R->pseg[j];
+            acc = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE * SFP_SUPER_TILE;
             R->ptile_start[j] = acc;
-            if (R->seg[s].instance != prev_inst) {
-                prev_inst = R->seg[s].instance;
-                chain = m_tiles + acc;
-            }
-            R->chain_first[s] = chain;
             acc += (R->n_buffered[s] + R->ptile - 1) / R->ptile;
         }
         R->ptile_start[R->n_pseg] = acc;
-        if (m_tiles + acc > R->max_tiles) {
+        if (m_tiles > R->max_tiles || acc > R->max_ptiles) {
             st->error = SFP_DEV_CAPACITY;
             st->skip = 1;
-            return;
+        } else {
+            st->n_mtiles = m_tiles;
+            st->n_ptiles = acc;
+            st->mticket = 0;
+            st->pticket = 0;
+            st->epoch = (unsigned int)((st->step + 1) & 0x3FFFFFFFll);
+            if (st->epoch == 0u) st->epoch = 1u;
+            st->skip = 0;
+            st->pending = 1;
+            st->particle_steps += ps;
+            s_nsuper = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
         }
-        st->n_mtiles = m_tiles;
-        st->n_ptiles = acc;
-        st->mticket = 0;
-        st->pticket = 0;
-        st->epoch = (unsigned int)((st->step + 1) & 0x3FFFFFFFll);
-        if (st->epoch == 0u) st->epoch = 1u;
-        st->skip = 0;
-        st->pending = 1;
-        st->particle_steps += ps;
     }
+    __syncthreads();
+    // the photon kernel adds into the super-tile counts: start them at zero
+    for (long long k = threadIdx.x; k < s_nsuper; k += blockDim.x) R->psuper_cnt[k] = 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -549,7 +574,7 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
 template <int FORM, int QED, int ITEMS>
 __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
-    extern __shared__ double s_tab[];
+    extern __shared__ __align__(16) double s_tab[];
     __shared__ long long s_tile;
     __shared__ int s_pos;
     __shared__ unsigned int s_warp[ITEMS][SFP_TILE / 32];
@@ -694,248 +719,400 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Photon group.  Streaming tiles of SUB * 256 photons: each sub-step loads,
-// tests for pair creation, pushes and stores its photons at once; events go
-// into per-warp shared-memory lists (no block barrier while streaming); at
-// the end of the tile one look-back orders them and the e-/e+ children are
-// written, unpushed, from the converted photons' (unmoved) state.
+// Photon group.  Each warp takes tiles of SFP_PHOTON_WSUB * 32 photons by
+// ticket and streams them 32 at a time through a ring of STAGES shared-
+// memory stages filled with cp.async, so the state of the next sub-steps is
+// in flight while the current one computes; after the QED tables are staged
+// no block barrier is taken.  Per photon: the pair event at t; a converted
+// photon is marked (pruned = 2, not pushed) and its delta stored for the
+// pairs kernel; every other alive photon is pushed.  The warp's event count
+// goes to its tile's counter and is added to its super-tile's.
 // ---------------------------------------------------------------------------
-template <int FORM, int QED, int SUB, int UNR>
+template <int QED>
+struct sfp_photon_ring {
+    static constexpr int NC = QED == SFP_QED_OPTICAL_DEPTH ? 7 : 6;  // staged doubles per photon
+    static constexpr int STAGE_BYTES = NC * 32 * 8 + 32;             // + the 32 pruned flags
+};
+
+SFP_DEVICE_INLINE const double* sfp_ring_src(const sfp_segment& S, int c) {
+    switch (c) {
+        case 0: return S.x;
+        case 1: return S.y;
+        case 2: return S.z;
+        case 3: return S.ux;
+        case 4: return S.uy;
+        case 5: return S.uz;
+        default: return S.tau;
+    }
+}
+
+// copies of sub-step `sub` (photons base + 32 sub .. + 31) into one stage:
+// component c of photons 2p, 2p+1 -> dst + 256 c + 16 p; flags -> dst + 256 NC.
+// Entries at or past N are zero-filled and not read.  One commit group.
+template <int QED>
+__device__ __forceinline__ void sfp_ring_issue(const sfp_segment& S, long long base, int sub, long long N,
+                                               unsigned char* dst, int lane) {
+    constexpr int NC = sfp_photon_ring<QED>::NC;
+    constexpr int NCOPY = NC * 16 + 2;
+    const long long i0 = base + (long long)sub * 32;
+#pragma unroll
+    for (int k = 0; k < (NCOPY + 31) / 32; ++k) {
+        const int c = lane + 32 * k;
+        if (c < NC * 16) {
+            const int comp = c >> 4, pair = c & 15;
+            const long long j = i0 + 2 * pair;
+            const long long left = N - j;
+            const double* src = sfp_ring_src(S, comp);
+            unsigned int nb = left >= 2 ? 16u : (left == 1 ? 8u : 0u);
+            if (!src) nb = 0u;  // no optical depth array on this segment
+            sfp::cp_async16(dst + comp * 256 + pair * 16, nb ? (const void*)(src + j) : (const void*)S.x, nb);
+        } else if (c < NCOPY) {
+            const int h = c - NC * 16;
+            const long long j = i0 + 16 * h;
+            const long long left = N - j;
+            const unsigned int nb = left >= 16 ? 16u : (left > 0 ? (unsigned int)left : 0u);
+            sfp::cp_async16(dst + NC * 256 + h * 16, nb ? (const void*)(S.pruned + j) : (const void*)S.pruned, nb);
+        }
+    }
+    sfp::cp_async_commit();
+}
+
+template <int FORM, int QED, int STAGES>
 __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
-    constexpr int NW = SFP_TILE / 32;
-    static_assert(SUB * NW <= 64, "scan covers at most 64 (sub, warp) groups");
-    extern __shared__ double s_tab[];
-    __shared__ long long s_tile;
-    __shared__ int s_pos;
-    __shared__ unsigned int s_cnt[SUB][NW];
-    __shared__ uint4 s_excl;
-    __shared__ double s_evd[NW][32 * SUB];
-    __shared__ unsigned int s_evi[NW][32 * SUB];
+    constexpr int NC = sfp_photon_ring<QED>::NC;
+    constexpr int SB = sfp_photon_ring<QED>::STAGE_BYTES;
+    constexpr int PT = 32 * SFP_PHOTON_WSUB;
+    extern __shared__ __align__(16) double s_tab[];
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
     const long long n_tiles = st->n_ptiles;
-    const long long flag0 = st->n_mtiles;
     const double t = st->t;
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
-    const unsigned int epoch = st->epoch;
     const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
-    const bool any_appends = R->any_appends != 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned int lt = (1u << lane) - 1u;
+    unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
 
-    while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const long long tk = (long long)atomicAdd(&st->pticket, 1);
-            s_tile = tk;
-            s_pos = tk < n_tiles ? sfp_find_group_pos(R->ptile_start, R->n_pseg, tk) : 0;
-        }
-        __syncthreads();
-        const long long tile = s_tile;
-        if (tile >= n_tiles) break;
-        const int pos = s_pos;
+    int tk = 0;
+    if (lane == 0) tk = atomicAdd(&st->pticket, 1);
+    long long tile = __shfl_sync(0xffffffffu, tk, 0);
+    while (tile < n_tiles) {
+        if (lane == 0) tk = atomicAdd(&st->pticket, 1);  // next ticket, in flight during this tile
+        const int pos = sfp_find_group_pos(R->ptile_start, R->n_pseg, tile);
         const int si = R->pseg[pos];
         const sfp_segment& S = R->seg[si];
         const sfp_instance& I = R->inst[S.instance];
         const double* __restrict__ P = I.field_params;
         const long long N = R->n_buf_step[si];
-        const long long base = (tile - R->ptile_start[pos]) * (long long)(SFP_TILE * SUB);
-        unsigned int wn = 0;  // events recorded by this warp
-
+        const long long base = (tile - R->ptile_start[pos]) * (long long)PT;
+        unsigned int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<QED>(S, base, k, N, ring + k * SB, lane);
 #pragma unroll 1
-        for (int sub = 0; sub < SUB; sub += UNR) {
-            bool alive[UNR], ev[UNR];
-            double x[UNR], y[UNR], z[UNR], ux[UNR], uy[UNR], uz[UNR], tau[UNR], delta[UNR];
-#pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                const long long i = base + (long long)(sub + u) * SFP_TILE + threadIdx.x;
-                alive[u] = (i < N) && (S.pruned[i] == 0);
-                ev[u] = false;
-                delta[u] = tau[u] = 0.0;
-                x[u] = y[u] = z[u] = ux[u] = uy[u] = uz[u] = 0.0;
-                if (alive[u]) {
-                    x[u] = S.x[i]; y[u] = S.y[i]; z[u] = S.z[i];
-                    ux[u] = S.ux[i]; uy[u] = S.uy[i]; uz[u] = S.uz[i];
-                    if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau[u] = S.tau[i];
-                }
+        for (int sub = 0; sub < SFP_PHOTON_WSUB; ++sub) {
+            __syncwarp();  // every lane has read the stage about to be refilled
+            const int nsub = sub + STAGES - 1;
+            if (nsub < SFP_PHOTON_WSUB) sfp_ring_issue<QED>(S, base, nsub, N, ring + (nsub % STAGES) * SB, lane);
+            else cp_async_commit();
+            cp_async_wait<STAGES - 1>();
+            __syncwarp();  // the stage of `sub` is complete for the whole warp
+            const unsigned char* stg = ring + (sub % STAGES) * SB;
+            const double* sd = reinterpret_cast<const double*>(stg);
+            const long long i = base + (long long)sub * 32 + lane;
+            const bool alive = (i < N) && stg[NC * 256 + lane] == 0;
+            double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
+            double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
+            double tau = QED == SFP_QED_OPTICAL_DEPTH ? sd[192 + lane] : 0.0;
+            bool ev = false;
+            double delta = 0.0;
+            if (alive && S.bw)
+                ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
+            if (ev) {
+                // converted photons are pruned, not pushed (cpu.py:190); 2 marks this step's events
+                S.pruned[i] = 2;
+                S.delta[i] = delta;
+            } else if (alive && S.push) {
+                if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
+                else push_photon32(x, y, z, ux, uy, uz, dt);
+                S.x[i] = x;
+                S.y[i] = y;
+                S.z[i] = z;
             }
-#pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                const long long i = base + (long long)(sub + u) * SFP_TILE + threadIdx.x;
-                if (alive[u] && S.bw)
-                    ev[u] = sfp_pair_event<FORM, QED>(R, T, S, I, P, x[u], y[u], z[u], ux[u], uy[u], uz[u], t, step, i,
-                                                      tau[u], delta[u]);
-                const unsigned int bal = __ballot_sync(0xffffffffu, ev[u]);
-                if (ev[u]) {
-                    const unsigned int r = __popc(bal & lt);
-                    s_evd[warp][wn + r] = delta[u];
-                    s_evi[warp][wn + r] = ((unsigned int)(sub + u) << 16) | (r << 5) | (unsigned int)lane;
-                    S.pruned[i] = 1;  // converted photons are pruned, not pushed (cpu.py:190)
-                } else if (alive[u]) {
-                    if (S.push) {
-                        if (FORM == SFP_FORM_FP64) push_photon(x[u], y[u], z[u], ux[u], uy[u], uz[u], dt);
-                        else push_photon32(x[u], y[u], z[u], ux[u], uy[u], uz[u], dt);
-                        S.x[i] = x[u]; S.y[i] = y[u]; S.z[i] = z[u];
-                    }
-                }
-                if (QED == SFP_QED_OPTICAL_DEPTH && alive[u] && S.tau && S.bw) S.tau[i] = tau[u];
-                if (lane == 0) s_cnt[sub + u][warp] = __popc(bal);
-                wn += __popc(bal);
-            }
+            if (QED == SFP_QED_OPTICAL_DEPTH && alive && S.bw && S.tau) S.tau[i] = tau;
+            cnt += __popc(__ballot_sync(0xffffffffu, ev));
         }
-        if (!any_appends) continue;
-        __syncthreads();
-        if (warp == 0) {
-            // exclusive scan over the (sub, warp) groups in index order: two per lane
-            constexpr int G = SUB * NW;
-            unsigned int a = (2 * lane < G) ? s_cnt[(2 * lane) / NW][(2 * lane) % NW] : 0u;
-            unsigned int b = (2 * lane + 1 < G) ? s_cnt[(2 * lane + 1) / NW][(2 * lane + 1) % NW] : 0u;
-            const unsigned int pair = a + b;
-            unsigned int inc = pair;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int n2 = __shfl_up_sync(0xffffffffu, inc, o);
-                if (lane >= o) inc += n2;
-            }
-            const unsigned int total = __shfl_sync(0xffffffffu, inc, 31);
-            const unsigned int ex0 = inc - pair;
-            if (2 * lane < G) s_cnt[(2 * lane) / NW][(2 * lane) % NW] = ex0;
-            if (2 * lane + 1 < G) s_cnt[(2 * lane + 1) / NW][(2 * lane + 1) % NW] = ex0 + a;
-            uint4 agg{0u, 0u, 0u, 0u};
-            if (S.bw) agg = u4_one(S.channel, total);
-            if (lane == 0 && total) {
-                atomicAdd(&R->appended[S.ele_dest], (unsigned long long)total);
-                atomicAdd(&R->appended[S.pos_dest], (unsigned long long)total);
-            }
-            const long long ft = flag0 + tile;
-            const long long first = R->chain_first[si];
-            uint4 ex{0u, 0u, 0u, 0u};
-            if (ft == first) {
-                publish(R, ft, agg, epoch, true);
-            } else {
-                publish(R, ft, agg, epoch, false);
-                if (!lookback_try(R, ft, first, epoch, ex)) ex = lookback_wait(R, ft, first, epoch);
-                publish(R, ft, u4_add(ex, agg), epoch, true);
-            }
-            if (lane == 0) s_excl = ex;
+        if (lane == 0) {
+            R->ptile_cnt[tile] = cnt;
+            if (cnt) atomicAdd(&R->psuper_cnt[tile / SFP_SUPER_TILE], cnt);
         }
-        __syncthreads();
-        // e- (delta) and e+ (1 - delta) children (cpu.py:119-189), unpushed;
-        // the children kernel pushes them after this kernel
-        if (wn) {
-            const long long ch_base = (long long)u4_get(s_excl, S.channel);
-            const sfp_segment& De = R->seg[S.ele_dest];
-            const sfp_segment& Dp = R->seg[S.pos_dest];
-            const long long be = R->n_buf_step[S.ele_dest] + ch_base;
-            const long long bp = R->n_buf_step[S.pos_dest] + ch_base;
-            for (unsigned int e = lane; e < wn; e += 32) {
-                const unsigned int code = s_evi[warp][e];
-                const int sb = (int)(code >> 16), r = (int)((code >> 5) & 0x7FFu), ln = (int)(code & 31u);
-                const double d = s_evd[warp][e];
-                const long long i = base + (long long)sb * SFP_TILE + warp * 32 + ln;
-                const long long rank = (long long)s_cnt[sb][warp] + r;
-                const double px = S.x[i], py = S.y[i], pz = S.z[i], pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
-                const double d2 = 1.0 - d;
-                long long slot = be + rank;
-                De.x[slot] = px; De.y[slot] = py; De.z[slot] = pz;
-                De.ux[slot] = d * pux; De.uy[slot] = d * puy; De.uz[slot] = d * puz;
-                if (De.spin) { De.sx[slot] = 0.0; De.sy[slot] = 0.0; De.sz[slot] = 0.0; }
-                if (De.tau) De.tau[slot] = 0.0;
-                De.pruned[slot] = 0;
-                slot = bp + rank;
-                Dp.x[slot] = px; Dp.y[slot] = py; Dp.z[slot] = pz;
-                Dp.ux[slot] = d2 * pux; Dp.uy[slot] = d2 * puy; Dp.uz[slot] = d2 * puz;
-                if (Dp.spin) { Dp.sx[slot] = 0.0; Dp.sy[slot] = 0.0; Dp.sz[slot] = 0.0; }
-                if (Dp.tau) Dp.tau[slot] = 0.0;
-                Dp.pruned[slot] = 0;
-            }
+        tile = __shfl_sync(0xffffffffu, tk, 0);
+    }
+}
+
+// segment of super-tile s and whether s starts a chain (the first super-tile
+// of its instance's photon tiles)
+SFP_DEVICE_INLINE void sfp_super_info(const sfp_run_dev* __restrict__ R, long long s, int& si, bool& head) {
+    const long long tile = s * SFP_SUPER_TILE;
+    si = R->pseg[sfp_find_group_pos(R->ptile_start, R->n_pseg, tile)];
+    if (s == 0) {
+        head = true;
+        return;
+    }
+    const int prev = R->pseg[sfp_find_group_pos(R->ptile_start, R->n_pseg, tile - SFP_SUPER_TILE)];
+    head = R->seg[prev].instance != R->seg[si].instance;
+}
+
+SFP_DEVICE_INLINE uint4 shfl_up_u4(uint4 v, int o) {
+    return uint4{__shfl_up_sync(0xffffffffu, v.x, o), __shfl_up_sync(0xffffffffu, v.y, o),
+                 __shfl_up_sync(0xffffffffu, v.z, o), __shfl_up_sync(0xffffffffu, v.w, o)};
+}
+
+// inclusive warp scan of (head, value) pairs: a head restarts the sum
+SFP_DEVICE_INLINE void seg_scan_warp(unsigned int& h, uint4& v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int oh = __shfl_up_sync(0xffffffffu, h, o);
+        const uint4 ov = shfl_up_u4(v, o);
+        if (lane >= o) {
+            if (!h) v = sfp::u4_add(ov, v);
+            h |= oh;
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Pair children of this step, pushed from t to t+dt like every other pushed
-// particle (simulation.py:128-137).  They occupy [n_buf_step, n_buf_step +
-// appended) of each pair-destination segment.
+// Pair scan: one block.  Exclusive scan of the super-tile pair-event counts
+// in tile order, restarted at each instance and kept per append channel, so
+// psuper_pre[s] is the number of pairs that the same instance's photon
+// segments with the same destinations create before super-tile s.  Also
+// adds every photon segment's events to its destinations' append counts.
+// ---------------------------------------------------------------------------
+extern "C" __global__ void __launch_bounds__(1024) sfp_pair_scan_kernel(const sfp_run_dev* __restrict__ R) {
+    __shared__ unsigned int s_wh[32];
+    __shared__ uint4 s_wv[32];
+    const sfp_step_state* st = R->st;
+    if (st->skip) return;
+    const long long n_super = (st->n_ptiles + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
+    if (n_super == 0) return;
+    const long long per = (n_super + blockDim.x - 1) / blockDim.x;
+    const long long s0 = min(n_super, (long long)threadIdx.x * per), s1 = min(n_super, s0 + per);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // this thread's run of super-tiles as one scan element
+    unsigned int h = 0;
+    uint4 v{0u, 0u, 0u, 0u};
+    for (long long s = s0; s < s1; ++s) {
+        int si;
+        bool hd;
+        sfp_super_info(R, s, si, hd);
+        if (hd) {
+            h = 1;
+            v = uint4{0u, 0u, 0u, 0u};
+        }
+        v = sfp::u4_add(v, sfp::u4_one(R->seg[si].channel, R->psuper_cnt[s]));
+    }
+    seg_scan_warp(h, v);
+    if (lane == 31) {
+        s_wh[warp] = h;
+        s_wv[warp] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        unsigned int wh = lane < nw ? s_wh[lane] : 0u;
+        uint4 wv = lane < nw ? s_wv[lane] : uint4{0u, 0u, 0u, 0u};
+        seg_scan_warp(wh, wv);
+        unsigned int eh = __shfl_up_sync(0xffffffffu, wh, 1);
+        uint4 ev = shfl_up_u4(wv, 1);
+        if (lane == 0) {
+            eh = 0u;
+            ev = uint4{0u, 0u, 0u, 0u};
+        }
+        if (lane < nw) {
+            s_wh[lane] = eh;
+            s_wv[lane] = ev;
+        }
+    }
+    __syncthreads();
+    // exclusive value of this thread: earlier warps, then earlier lanes of this warp
+    unsigned int lh = __shfl_up_sync(0xffffffffu, h, 1);
+    uint4 lv = shfl_up_u4(v, 1);
+    if (lane == 0) {
+        lh = 0u;
+        lv = uint4{0u, 0u, 0u, 0u};
+    }
+    uint4 run = lh ? lv : sfp::u4_add(s_wv[warp], lv);
+    int cur = -1;
+    unsigned long long acc = 0ull;
+    for (long long s = s0; s < s1; ++s) {
+        int si;
+        bool hd;
+        sfp_super_info(R, s, si, hd);
+        if (hd) run = uint4{0u, 0u, 0u, 0u};
+        const int ch = R->seg[si].channel;
+        R->psuper_pre[s] = (long long)sfp::u4_get(run, ch);
+        const unsigned int c = R->psuper_cnt[s];
+        run = sfp::u4_add(run, sfp::u4_one(ch, c));
+        if (si != cur) {
+            if (cur >= 0 && acc) {
+                atomicAdd(&R->appended[R->seg[cur].ele_dest], acc);
+                atomicAdd(&R->appended[R->seg[cur].pos_dest], acc);
+            }
+            cur = si;
+            acc = 0ull;
+        }
+        acc += c;
+    }
+    if (cur >= 0 && acc) {
+        atomicAdd(&R->appended[R->seg[cur].ele_dest], acc);
+        atomicAdd(&R->appended[R->seg[cur].pos_dest], acc);
+    }
+}
+
+// one pair child: created at the converted photon's position with momentum
+// d * u (cpu.py:119-189), then pushed from t to t+dt like every pushed
+// particle of this step (simulation.py:128-137)
+template <int FORM>
+__device__ __forceinline__ void sfp_write_pair_child(const sfp_segment& D, long long slot, const double* __restrict__ P,
+                                                     double x, double y, double z, double ux, double uy, double uz,
+                                                     double t, double dt) {
+    using namespace sfp;
+    if (D.push) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, D, P, t, dt);
+        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, D, P, t, dt);
+    }
+    D.x[slot] = x;
+    D.y[slot] = y;
+    D.z[slot] = z;
+    D.ux[slot] = ux;
+    D.uy[slot] = uy;
+    D.uz[slot] = uz;
+    if (D.spin) {
+        D.sx[slot] = 0.0;
+        D.sy[slot] = 0.0;
+        D.sz[slot] = 0.0;
+    }
+    if (D.tau) D.tau[slot] = 0.0;
+    D.pruned[slot] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Pairs: each warp scans 32 photon-tile counters at a time; for a tile with
+// events it adds the counts of the earlier tiles of its super-tile to the
+// super-tile's prefix, finds the marked photons in index order and writes
+// their e- (delta) and e+ (1 - delta) children, pushed, at
+// n_buffered(start of step) + prefix + rank.  The marks become plain prunes.
 // ---------------------------------------------------------------------------
 template <int FORM>
-__device__ __forceinline__ void sfp_children_body(const sfp_run_dev* __restrict__ R) {
+__device__ __forceinline__ void sfp_pairs_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
-    sfp_step_state* st = R->st;
+    constexpr int PT = 32 * SFP_PHOTON_WSUB;
+    const sfp_step_state* st = R->st;
     if (st->skip) return;
+    const long long n_tiles = st->n_ptiles;
     const double t = st->t;
     const double dt = R->dt;
-    const long long gsize = (long long)gridDim.x * blockDim.x;
-    for (int c = 0; c < R->n_cseg; ++c) {
-        const int si = R->cseg[c];
-        const sfp_segment& S = R->seg[si];
-        if (!S.push) continue;
-        const long long cnt = (long long)R->appended[si];
-        const long long start = R->n_buf_step[si];
-        const double* __restrict__ P = R->inst[S.instance].field_params;
-        for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < cnt; j += gsize) {
-            const long long i = start + j;
-            double x = S.x[i], y = S.y[i], z = S.z[i], ux = S.ux[i], uy = S.uy[i], uz = S.uz[i];
-            double sx = 0.0, sy = 0.0, sz = 0.0;
-            if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
-            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
-            S.x[i] = x; S.y[i] = y; S.z[i] = z;
-            S.ux[i] = ux; S.uy[i] = uy; S.uz[i] = uz;
+    const int lane = threadIdx.x & 31;
+    const unsigned int lt = (1u << lane) - 1u;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c0 = gw * 32; c0 < n_tiles; c0 += nw * 32) {
+        const long long mine = c0 + lane;
+        const unsigned int mc = mine < n_tiles ? R->ptile_cnt[mine] : 0u;
+        unsigned int busy = __ballot_sync(0xffffffffu, mc != 0u);
+        while (busy) {
+            const int b = __ffs(busy) - 1;
+            busy &= busy - 1u;
+            const long long tile = c0 + b;
+            const unsigned int c = __shfl_sync(0xffffffffu, mc, b);
+            const long long s = tile / SFP_SUPER_TILE;
+            unsigned int part = 0u;
+            for (long long k = s * SFP_SUPER_TILE + lane; k < tile; k += 32) part += R->ptile_cnt[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            const long long pre = R->psuper_pre[s] + (long long)part;
+            const int pos = sfp_find_group_pos(R->ptile_start, R->n_pseg, tile);
+            const int si = R->pseg[pos];
+            const sfp_segment& S = R->seg[si];
+            const double* __restrict__ P = R->inst[S.instance].field_params;
+            const long long N = R->n_buf_step[si];
+            const long long base = (tile - R->ptile_start[pos]) * (long long)PT;
+            const sfp_segment& De = R->seg[S.ele_dest];
+            const sfp_segment& Dp = R->seg[S.pos_dest];
+            const long long be = R->n_buf_step[S.ele_dest] + pre;
+            const long long bp = R->n_buf_step[S.pos_dest] + pre;
+            unsigned int rank = 0u;
+            for (int sub = 0; sub < SFP_PHOTON_WSUB && rank < c; ++sub) {
+                const long long i = base + (long long)sub * 32 + lane;
+                const bool m = i < N && S.pruned[i] == 2;
+                const unsigned int bal = __ballot_sync(0xffffffffu, m);
+                if (m) {
+                    const long long r = (long long)(rank + __popc(bal & lt));
+                    const double d = S.delta[i];
+                    const double px = S.x[i], py = S.y[i], pz = S.z[i];
+                    const double pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
+                    S.pruned[i] = 1;
+                    sfp_write_pair_child<FORM>(De, be + r, P, px, py, pz, d * pux, d * puy, d * puz, t, dt);
+                    const double d2 = 1.0 - d;
+                    sfp_write_pair_child<FORM>(Dp, bp + r, P, px, py, pz, d2 * pux, d2 * puy, d2 * puz, t, dt);
+                }
+                rank += __popc(bal);
+            }
         }
     }
 }
 
-// kernels: sfp_{massive,photon}_<form>_<qed>_<variant>, sfp_children_<form>
-#ifndef SFP_PHOTON_SUB
-#define SFP_PHOTON_SUB 8
-#endif
+// kernels: sfp_massive_<form>_<qed>_i<items>_b<blocks>,
+// sfp_photon_<form>_<qed>_s<stages>_b<blocks>, sfp_pair_scan_kernel, sfp_pairs_<form>
 #define SFP_MASSIVE_KERNEL(FORM_S, QED_S, FORM, QED, ITEMS, MINB)                                              \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
         sfp_massive_##FORM_S##_##QED_S##_i##ITEMS##_b##MINB(const sfp_run_dev* __restrict__ R) {              \
         sfp_massive_body<FORM, QED, ITEMS>(R);                                                               \
     }
-#define SFP_PHOTON_KERNEL(FORM_S, QED_S, FORM, QED, UNR, MINB)                                                 \
+#define SFP_PHOTON_KERNEL(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                              \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
-        sfp_photon_##FORM_S##_##QED_S##_u##UNR##_b##MINB(const sfp_run_dev* __restrict__ R) {                 \
-        sfp_photon_body<FORM, QED, SFP_PHOTON_SUB, UNR>(R);                                                  \
+        sfp_photon_##FORM_S##_##QED_S##_s##STAGES##_b##MINB(const sfp_run_dev* __restrict__ R) {              \
+        sfp_photon_body<FORM, QED, STAGES>(R);                                                               \
     }
 
 #if defined(SFP_STEP_FORM_FP64)
-extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_children_fp64(const sfp_run_dev* __restrict__ R) {
-    sfp_children_body<SFP_FORM_FP64>(R);
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_pairs_fp64(const sfp_run_dev* __restrict__ R) {
+    sfp_pairs_body<SFP_FORM_FP64>(R);
 }
 #if defined(SFP_STEP_QED_RS)
 SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 2)
 SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
-SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 3)
-SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 3)
+SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 3)
+SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 2)
 #else
 SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 2)
 SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
-SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 3)
-SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 3)
+SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif
 #endif
 #if defined(SFP_STEP_FORM_FP32)
-extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_children_fp32(const sfp_run_dev* __restrict__ R) {
-    sfp_children_body<SFP_FORM_FP32>(R);
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_pairs_fp32(const sfp_run_dev* __restrict__ R) {
+    sfp_pairs_body<SFP_FORM_FP32>(R);
 }
 #if defined(SFP_STEP_QED_RS)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 3)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 2)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
-SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
-SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 4)
+SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 3)
 #else
 SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 3)
 SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 2)
-SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 4)
-SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 3)
+SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 4)
+SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif
 #endif
 #endif  // SFP_WANT_STEP

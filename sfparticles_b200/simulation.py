@@ -9,10 +9,10 @@ generates QED events, appends photons then pairs, and pushes every pushed
 particle (children included) from t to t+dt (simulation.py:102-144);
 ``start`` ends by pruning and returning host arrays (simulation.py:158-161).
 
-Each step is three persistent launches over all species -- the massive
-kernel (e+-: emission, recoil, push, photon children), the photon kernel
-(pair creation, photon push) and the pair-children push -- after a one-block
-bookkeeping launch; steps between progress reports / callbacks run back to
+Each step is a one-block bookkeeping launch followed by the massive kernel
+(e+-: emission, recoil, push, photon children), the photon kernel (pair
+creation, photon push), a one-block scan of the pair-event counts and the
+pairs kernel (e-/e+ children written in order and pushed); steps between progress reports / callbacks run back to
 back on the device, replayed from CUDA graphs, with no host
 synchronisation.  The kernel never overruns a buffer: a device-side guard
 skips the step when a destination lacks room for the worst case (every
@@ -25,8 +25,9 @@ Extra keyword arguments (no reference counterpart):
   graph_chunk -- steps per captured CUDA graph (0 disables graphs);
   items, min_blocks -- massive-kernel variant: particles per thread per
                  tile and minimum resident blocks per SM (see autotune.py);
-  p_unroll, p_min_blocks -- photon-kernel variant: sub-tiles in flight per
-                 thread and minimum resident blocks per SM.
+  p_stages, p_min_blocks -- photon-kernel variant: depth of the copy ring
+                 that streams photon state into shared memory and minimum
+                 resident blocks per SM.
 """
 from __future__ import annotations
 
@@ -50,7 +51,7 @@ except Exception:  # pragma: no cover
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
-                 items: int = 0, min_blocks: int = 0, p_unroll: int = 0, p_min_blocks: int = 0) -> None:
+                 items: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0) -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -69,7 +70,7 @@ class Simulation(object):
         self.graph_chunk = int(graph_chunk)
         self.items = int(items)  # massive kernel: particles per thread per tile (0: the form's default)
         self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
-        self.p_unroll = int(p_unroll)  # photon kernel: sub-tiles in flight per thread (0: default)
+        self.p_stages = int(p_stages)  # photon kernel: depth of the copy ring (0: default)
         self.p_min_blocks = int(p_min_blocks)  # photon kernel: resident blocks per SM (0: default)
         self.particle_steps = 0  # sum over executed steps of all species' N_buffered
         self.kernel_launches = 0  # libsfp kernels launched by start()/run_on_device()
@@ -93,8 +94,8 @@ class Simulation(object):
         dm, dp = DEFAULT[(self.form, self.qed_method)]
         if self.items <= 0 or self.min_blocks <= 0:
             self.items, self.min_blocks = dm
-        if self.p_unroll <= 0 or self.p_min_blocks <= 0:
-            self.p_unroll, self.p_min_blocks = dp
+        if self.p_stages <= 0 or self.p_min_blocks <= 0:
+            self.p_stages, self.p_min_blocks = dp
 
     # ------------------------------------------------------------------
     def _index(self, p):
@@ -124,6 +125,7 @@ class Simulation(object):
             if spin:
                 s.sx, s.sy, s.sz = (p._d(k).data_ptr() for k in ("sx", "sy", "sz"))
             s.tau = p._d("tau").data_ptr() if "tau" in p.attrs else None
+            s.delta = p._d("pair_delta").data_ptr() if p.bw else None
             s.capacity = p.buffer_size
             s.q = p.q
             s.ae = getattr(p, "ae", 0.0) if spin else 0.0
@@ -177,7 +179,7 @@ class Simulation(object):
         cfg.form = _lib.SFP_FORM_FP32 if self.form == "fp32" else _lib.SFP_FORM_FP64
         cfg.items = self.items
         cfg.min_blocks = self.min_blocks
-        cfg.p_unroll = self.p_unroll
+        cfg.p_stages = self.p_stages
         cfg.p_min_blocks = self.p_min_blocks
         if self.qed_method == "od":
             cfg.od_photon, cfg.od_pair = device_tables.od_tables(dev)
@@ -236,12 +238,12 @@ class Simulation(object):
 
     def set_kernel(self, massive=None, photon=None):
         """Switch the kernel variants of a device-resident run: `massive` =
-        (items, min_blocks), `photon` = (p_unroll, p_min_blocks); None keeps
+        (items, min_blocks), `photon` = (p_stages, p_min_blocks); None keeps
         the current one."""
         if massive is not None:
             self.items, self.min_blocks = int(massive[0]), int(massive[1])
         if photon is not None:
-            self.p_unroll, self.p_min_blocks = int(photon[0]), int(photon[1])
+            self.p_stages, self.p_min_blocks = int(photon[0]), int(photon[1])
         if getattr(self, "_run", None) is not None:
             self._end()
             self._begin()
@@ -262,7 +264,7 @@ class Simulation(object):
 
     def time_step_kernel(self, nstep: int):
         """Advance `nstep` steps with eager launches and return, per step, the
-        CUDA-event durations [ms] of its (massive, photon, pair-children)
+        CUDA-event durations [ms] of its (massive, photon, pair scan + pairs)
         kernels (recorded on the stream they run on; 0 for a kernel the run
         does not launch), with the buffered counts before and after."""
         if getattr(self, "_run", None) is None:
@@ -291,11 +293,12 @@ class Simulation(object):
         return out, before, [p.N_buffered for p in self.all_particles]
 
     def _launches_per_step(self):
-        """libsfp kernels one step launches: bookkeeping + the massive,
-        photon and pair-children kernels that have species to work on."""
+        """libsfp kernels one step launches: bookkeeping + the massive and
+        photon kernels that have species to work on + pair scan and pairs
+        when a species creates pairs."""
         ps = self.all_particles
         return (1 + any(p.m != 0 for p in ps) + any(p.m == 0 for p in ps)
-                + any(p.bw for p in ps))
+                + 2 * any(p.bw for p in ps))
 
     def _loop(self, run, nstep, call_back):
         L = _lib.load()
@@ -304,8 +307,12 @@ class Simulation(object):
         st = _lib.RunState()
         remaining = int(nstep)
         tic = perf_counter_ns()
+        # A step that meets a full destination halts the run and the rest of
+        # the queued chunk is launched as no-op kernels: bound the chunk so a
+        # halt wastes at most a few graphs (one host sync per chunk).
+        max_chunk = 4 * self.graph_chunk if self.graph_chunk > 0 else 256
         while remaining > 0:
-            chunk = remaining
+            chunk = min(remaining, max_chunk)
             if call_back:
                 chunk = 1
             if self.print_every:

@@ -333,7 +333,7 @@ def test_kernel_variants_give_the_same_results(form):
         species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
         sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
                            photon_threshold=case["thr"], seed=case["seed"], form=form, items=m[0], min_blocks=m[1],
-                           p_unroll=p[0], p_min_blocks=p[1])
+                           p_stages=p[0], p_min_blocks=p[1])
         sim.start(case["steps"])
         got = [np.stack([getattr(q, k) for k in ("x", "y", "z", "ux", "uy", "uz")]) for q in species]
         if ref is None:
@@ -361,7 +361,7 @@ def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
     best, times = autotune.tune(sim, sample=10_000, steps=2)
     mv, pv = autotune.VARIANTS[("fp32", "rs")]
     assert tuple(best[0]) in mv and tuple(best[1]) in pv and len(times) == len(mv) + len(pv)
-    assert (sim.items, sim.min_blocks) == tuple(best[0]) and (sim.p_unroll, sim.p_min_blocks) == tuple(best[1])
+    assert (sim.items, sim.min_blocks) == tuple(best[0]) and (sim.p_stages, sim.p_min_blocks) == tuple(best[1])
     assert (sim.step, sim.t) == (step, t)  # tuning ran on a copy
     assert os.path.exists(os.path.join(str(tmp_path), "autotune.json"))
     sim.run_on_device(10)
