@@ -45,6 +45,10 @@ BYTES_DEAD = 1      # pruned slot: flag read
 BYTES_APPEND = 49   # appended particle: x,y,z,ux,uy,uz + flag written
 BYTES_PAIR = 155    # pair event in the pairs kernel: parent state + delta read (56), flag (1), e- and e+ written (98)
 BYTES_PTILE = 4     # photon-tile event counter read by the pairs kernel (one per 1024 photons)
+# DRAM bytes (read + write, ncu) / algorithmic bytes of one launch, from an ncu capture of the same
+# cascade at 1e6 electrons at its final state (2.8 GB of photon state, larger than L2, so traffic
+# scales with the units processed).  Only kernels whose state exceeds L2 in that capture are listed.
+NCU_TRAFFIC_RATIO = {"photon": 2.801e9 / 2.806e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
@@ -60,7 +64,7 @@ def beam(n, seed, steps=STEPS_FULL):
     return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
 
 
-def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64):
+def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64, engine="fused"):
     import sfparticles_b200 as S
     from sfparticles_b200.fields import gaussian_laser_pulse
     props, L = beam(n, seed)
@@ -73,7 +77,7 @@ def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64
     fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
     sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form,
                        items=massive[0], min_blocks=massive[1], p_stages=photon[0], p_min_blocks=photon[1],
-                       graph_chunk=graph_chunk)
+                       graph_chunk=graph_chunk, engine=engine)
     return sim
 
 
@@ -279,6 +283,25 @@ def run_ours(args, rank, world):
             res[form] = dict(value=cps / (cms * 1e-3), energies=D.photon_energies(pho), pairs=pos.N_buffered,
                              photons=pho.N_buffered)
             del s
+        if not args.no_ops:
+            # the reference's own step loop over the one-for-one float64 kernels (engine 'ops')
+            s = make_sim(args.compare_electrons, seed + 7, "fp64", engine="ops")
+            for p in s.all_particles:
+                p._to_gpu()
+            torch.cuda.synchronize()
+            e0.record()
+            s._loop_ops(args.steps, None)
+            e1.record()
+            torch.cuda.synchronize()
+            cms = e0.elapsed_time(e1)
+            cps = s.particle_steps
+            for p in s.all_particles:
+                p._prune()
+                p._to_host()
+            ele, pos, pho = s.all_particles
+            res["ops"] = dict(value=cps / (cms * 1e-3), energies=D.photon_energies(pho), pairs=pos.N_buffered,
+                              photons=pho.N_buffered)
+            del s
         a, b = res[args.form], res["fp64"]
         hi = max(a["energies"].max(initial=2.0), b["energies"].max(initial=2.0))
         ha, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=a["energies"])
@@ -288,6 +311,13 @@ def run_ours(args, rank, world):
                    "spectrum_rel_l1": D.spectrum_rel_l1(ha, hb), "spectrum_bins": 64,
                    "pair_yield_rel": D.rel_diff(a["pairs"], b["pairs"]), "pairs_fp64": b["pairs"],
                    "pairs_form": a["pairs"], "photons_fp64": b["photons"], "photons_form": a["photons"]}
+        if "ops" in res:
+            o = res["ops"]
+            ho, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=o["energies"])
+            compare.update({"ops_fp64_value": o["value"], "speedup_vs_ops_fp64": a["value"] / o["value"],
+                            "spectrum_rel_l1_vs_ops": D.spectrum_rel_l1(ha, ho),
+                            "pair_yield_rel_vs_ops": D.rel_diff(a["pairs"], o["pairs"]), "pairs_ops": o["pairs"],
+                            "photons_ops": o["photons"]})
         torch.cuda.empty_cache()
 
     # max over ranks of the device time; sum of work
@@ -305,7 +335,10 @@ def run_ours(args, rank, world):
         v["frac"] = v["achieved_gbs"] / peak
     return dict(ms=ms, particle_steps=tot_ps, counts=counts, launches=launches, clocks=clk.summary(),
                 roofline={"bound": "hbm", "achieved": dk["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                          "frac": dk["achieved_gbs"] / peak, "traffic": None, "peak_kind": peak_kind,
+                          "frac": dk["achieved_gbs"] / peak, "peak_kind": peak_kind,
+                          "traffic": (dk["alg_bytes_per_launch"] * NCU_TRAFFIC_RATIO[dominant]
+                                      if dominant in NCU_TRAFFIC_RATIO else None),
+                          "traffic_note": "ncu DRAM bytes of a 1e6-electron capture scaled by units processed",
                           "kernel": dk["kernel"], "kernel_avg_ms": dk["avg_ms"],
                           "alg_bytes_per_launch": dk["alg_bytes_per_launch"], "launches_timed": args.roofline_steps,
                           "units_at_final_state": step_units, "per_kernel": per_kernel,
@@ -324,6 +357,7 @@ def main():
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--compare-electrons", type=int, default=1_000_000)
     ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--no-ops", action="store_true", help="skip the per-op float64 engine in the comparison")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--items", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0)

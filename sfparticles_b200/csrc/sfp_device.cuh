@@ -108,6 +108,11 @@ SFP_DEVICE_INLINE void field_static(const double* __restrict__ P, double F[6]) {
     for (int i = 0; i < 6; ++i) F[i] = P[i];
 }
 
+// |phi| / kc beyond which a Gaussian envelope exp(-(phi/kc)^2) is exactly 0
+// in float64: sqrt(800), with exp(-745.2) already below half the smallest
+// denormal
+constexpr double kFieldCut64 = 28.2843;
+
 // simple_laser_pulse, fields.py:102-116.
 // P = E0, k0, w0, ctau, direction, x0, cep, cos(pol), sin(pol), t_order, t_order_is_int
 SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, double y, double z, double t,
@@ -117,6 +122,13 @@ SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, doub
     x = dir * x;
     const double r2 = y * y + z * z;
     const double phi = k0 * ((x - dir * x0) - kC * t);
+    // far outside the pulse the envelope exp(-(phi/kc)^2) is exactly 0 in
+    // float64 ((phi/kc)^2 > 745.2); past (phi/kc)^2 = 800 the field is 0
+    // without evaluating cos and exp (the formula gives +-0 there)
+    if (P[10] != 0.0 && tord == 2.0 && fabs(phi) > kFieldCut64 * (k0 * ctau)) {
+        for (int k = 0; k < 6; ++k) F[k] = 0.0;
+        return;
+    }
     double num, den;
     if (P[10] != 0.0) {
         if (tord == 2.0) {
@@ -147,6 +159,16 @@ SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, do
     const double E0 = P[0], k0 = P[1], zR = P[2], w0 = P[3], ctau = P[4], dir = P[5], x0 = P[6];
     const double cep = P[7], cp = P[8], sp = P[9];
     const double r2 = y * y + z * z;
+    // Far outside the pulse the envelope exp(-(phi/kc)^2) is exactly 0 in
+    // float64 ((phi/kc)^2 > 745.2).  |phi| >= |k0 xr| - k0 r2 / (4 zR) - pi/2,
+    // because |x| / (x^2 + zR^2) <= 1 / (2 zR) and |atan| < pi/2; once that
+    // bound exceeds sqrt(800) kc the field is 0 without evaluating atan, cos
+    // and the divisions (the formula gives +-0 there).  Multiplied by 4 zR > 0.
+    if (4.0 * zR * fabs(k0 * ((x - x0) - (dir * kC) * t)) - k0 * r2 - 6.2832 * zR >
+        4.0 * zR * kFieldCut64 * (k0 * ctau)) {
+        for (int k = 0; k < 6; ++k) F[k] = 0.0;
+        return;
+    }
     const double xz = x / zR;
     const double wx = w0 * sqrt(1.0 + xz * xz);
     const double zx = zR / x;

@@ -50,6 +50,11 @@ SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, u
 // ---- field presets (same parameter blocks as the float64 forms) ----------
 // gaussian_laser_pulse (fields.py:152-168); the curvature term k0 r^2 / (2 Rx)
 // is written as k0 r^2 x / (2 (x^2 + zR^2)), finite at x = 0.
+// |phi| / kc beyond which a Gaussian envelope exp(-(phi/kc)^2) is exactly 0
+// in float32, denormals included: sqrt(110), with exp(-104) already below
+// half the smallest denormal
+constexpr float kFieldCut32 = 10.5f;
+
 SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
                                       float F[6]) {
     const float E0 = (float)P[0], k0 = (float)P[1], zR = (float)P[2], w0 = (float)P[3], ctau = (float)P[4];
@@ -58,6 +63,12 @@ SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, do
     const float xf = (float)x, yf = (float)y, zf = (float)z;
     const float xr = (float)((x - x0) - (dir * sfp::kC) * t);
     const float r2 = yf * yf + zf * zf;
+    // |phi| >= |k0 xr| - k0 r2 / (4 zR) - pi/2 (as in the float64 form):
+    // beyond kFieldCut32 kc the envelope is exactly 0, and so is the field
+    if (4.0f * zR * fabsf(k0 * xr) - k0 * r2 - 6.2832f * zR > 4.0f * zR * kFieldCut32 * (k0 * ctau)) {
+        for (int k = 0; k < 6; ++k) F[k] = 0.0f;
+        return;
+    }
     const float xz = xf / zR;
     const float q = 1.0f + xz * xz;
     const float wx2 = (w0 * w0) * q;
@@ -87,6 +98,11 @@ SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, doub
     const float r2 = yf * yf + zf * zf;
     float num, den;
     const float kc = k0 * ctau;
+    // far outside the pulse the envelope is exactly 0 in float32 (see kFieldCut32)
+    if (P[10] != 0.0 && tord == 2 && fabsf(phi) > kFieldCut32 * kc) {
+        for (int k = 0; k < 6; ++k) F[k] = 0.0f;
+        return;
+    }
     if (P[10] != 0.0 && tord == 2) {
         num = phi * phi;
         den = kc * kc;

@@ -27,7 +27,13 @@ Extra keyword arguments (no reference counterpart):
                  tile and minimum resident blocks per SM (see autotune.py);
   p_stages, p_min_blocks -- photon-kernel variant: depth of the copy ring
                  that streams photon state into shared memory and minimum
-                 resident blocks per SM.
+                 resident blocks per SM;
+  engine      -- 'fused' (the persistent step kernels) or 'ops': the
+                 reference's own step loop (simulation.py:102-144) over the
+                 one-for-one kernels of the C-ABI (float64, materialised
+                 fields, host-synchronised appends).  'ops' keys every
+                 species' Philox stream by (seed, species index, step), like
+                 the fused step, so both engines draw the same numbers.
 """
 from __future__ import annotations
 
@@ -51,7 +57,8 @@ except Exception:  # pragma: no cover
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
-                 items: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0) -> None:
+                 items: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0,
+                 engine: str = "fused") -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -67,6 +74,11 @@ class Simulation(object):
         if form not in ("fp64", "fp32"):
             raise ValueError("form must be 'fp64' or 'fp32'")
         self.form = form
+        if engine not in ("fused", "ops"):
+            raise ValueError("engine must be 'fused' or 'ops'")
+        if engine == "ops" and form != "fp64":
+            raise ValueError("the 'ops' engine computes in float64 only")
+        self.engine = engine
         self.graph_chunk = int(graph_chunk)
         self.items = int(items)  # massive kernel: particles per thread per tile (0: the form's default)
         self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
@@ -195,14 +207,55 @@ class Simulation(object):
         if self.progress_bar is None and self.print_every and tqdm is not None:
             self.progress_bar = tqdm(total=total, unit='step', smoothing=1)
 
-        self._begin()
-        try:
-            self._loop(self._run, nstep, call_back)
-        finally:
-            self._end()
+        if self.engine == "ops":
+            self._loop_ops(nstep, call_back)
+        else:
+            self._begin()
+            try:
+                self._loop(self._run, nstep, call_back)
+            finally:
+                self._end()
         for p in self.all_particles:
             p._prune()
             p._to_host()
+
+    def _loop_ops(self, nstep, call_back):
+        """The reference's step loop (simulation.py:102-144) over the per-op
+        kernels: one launch per kernel per species, fields and events
+        materialised in HBM, a host synchronisation per append."""
+        for i, p in enumerate(self.all_particles):
+            p._to_gpu()
+            p.seed = self.seed
+            p.rng_stream = i
+        dt = self.dt
+        for _ in range(int(nstep)):
+            self.particle_steps += sum(p.N_buffered for p in self.all_particles)
+            for p in self.particles_push:
+                p._eval_field(self.fields, self.t)
+            for p in self.particles_bw:
+                p._calculate_chi()
+                p._rng_step = self.step
+                p._pair_event(dt)
+            for p in self.particles_rad:
+                p._calculate_chi()
+                p._rng_step = self.step
+                p._photon_event(dt)
+                p._pick_hard_photon(self.photon_threshold)
+            for p in self.particles_rad:
+                p._create_photon(p.photon_ref())
+            for p in self.particles_bw:
+                p._create_pair(p.bw_electron_ref(), p.bw_positron_ref())
+            for p in self.particles_push:
+                p._push_position(0.5 * dt)
+                p._eval_field(self.fields, self.t + 0.5 * dt)
+                p._push_momentum(dt)
+                p._push_position(0.5 * dt)
+            if call_back:
+                call_back(self.step)
+            self.t += dt
+            self.step += 1
+            if self.print_every and self.step % self.print_every == 0 and self.progress_bar is not None:
+                self.progress_bar.update(self.print_every)
 
     # -- device-resident driving (start() = _begin + _loop + _end + prune) --
     def _begin(self):

@@ -366,3 +366,64 @@ def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
     assert os.path.exists(os.path.join(str(tmp_path), "autotune.json"))
     sim.run_on_device(10)
     sim.finish()
+
+
+@pytest.mark.parametrize("name", ["cascade", "spin_photon", "CLL_focused"])
+def test_ops_engine_matches_fused_fp64(name):
+    """The reference's step loop over the one-for-one kernels (engine 'ops')
+    and the fused step draw the same Philox numbers, so they take the same
+    events and give the same states within the float64 bound."""
+    cuda_or_skip()
+    import sfparticles_b200 as S
+    g = golden(f"ref_sim_{name}.npz")
+    case = json.loads(str(g["case"]))
+    out = []
+    for engine in ("fused", "ops"):
+        species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
+        sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
+                           photon_threshold=case["thr"], seed=case["seed"], engine=engine)
+        sim.start(case["steps"])
+        out.append((species, sim))
+    (a, sa), (b, sb) = out
+    assert sa.step == sb.step and sa.particle_steps == sb.particle_steps
+    for p, q in zip(a, b):
+        assert p.N_buffered == q.N_buffered, (p.name, p.N_buffered, q.N_buffered)
+        keys = ["x", "y", "z", "ux", "uy", "uz"] + (["sx", "sy", "sz"] if "sx" in p.attrs else [])
+        for k in keys:
+            assert _rel(getattr(q, k), getattr(p, k)) < RTOL_RUN, (name, p.name, k)
+
+
+@pytest.mark.parametrize("preset", ["gaussian_laser_pulse", "simple_laser_pulse"])
+def test_far_field_cut_is_exact(preset):
+    """Far outside the pulse the field kernels return 0 without evaluating
+    the pulse; across the cut (|phi| / kc from 20 to 40) they agree with the
+    oracle, which always evaluates the formula: 0 where it underflows, to
+    1e-13 where it does not."""
+    cuda_or_skip()
+    import torch
+    from sfparticles_b200 import _lib, fields as F, program
+    from sfparticles_b200.constants import C
+    kw = dict(a0=200.0, w0=3e-6, ctau=6.366e-6, direction=-1, x0=4.5e-5)
+    f, o = getattr(F, preset)(**kw), getattr(orc, preset)(**kw)
+    k0 = 2 * np.pi / 0.8e-6
+    t = 1e-13
+    # phase distance from the pulse centre in units of kc, both sides
+    s = np.concatenate([np.linspace(20, 40, 2001), -np.linspace(20, 40, 2001)])
+    x = kw["x0"] - C * t + s * kw["ctau"]
+    rng = np.random.default_rng(3)
+    y, z = rng.normal(0, 2e-6, x.size), rng.normal(0, 2e-6, x.size)
+    ref = np.stack(orc.field_eval(o, x, y, z, t))
+    mod = program.get_module(f, form=None, qed=None)
+    prm = f.params_device()
+    xd, yd, zd = dev(x), dev(y), dev(z)
+    pr = dev(np.zeros(x.size, dtype=np.uint8))
+    out = [torch.full((x.size,), np.nan, dtype=torch.float64, device="cuda") for _ in range(6)]
+    _lib.call("sfp_field_eval", mod.handle, ptr(prm), ptr(xd), ptr(yd), ptr(zd), float(t), x.size, ptr(pr),
+              *map(ptr, out), stream())
+    got = np.stack([host(q) for q in out])
+    # near the cut the envelope is a float64 denormal (exp(-729..-745)), good
+    # to a few digits only: compare with an absolute floor far below any field
+    np.testing.assert_allclose(got, ref, rtol=1e-13, atol=1e-280)
+    far = np.abs(s) > 29.0
+    assert far.any() and (~far).any()
+    assert np.all(ref[:, far] == 0.0) and np.all(got[:, far] == 0.0), preset
