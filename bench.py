@@ -81,6 +81,104 @@ def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64
     return sim
 
 
+WORKLOAD_C4 = "batched uneven instances: 256 collisions, a0 log-U[10,500], electrons log-U[1e3,1e6], gamma0 " \
+              "U[500,5000] (rng default_rng(0)), Philox seed = index, w0 3um, 25fs, photons + pairs, dt=T0/100, 2000 steps"
+
+
+def make_c4(form="fp32", n_inst=256, steps=2000, scale=1.0):
+    """The batched-instances workload as an Ensemble (scale shrinks every
+    member's electron count, for tests and warm-up)."""
+    import sfparticles_b200 as S
+    from sfparticles_b200.fields import gaussian_laser_pulse
+    rng = np.random.default_rng(0)
+    a0s = 10 ** rng.uniform(1, math.log10(500), n_inst)
+    ns = np.round(10 ** rng.uniform(3, 6, n_inst) * scale).astype(int)
+    g0s = rng.uniform(500, 5000, n_inst)
+    sims = []
+    L = C * (steps * DT) / 2
+    for k in range(n_inst):
+        r = np.random.default_rng(10_000 + k)
+        n = max(int(ns[k]), 1)
+        g = g0s[k] * (1 + 0.01 * r.normal(size=n))
+        props = (r.normal(-L, 5e-6, n), r.normal(0, 1e-6, n), r.normal(0, 1e-6, n), np.sqrt(g * g - 1),
+                 np.zeros(n), np.zeros(n))
+        ele = S.Particles("electron", -1, 1, N=n, props=props)
+        pos = S.Particles("positron", 1, 1)
+        pho = S.Particles("photon", 0, 0)
+        ele.set_photon(pho)
+        pos.set_photon(pho)
+        pho.set_pair(ele, pos)
+        fld = gaussian_laser_pulse(float(a0s[k]), W0, CTAU, direction=-1, x0=L)
+        sims.append(S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=k, form=form))
+    ens = S.Ensemble(sims)
+    ens.electrons_initial = int(sum(max(int(n), 1) for n in ns))
+    return ens
+
+
+def run_c4(args):
+    """Batched uneven instances on one GPU: value, per-kernel roofline."""
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    w = make_c4(args.form, n_inst=8, steps=args.steps, scale=1e-3)
+    w.run_on_device(args.warmup)
+    w.finish()
+    del w
+    ens = make_c4(args.form, steps=args.steps)
+    ens._begin()
+    torch.cuda.synchronize()
+    launches0 = ens.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        e0.record()
+        ens.run_on_device(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = ens.kernel_launches - launches0
+    ps = ens.particle_steps
+    allp = ens.species
+    counts = {k: int(sum(p.N_buffered for p in allp if p.name == k)) for k in ("electron", "positron", "photon")}
+    alive = {k: int(sum(p.Npart for p in allp if p.name == k)) for k in ("electron", "positron", "photon")}
+    torch.cuda.nvtx.range_push("roofline")
+    kms, before, after = ens.time_step_kernel(args.roofline_steps)
+    torch.cuda.nvtx.range_pop()
+    k_ms = [float(np.mean([k[j] for k in kms])) for j in range(3)]
+    names = [p.name for p in allp]
+    n_ph_app = sum(a - b for a, b, nm in zip(after, before, names) if nm == "photon") / args.roofline_steps
+    n_pairs = sum(a - b for a, b, nm in zip(after, before, names) if nm == "positron") / args.roofline_steps
+    buf = {k: int(sum(n for n, nm in zip(before, names) if nm == k)) for k in ("electron", "positron", "photon")}
+    n_epm = alive["electron"] + alive["positron"]
+    alg = {"massive": n_epm * BYTES_EPM + (buf["electron"] + buf["positron"] - n_epm) * BYTES_DEAD
+           + n_ph_app * BYTES_APPEND,
+           "photon": alive["photon"] * BYTES_PHOTON + (buf["photon"] - alive["photon"]) * BYTES_DEAD
+           + 2 * n_pairs * BYTES_APPEND}
+    peak, peak_kind = measured_peak_hbm()
+    per_kernel = {}
+    for j, k in enumerate(("massive", "photon")):
+        gbs = alg[k] / (k_ms[j] * 1e-3) / 1e9 if k_ms[j] > 0 else 0.0
+        per_kernel[k] = {"avg_ms": k_ms[j], "alg_bytes_per_launch": alg[k], "achieved_gbs": gbs, "frac": gbs / peak}
+    per_kernel["pairs"] = {"avg_ms": k_ms[2]}
+    dominant = max(("massive", "photon"), key=lambda k: per_kernel[k]["avg_ms"])
+    dk = per_kernel[dominant]
+    ens.finish()
+    value = ps / (ms * 1e-3)
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_C4, "form": args.form, "instances": len(ens.sims),
+                       "electrons_initial": ens.electrons_initial,
+                       "final_counts": counts, "l2": "state larger than L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": dk["achieved_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": dk["frac"], "traffic": None, "peak_kind": peak_kind,
+                         "per_kernel": per_kernel, "launches_timed": args.roofline_steps},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk.summary(),
+            "particle_steps": ps}
+    print(json.dumps(line), flush=True)
+
+
 def make_oracle_sim(n, seed):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as orc
@@ -353,6 +451,8 @@ def main():
     ap.add_argument("--steps", type=int, default=STEPS_FULL)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                    help="c2: the scaled cascade (default); c4: 256 batched uneven instances (2000 steps)")
     ap.add_argument("--electrons", type=int, default=10_000_000)
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--compare-electrons", type=int, default=1_000_000)
@@ -374,6 +474,15 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "c4":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "c4",
+                              "unavailable": "the batched-instances mode runs one GPU, product arm only"}))
+            return
+        if args.steps == STEPS_FULL:
+            args.steps = 2000
+        run_c4(args)
+        return
 
     if args.impl == "reference":
         # the reference's CPU algorithm (oracle port) on the host cores; rank 0 only

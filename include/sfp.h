@@ -162,11 +162,17 @@ typedef struct sfp_run_config {
 
 int sfp_run_create(sfp_module *m, const sfp_run_config *cfg, int n_inst, const sfp_instance *inst, int n_seg,
                    const sfp_segment *seg, const int64_t *n_buffered, sfp_run **out);
-/* after buffers were regrown / moved: new segment table and counts */
+/* after buffers were regrown / moved: new segment table and counts
+ * (n_buffered NULL keeps the device's counts) */
 int sfp_run_update(sfp_run *r, int n_seg, const sfp_segment *seg, const int64_t *n_buffered);
-/* advance up to nsteps steps (stops early, halted=1, when a destination
- * lacks the worst-case headroom); graph_chunk > 0 replays CUDA graphs of
- * that many steps.  Asynchronous on `stream`. */
+/* advance up to nsteps steps; graph_chunk > 0 replays CUDA graphs of that
+ * many steps.  Asynchronous on `stream`.  The run stops early with halted=1
+ * (a) before a step when a photon destination lacks room for every emitter
+ * emitting -- grow it (the reference's _extend rule), sfp_run_update,
+ * sfp_run_clear_halt -- or (b) inside a step, after its pair events are
+ * counted, when an e-/e+ destination lacks room for them (pairs_pending=1):
+ * grow every segment to sfp_run_pending_need, sfp_run_update with NULL
+ * counts, then sfp_run_resume to finish that step. */
 int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
 /* like sfp_run_steps without graphs, with CUDA events recorded around each
  * of the three kernels of every step on the run's stream; synchronous.
@@ -178,6 +184,12 @@ int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stre
 int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);
 /* clear the halted flag after the caller made room */
 int sfp_run_clear_halt(sfp_run *r, void *stream);
+/* synchronous: while pairs_pending, the buffer size each segment needs to
+ * finish the stopped step (n_seg entries); otherwise its buffered count */
+int sfp_run_pending_need(sfp_run *r, int64_t *need);
+/* finish a step stopped with pairs_pending: write and push its pairs, fold
+ * its appends and advance t / step.  Asynchronous on the run's stream. */
+int sfp_run_resume(sfp_run *r, void *stream);
 int sfp_run_destroy(sfp_run *r);
 
 #ifdef __cplusplus

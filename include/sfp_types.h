@@ -103,9 +103,13 @@ typedef struct sfp_rs_table {
 typedef struct sfp_run_state {
     double t;               /* time of the next step                        */
     sfp_i64 step;           /* steps completed                              */
-    sfp_i32 halted;         /* 1: a step was skipped for lack of capacity   */
+    sfp_i32 halted;         /* 1: the run stopped for lack of capacity      */
     sfp_i32 error;          /* device error code (0 = none)                 */
     sfp_i64 particle_steps; /* sum over executed steps of all N_buffered    */
+    sfp_i32 pairs_pending;  /* 1: a step stopped before writing its pairs:
+                               grow to sfp_run_pending_need, then
+                               sfp_run_resume                               */
+    sfp_i32 pad;
 } sfp_run_state;
 
 #define SFP_MAX_SEGMENTS 4096

@@ -17,7 +17,8 @@ if _getenv("SFPARTICLES_USE_GPU", "1") == "0":
 from .fields import Fields  # noqa: E402
 from .particles import Particles, RadiationReactionType, SpinParticles  # noqa: E402
 from .simulation import Simulation  # noqa: E402
+from .ensemble import Ensemble  # noqa: E402
 
 _use_gpu = True
-__all__ = ["Particles", "SpinParticles", "Simulation", "Fields", "RadiationReactionType"]
+__all__ = ["Particles", "SpinParticles", "Simulation", "Ensemble", "Fields", "RadiationReactionType"]
 __version__ = "0.1.0"

@@ -52,7 +52,8 @@ class RSTable(ctypes.Structure):
 
 
 class RunState(ctypes.Structure):
-    _fields_ = [("t", c_d), ("step", c_i64), ("halted", c_i32), ("error", c_i32), ("particle_steps", c_i64)]
+    _fields_ = [("t", c_d), ("step", c_i64), ("halted", c_i32), ("error", c_i32), ("particle_steps", c_i64),
+                ("pairs_pending", c_i32), ("pad", c_i32)]
 
 
 class RunConfig(ctypes.Structure):
@@ -100,6 +101,8 @@ _SIGS = {
     "sfp_run_steps_timed": ([P, c_i64, P, P], c_i32),
     "sfp_run_read_state": ([P, P, P, P], c_i32),
     "sfp_run_clear_halt": ([P, P], c_i32),
+    "sfp_run_pending_need": ([P, P], c_i32),
+    "sfp_run_resume": ([P, P], c_i32),
     "sfp_run_destroy": ([P], c_i32),
 }
 

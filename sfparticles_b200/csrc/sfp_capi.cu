@@ -769,18 +769,33 @@ static int run_alloc_tiles(sfp_run* r) {
         r->h.max_tiles = n;
     }
     if (need_p > r->h.max_ptiles) {
+        // grown between steps, or while a stopped step waits for its pairs:
+        // the counters of that step are carried over
         const long long n = need_p + need_p / 4 + 64;
         const long long ns = n / SFP_SUPER_TILE_HOST + 2;
-        if (r->h.ptile_cnt) cudaFree(r->h.ptile_cnt);
-        if (r->h.psuper_cnt) cudaFree(r->h.psuper_cnt);
-        if (r->h.psuper_pre) cudaFree(r->h.psuper_pre);
-        r->h.ptile_cnt = nullptr;
-        r->h.psuper_cnt = nullptr;
-        r->h.psuper_pre = nullptr;
-        r->h.max_ptiles = 0;
-        SFP_CUDA(cudaMalloc(&r->h.ptile_cnt, n * sizeof(unsigned int)));
-        SFP_CUDA(cudaMalloc(&r->h.psuper_cnt, ns * sizeof(unsigned int)));
-        SFP_CUDA(cudaMalloc(&r->h.psuper_pre, ns * sizeof(long long)));
+        const long long n_old = r->h.max_ptiles, ns_old = n_old ? n_old / SFP_SUPER_TILE_HOST + 2 : 0;
+        unsigned int *cnt = nullptr, *scnt = nullptr;
+        long long* spre = nullptr;
+        if (cudaMalloc(&cnt, n * sizeof(unsigned int)) != cudaSuccess ||
+            cudaMalloc(&scnt, ns * sizeof(unsigned int)) != cudaSuccess ||
+            cudaMalloc(&spre, ns * sizeof(long long)) != cudaSuccess) {
+            cudaFree(cnt);
+            cudaFree(scnt);
+            cudaFree(spre);
+            return fail(SFP_ENOMEM, "cudaMalloc of the photon-tile counters");
+        }
+        if (n_old) {
+            SFP_CUDA(cudaMemcpyAsync(cnt, r->h.ptile_cnt, n_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
+            SFP_CUDA(cudaMemcpyAsync(scnt, r->h.psuper_cnt, ns_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
+            SFP_CUDA(cudaMemcpyAsync(spre, r->h.psuper_pre, ns_old * sizeof(long long), cudaMemcpyDeviceToDevice, r->s));
+            SFP_CUDA(cudaStreamSynchronize(r->s));
+        }
+        cudaFree(r->h.ptile_cnt);
+        cudaFree(r->h.psuper_cnt);
+        cudaFree(r->h.psuper_pre);
+        r->h.ptile_cnt = cnt;
+        r->h.psuper_cnt = scnt;
+        r->h.psuper_pre = spre;
         r->h.max_ptiles = n;
     }
     return SFP_OK;
@@ -1109,6 +1124,8 @@ int sfp_run_read_state(sfp_run* r, sfp_run_state* state, int64_t* n_buffered, vo
     state->halted = st.halted;
     state->error = st.error;
     state->particle_steps = st.particle_steps;
+    state->pairs_pending = st.pair_wait;
+    state->pad = 0;
     return SFP_OK;
 }
 
@@ -1118,10 +1135,60 @@ int sfp_run_clear_halt(sfp_run* r, void* stream) {
     sfp_step_state st;
     SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
+    if (st.pair_wait)
+        return fail(SFP_EINVAL, "sfp_run_clear_halt: a step waits for its pairs; finish it with sfp_run_resume");
     st.halted = 0;
     st.skip = 1;
     SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
+    return SFP_OK;
+}
+
+int sfp_run_pending_need(sfp_run* r, int64_t* need) {
+    if (!r || !need) return fail(SFP_EINVAL, "sfp_run_pending_need: NULL argument");
+    sfp_step_state st;
+    std::vector<long long> nb(r->n_seg), ns(r->n_seg);
+    std::vector<unsigned long long> ap(r->n_seg);
+    SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(nb.data(), r->h.n_buffered, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(ns.data(), r->h.n_buf_step, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(ap.data(), r->h.appended, r->n_seg * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    for (int s = 0; s < r->n_seg; ++s) need[s] = st.pair_wait ? ns[s] + (long long)ap[s] : nb[s];
+    return SFP_OK;
+}
+
+int sfp_run_resume(sfp_run* r, void* stream) {
+    if (!r) return fail(SFP_EINVAL, "sfp_run_resume: NULL run");
+    sfp_step_state st;
+    std::vector<long long> ns(r->n_seg);
+    std::vector<unsigned long long> ap(r->n_seg);
+    SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(ns.data(), r->h.n_buf_step, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(ap.data(), r->h.appended, r->n_seg * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    if (!st.pair_wait) return SFP_OK;
+    // the pairs kernel runs only when every destination holds its pairs
+    for (int c : r->cseg)
+        if (ns[c] + (long long)ap[c] > r->segs[c].capacity)
+            return fail(SFP_EINVAL, "sfp_run_resume: segment " + std::to_string(c) +
+                                        " still lacks room for the pairs of the stopped step");
+    st.pair_wait = 0;
+    st.halted = 0;
+    st.skip = 0;
+    cudaStream_t cs = as_stream(stream);
+    SFP_CUDA(cudaEventRecord(r->ev_in, cs));
+    SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
+    SFP_CUDA(cudaStreamSynchronize(r->s));
+    void* a[] = {&r->d};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_pairs, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, r->s));
+    const int rc = launch_fold(r);
+    if (rc) return rc;
+    SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
+    SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
     return SFP_OK;
 }
 

@@ -27,7 +27,7 @@ struct sfp_step_state {
     int error;                  // sticky device error (SFP_DEV_*)
     unsigned int epoch;         // look-back flag epoch of the prepared step
     int pending;                // a prepared step awaits folding
-    int pad;
+    int pair_wait;              // the prepared step stopped before writing its pairs (no room)
     long long particle_steps;   // sum over executed steps of all N_buffered
 };
 

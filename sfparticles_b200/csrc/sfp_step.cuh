@@ -469,7 +469,8 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
     __shared__ long long s_nsuper;
     sfp_step_state* st = R->st;
     const int n = R->n_seg;
-    if (st->pending) {
+    // a step that stopped before writing its pairs is folded only once resumed
+    if (st->pending && !st->pair_wait) {
         for (int s = threadIdx.x; s < n; s += blockDim.x) {
             R->n_buffered[s] += (long long)R->appended[s];
             R->appended[s] = 0ull;
@@ -488,11 +489,12 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
         s_nsuper = 0;
     }
     __syncthreads();
-    if (st->halted || st->error) {
+    if (st->halted || st->error || st->pair_wait) {
         if (threadIdx.x == 0) st->skip = 1;
         return;
     }
-    // worst case appends per destination: every emitter emits, every photon converts
+    // worst case photon appends per destination: every emitter emits.  (Pair
+    // destinations are checked against the exact pair count by the pair scan.)
     for (int d = threadIdx.x; d < n; d += blockDim.x) {
         long long need = 0;
         const int inst = R->seg[d].instance;
@@ -500,7 +502,6 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
         for (int s = f; s < l; ++s) {
             const sfp_segment& S = R->seg[s];
             if (S.radiating && S.photon_dest == d) need += R->n_buffered[s];
-            if (S.bw && (S.ele_dest == d || S.pos_dest == d)) need += R->n_buffered[s];
         }
         if (R->n_buffered[d] + need > R->seg[d].capacity) atomicExch(&s_bad, 1);
     }
@@ -807,6 +808,11 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         const double* __restrict__ P = I.field_params;
         const long long N = R->n_buf_step[si];
         const long long base = (tile - R->ptile_start[pos]) * (long long)PT;
+        if (base >= N) {  // alignment padding between segments: no photons
+            if (lane == 0) R->ptile_cnt[tile] = 0u;
+            tile = __shfl_sync(0xffffffffu, tk, 0);
+            continue;
+        }
         unsigned int cnt = 0;
 #pragma unroll
         for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<QED>(S, base, k, N, ring + k * SB, lane);
@@ -969,6 +975,21 @@ extern "C" __global__ void __launch_bounds__(1024) sfp_pair_scan_kernel(const sf
         atomicAdd(&R->appended[R->seg[cur].ele_dest], acc);
         atomicAdd(&R->appended[R->seg[cur].pos_dest], acc);
     }
+    __syncthreads();
+    // exact room check: the pairs kernel writes nothing unless every e-/e+
+    // destination holds its pairs; otherwise the step waits for the host
+    __shared__ int s_short;
+    if (threadIdx.x == 0) s_short = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < R->n_cseg; c += blockDim.x) {
+        const int d = R->cseg[c];
+        if (R->n_buf_step[d] + (long long)R->appended[d] > R->seg[d].capacity) atomicExch(&s_short, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_short) {
+        R->st->pair_wait = 1;
+        R->st->halted = 1;
+    }
 }
 
 // one pair child: created at the converted photon's position with momentum
@@ -1011,7 +1032,7 @@ __device__ __forceinline__ void sfp_pairs_body(const sfp_run_dev* __restrict__ R
     using namespace sfp;
     constexpr int PT = 32 * SFP_PHOTON_WSUB;
     const sfp_step_state* st = R->st;
-    if (st->skip) return;
+    if (st->skip || st->pair_wait) return;
     const long long n_tiles = st->n_ptiles;
     const double t = st->t;
     const double dt = R->dt;

@@ -54,6 +54,20 @@ except Exception:  # pragma: no cover
     tqdm = None
 
 
+def resolve_pending_pairs(run, species, update):
+    """Finish a step that stopped before writing its pairs: grow every
+    species to the size the step needs (the reference's _extend rule,
+    particles.py:487-500), hand the new buffers to the run and resume it."""
+    L = _lib.load()
+    need = (ctypes.c_int64 * len(species))()
+    _lib.check(L.sfp_run_pending_need(run, need), "sfp_run_pending_need")
+    for i, p in enumerate(species):
+        if int(need[i]) > p.buffer_size:
+            p._extend(int(need[i]) - p.N_buffered)
+    update()
+    _lib.check(L.sfp_run_resume(run, _stream_ptr()), "sfp_run_resume")
+
+
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
@@ -160,16 +174,16 @@ class Simulation(object):
         return segs
 
     def _worst_case_need(self):
+        """Photon appends of one step if every emitter emits.  Pair
+        destinations are grown on demand: the device counts a step's pairs
+        before writing them and stops when they do not fit."""
         need = {id(p): 0 for p in self.all_particles}
         for p in self.particles_rad:
             need[id(p.photon_ref())] += p.N_buffered
-        for p in self.particles_bw:
-            need[id(p.bw_electron_ref())] += p.N_buffered
-            need[id(p.bw_positron_ref())] += p.N_buffered
         return need
 
     def _ensure_headroom(self) -> bool:
-        """Grow destinations that could overflow in one step; True if any grew."""
+        """Grow photon destinations that could overflow in one step; True if any grew."""
         grew = False
         need = self._worst_case_need()
         for p in self.all_particles:
@@ -333,13 +347,18 @@ class Simulation(object):
             ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
-            if st.error or st.halted:
+            self.kernel_launches += self._launches_per_step() + 1
+            if st.error or (st.halted and not st.pairs_pending):
                 raise _lib.SFPError("timed step did not complete")
+            if st.pairs_pending:  # finish the step; its pair kernels were not timed
+                resolve_pending_pairs(self._run, self.all_particles,
+                                      lambda: self._update_run(self._run, counts=False))
+                _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
+            else:
+                out.append((float(ms[0]), float(ms[1]), float(ms[2])))
             for i, p in enumerate(self.all_particles):
                 p.N_buffered = int(nbuf[i])
                 p._touch()
-            self.kernel_launches += self._launches_per_step() + 1
-            out.append((float(ms[0]), float(ms[1]), float(ms[2])))
         self.particle_steps = self._ps_base + int(st.particle_steps)
         self.step = int(st.step)
         self.t = float(st.t)
@@ -375,24 +394,19 @@ class Simulation(object):
             _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
             self.kernel_launches += self._launches_per_step() * chunk + 1
-            _lib.check(L.sfp_run_read_state(run, ctypes.byref(st), nbuf, _stream_ptr()), "sfp_run_read_state")
-            if st.error:
-                raise _lib.SFPError(f"device error in the step kernel: {_lib.DEV_ERRORS.get(st.error, st.error)}")
-            done = int(st.step) - self.step
-            for i, p in enumerate(self.all_particles):
-                p.N_buffered = int(nbuf[i])
-            self.particle_steps = self._ps_base + int(st.particle_steps)
-            if done > 0:
-                for p in self.all_particles:
-                    p._touch()
-            self.step = int(st.step)
-            self.t = float(st.t)
+            done = self._sync_state(run, st, nbuf)
+            halted = bool(st.halted)
+            if halted:
+                if st.pairs_pending:
+                    # finishing the stopped step completes it: count it
+                    resolve_pending_pairs(run, self.all_particles, lambda: self._update_run(run, counts=False))
+                    done += self._sync_state(run, st, nbuf)
+                else:
+                    self._ensure_headroom()
+                    self._update_run(run)
+                    _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
-            if st.halted:
-                self._ensure_headroom()
-                self._update_run(run)
-                _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
-            if done == 0 and not st.halted:
+            if done == 0 and not halted:
                 raise _lib.SFPError("the step made no progress")
             if call_back and done:
                 call_back(self.step - 1)
@@ -407,8 +421,24 @@ class Simulation(object):
                 self.progress_bar.set_postfix_str(f"{particle_num_str}, {ns_per_particle:.0f}ns/particle")
                 self.progress_bar.update(self.print_every)
 
-    def _update_run(self, run):
+    def _sync_state(self, run, st, nbuf) -> int:
+        """Read the run's state into the species; returns the steps completed
+        since the last read."""
+        _lib.check(_lib.load().sfp_run_read_state(run, ctypes.byref(st), nbuf, _stream_ptr()), "sfp_run_read_state")
+        if st.error:
+            raise _lib.SFPError(f"device error in the step kernel: {_lib.DEV_ERRORS.get(st.error, st.error)}")
+        done = int(st.step) - self.step
+        for i, p in enumerate(self.all_particles):
+            p.N_buffered = int(nbuf[i])
+            if done > 0:
+                p._touch()
+        self.particle_steps = self._ps_base + int(st.particle_steps)
+        self.step = int(st.step)
+        self.t = float(st.t)
+        return done
+
+    def _update_run(self, run, counts=True):
         segs = self._segments()
         n = len(self.all_particles)
-        nbuf = (ctypes.c_int64 * n)(*[p.N_buffered for p in self.all_particles])
+        nbuf = (ctypes.c_int64 * n)(*[p.N_buffered for p in self.all_particles]) if counts else None
         _lib.call("sfp_run_update", run, n, segs, nbuf)
