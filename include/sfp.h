@@ -155,6 +155,8 @@ typedef struct sfp_run_config {
     int32_t min_blocks;      /* massive kernel: min resident blocks per SM (0 = default)    */
     int32_t p_stages;        /* photon kernel: depth of the copy ring, 2..4 (0 = default)   */
     int32_t p_min_blocks;    /* photon kernel: min resident blocks per SM (0 = default)     */
+    const float *mlp_params; /* optical depth: the learned photon-energy sampler's 8577
+                                parameters (device), or NULL for the table sampler      */
     sfp_rs_table rs;
     sfp_od_table od_photon;
     sfp_od_table od_pair;
@@ -191,6 +193,34 @@ int sfp_run_pending_need(sfp_run *r, int64_t *need);
  * its appends and advance t / step.  Asynchronous on the run's stream. */
 int sfp_run_resume(sfp_run *r, void *stream);
 int sfp_run_destroy(sfp_run *r);
+
+/* ---- learned photon-energy sampler (no counterpart in the reference) ------
+ * An MLP (log10 chi, u) -> delta, 2 -> 64 -> 64 -> 64 -> 1 with SiLU, that can
+ * stand in for the optical-depth method's inverse-CDF table sampler
+ * (_bisect_interp, qed/optical_depth_tables.py:59-102).  Parameters: 8577
+ * float32, W0[64][2] b0[64] W1[64][64] b1[64] W2[64][64] b2[64] W3[64] b3.
+ * Features (log10 chi / 3, log(u / (1 - u)) / 8); output y, delta =
+ * 10^(3 (y - 1)) clamped to [1e-6, 1]. */
+#define SFP_MLP_HIDDEN 64
+#define SFP_MLP_NPARAM 8577
+/* the table sampler, batched: delta[i] = _bisect_interp at chi = 10^log_chi[i], u[i] */
+int sfp_od_inverse_cdf(const sfp_od_table *table, const double *log_chi, const double *u, double *delta, int64_t N,
+                       void *stream);
+/* N training samples: log10 chi ~ U[lo, hi]; u ~ U(0,1) for 3 in 4 samples and
+ * 1 - u log-uniform in [1e-8, 0.1] for the rest (Philox(seed, chunk));
+ * features[2i], features[2i+1] as above, targets[i] = log10(table delta) / 3 + 1 */
+int sfp_mlp_make_samples(const sfp_od_table *table, uint64_t seed, uint32_t chunk, double log_chi_lo,
+                         double log_chi_hi, int64_t N, float *features, float *targets, void *stream);
+/* adds to grad (8577 floats) the gradient of sum_i (y_i - targets_i)^2 with
+ * respect to the BF16-rounded weights, and that sum to *loss (device double) */
+int sfp_mlp_grad(const float *params, const float *features, const float *targets, int64_t N, float *grad,
+                 double *loss, void *stream);
+/* one Adam step (step counts from 1) with gradient grad * grad_scale */
+int sfp_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t step, float lr, float beta1,
+                 float beta2, float eps, float grad_scale, void *stream);
+/* batched inference on the tensor cores (BF16 weights, FP32 accumulation) */
+int sfp_mlp_infer(const float *params, const double *log_chi, const double *u, double *delta, int64_t N,
+                  void *stream);
 
 #ifdef __cplusplus
 }

@@ -58,7 +58,7 @@ class RunState(ctypes.Structure):
 
 class RunConfig(ctypes.Structure):
     _fields_ = [("dt", c_d), ("photon_threshold", c_d), ("t0", c_d), ("step0", c_i64), ("qed", c_i32), ("form", c_i32),
-                ("items", c_i32), ("min_blocks", c_i32), ("p_stages", c_i32), ("p_min_blocks", c_i32),
+                ("items", c_i32), ("min_blocks", c_i32), ("p_stages", c_i32), ("p_min_blocks", c_i32), ("mlp_params", P),
                 ("rs", RSTable), ("od_photon", ODTable),
                 ("od_pair", ODTable)]
 
@@ -103,6 +103,12 @@ _SIGS = {
     "sfp_run_clear_halt": ([P, P], c_i32),
     "sfp_run_pending_need": ([P, P], c_i32),
     "sfp_run_resume": ([P, P], c_i32),
+    "sfp_od_inverse_cdf": ([P, P, P, P, c_i64, P], c_i32),
+    "sfp_mlp_make_samples": ([P, ctypes.c_uint64, ctypes.c_uint32, c_d, c_d, c_i64, P, P, P], c_i32),
+    "sfp_mlp_grad": ([P, P, P, c_i64, P, P, P], c_i32),
+    "sfp_mlp_adam": ([P, P, P, P, c_i64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                      ctypes.c_float, P], c_i32),
+    "sfp_mlp_infer": ([P, P, P, P, c_i64, P], c_i32),
     "sfp_run_destroy": ([P], c_i32),
 }
 

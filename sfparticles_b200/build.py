@@ -1,6 +1,6 @@
 """Build steps of sfparticles_b200.
 
-* ``build_library()``  -- nvcc: csrc/sfp_capi.cu -> libsfp.so (sm_100a, in-tree)
+* ``build_library()``  -- nvcc: csrc/sfp_capi.cu + csrc/sfp_mlp.cu -> libsfp.so (sm_100a, in-tree)
 * ``build_tables()``   -- QED tables into qed/data (scipy, CPU)
 * ``prebuild_modules()`` -- NVRTC: field-specialised step modules for the
   presets into the module cache (NVRTC needs no GPU)
@@ -26,7 +26,7 @@ def nvcc() -> str:
 
 
 def library_sources():
-    return [os.path.join(CSRC, "sfp_capi.cu")]
+    return [os.path.join(CSRC, "sfp_capi.cu"), os.path.join(CSRC, "sfp_mlp.cu")]
 
 
 def library_headers():

@@ -22,6 +22,8 @@
 
 #include "sfp.h"
 #include "sfp_device.cuh"
+#include "sfp_internal.h"
+#include "sfp_mlp.cuh"
 #include "sfp_run.cuh"
 
 #define SFP_VERSION_STRING "sfparticles_b200 0.1.0 (sm_100a)"
@@ -351,6 +353,8 @@ __global__ void k_inv_gamma(const double* __restrict__ ux, const double* __restr
 }
 
 }  // namespace
+
+int sfp_set_error(int code, const std::string& msg) { return fail(code, msg); }
 
 // ============== find_event_index without allocation (scratch) ===============
 //
@@ -876,6 +880,8 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if (!m) return fail(SFP_EINVAL, "sfp_run_create: NULL module");
     if (cfg->qed != SFP_QED_REJECTION && cfg->qed != SFP_QED_OPTICAL_DEPTH) return fail(SFP_EINVAL, "unknown QED method");
     if (cfg->form != SFP_FORM_FP64 && cfg->form != SFP_FORM_FP32) return fail(SFP_EINVAL, "unknown arithmetic form");
+    if (cfg->mlp_params && cfg->qed != SFP_QED_OPTICAL_DEPTH)
+        return fail(SFP_EINVAL, "the learned photon-energy sampler serves the optical-depth method only");
     const bool f64 = cfg->form == SFP_FORM_FP64;
     const int items = cfg->items > 0 ? cfg->items : (f64 ? 1 : 1);
     const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (f64 ? 2 : 3);
@@ -978,7 +984,9 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     else
         tab = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
     const size_t nc = cfg->qed == SFP_QED_OPTICAL_DEPTH ? 7 : 6;
-    r->smem_m = tab;
+    h.mlp_params = cfg->mlp_params;
+    h.mlp_off = (int)((tab + 127) / 128 * 128);
+    r->smem_m = cfg->mlp_params ? (size_t)h.mlp_off + sizeof(sfp_mlp::Smem) : tab;
     h.ring_off = (int)((tab + 127) / 128 * 128);
     r->smem_p = (size_t)h.ring_off + (size_t)(SFP_TILE_HOST / 32) * stages * (nc * 32 * 8 + 32);
     if ((rc = run_alloc_tiles(r))) return cleanup(rc);

@@ -512,14 +512,16 @@ SFP_DEVICE_INLINE double od_bisect(double chi, double r_uniform, const sfp_od_ta
     return dl + k * (r - y1);
 }
 
-// update_tau_e / update_tau_gamma body for one particle (optical_depth.py:42-62).
-// Draws: purpose 1 -> (tau reset, tau after event), purpose 2 -> inverse-CDF r.
-SFP_DEVICE_INLINE bool od_event(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
-                                const double* rate, unsigned long long seed, unsigned int stream, unsigned int step,
-                                long long slot, double& delta) {
+// update_tau_e / update_tau_gamma body for one particle (optical_depth.py:42-62)
+// up to the energy draw: true on an event, with `u` the uniform that the
+// inverse CDF maps to delta.
+// Draws: purpose 1 -> (tau reset, tau after event), purpose 2 -> inverse-CDF u.
+SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
+                                  const double* rate, unsigned long long seed, unsigned int stream, unsigned int step,
+                                  long long slot, double& u) {
     const double chi_min = pow(10.0, t.log_chi_min);
     if (chi < chi_min) {
-        delta = 0.0;
+        u = 0.0;
         return false;
     }
     const double rtot = od_interp1d(chi, t, rate);
@@ -532,11 +534,21 @@ SFP_DEVICE_INLINE bool od_event(double chi, double ig, double dt, double& tau, c
         double rc, rd;
         uniform2(seed, stream, step, 2u, slot, rc, rd);
         tau = -log(1.0 - rb);
-        delta = od_bisect(chi, rc, t);
+        u = rc;
         return true;
     }
-    delta = 0.0;
+    u = 0.0;
     return false;
+}
+
+// the whole update with the table's inverse CDF for delta
+SFP_DEVICE_INLINE bool od_event(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
+                                const double* rate, unsigned long long seed, unsigned int stream, unsigned int step,
+                                long long slot, double& delta) {
+    double u;
+    const bool ev = od_event_u(chi, ig, dt, tau, t, rate, seed, stream, step, slot, u);
+    delta = ev ? od_bisect(chi, u, t) : 0.0;
+    return ev;
 }
 
 }  // namespace sfp

@@ -63,7 +63,8 @@ struct sfp_run_dev {
     unsigned int* psuper_cnt;     // [max_ptiles / 64 + 1] pair events per super-tile
     long long* psuper_pre;        // [max_ptiles / 64 + 1] exclusive prefix in its chain
     int ring_off;                 // photon kernel: byte offset of the copy ring in dynamic smem
-    int pad2;
+    int mlp_off;                  // massive kernel: byte offset of the network weights in dynamic smem
+    const float* mlp_params;      // learned photon-energy sampler (optical depth), or NULL: the table
     long long max_tiles;
     unsigned int* tile_flag;      // [max_tiles] (epoch << 2) | status
     uint4* tile_agg;              // [max_tiles] per-channel tile counts

@@ -26,6 +26,7 @@
 #pragma once
 #include "sfp_device.cuh"
 #include "sfp_device32.cuh"
+#include "sfp_mlp.cuh"
 #include "sfp_run.cuh"
 
 #ifndef SFP_TILE
@@ -345,13 +346,17 @@ __device__ __forceinline__ sfp_qed_smem sfp_stage_tables(const sfp_run_dev* __re
 }
 
 // photon emission by a massive particle at t (qed/rejection_sampling.py:73-89,
-// optical_depth.py:15-62, hard-photon filter cpu.py:226-231)
+// optical_depth.py:15-62, hard-photon filter cpu.py:226-231).  With the
+// learned sampler (optical depth, R->mlp_params) an event returns, instead of
+// delta, the uniform u its energy is drawn from, with log10 chi and the
+// hard-photon scale hs (1/gamma in float64, gamma in float32); the warp then
+// samples delta with the network and applies the cut (sfp_mlp_events).
 template <int FORM, int QED>
 __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
                                                  const sfp_segment& S, const sfp_instance& I,
                                                  const double* __restrict__ P, double x, double y, double z, double ux,
                                                  double uy, double uz, double t, unsigned int step, long long i,
-                                                 double& tau, double& delta) {
+                                                 double& tau, double& delta, double& hs, double& lchi) {
     using namespace sfp;
     const double dt = R->dt;
     bool ev = false;
@@ -367,10 +372,14 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
                 ev = photon_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
             }
+        } else if (R->mlp_params) {
+            ev = od_event_u(chi, ig, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+            hs = ig;
+            lchi = ev ? log10(chi) : 0.0;
         } else {
             ev = od_event(chi, ig, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
         }
-        if (ev && d / ig < R->photon_threshold) ev = false;
+        if (ev && !(QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) && d / ig < R->photon_threshold) ev = false;
     } else {
         float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (S.push) sfp_field_program32(x, y, z, t, P, F);
@@ -388,6 +397,11 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 d = (double)dl;
                 if (ev && dl * g < (float)R->photon_threshold) ev = false;
             }
+        } else if (R->mlp_params) {
+            ev = od_event_u((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i,
+                            d);
+            hs = (double)g;
+            lchi = ev ? log10((double)chi) : 0.0;
         } else {
             ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
             if (ev && d * (double)g < R->photon_threshold) ev = false;
@@ -446,6 +460,62 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
     }
     delta = d;
     return ev;
+}
+
+// Energies of this warp's emission events from the learned sampler: the
+// events are packed into per-warp rows, run through the network 16 rows per
+// tensor-core tile (sfp_mlp.cuh), and the hard-photon cut is applied.  On
+// entry delta[k] holds each event's uniform u, on exit its delta (0 if cut).
+template <int FORM, int ITEMS>
+__device__ __forceinline__ void sfp_mlp_events(const sfp_run_dev* __restrict__ R, const sfp_mlp::Smem& M,
+                                               bool (&ev)[ITEMS], double (&delta)[ITEMS], const double (&hs)[ITEMS],
+                                               const double (&lchi)[ITEMS]) {
+    constexpr int NW = SFP_TILE / 32;
+    __shared__ float s_x[NW][32 * ITEMS][2];
+    __shared__ float s_y[NW][32 * ITEMS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const unsigned int lt = (1u << lane) - 1u;
+    int rk[ITEMS];
+    int ne = 0;
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        const unsigned int bal = __ballot_sync(0xffffffffu, ev[k]);
+        rk[k] = ne + __popc(bal & lt);
+        if (ev[k]) {
+            s_x[warp][rk[k]][0] = sfp_mlp::feat_chi(lchi[k]);
+            s_x[warp][rk[k]][1] = sfp_mlp::feat_u(delta[k]);
+        }
+        ne += __popc(bal);
+    }
+    if (ne == 0) return;
+    __syncwarp();
+    for (int r0 = 0; r0 < ne; r0 += 16) {
+        float x0[2], x1[2], y[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = r0 + g + 8 * h;
+            x0[h] = r < ne ? s_x[warp][r][0] : 0.0f;
+            x1[h] = r < ne ? s_x[warp][r][1] : 0.0f;
+        }
+        sfp_mlp::tile16(M, x0, x1, y);
+        if (t == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + g + 8 * h;
+                if (r < ne) s_y[warp][r] = y[h];
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        if (!ev[k]) continue;
+        const double d = sfp_mlp::delta_of(s_y[warp][rk[k]]);
+        const bool cut = FORM == SFP_FORM_FP64 ? d / hs[k] < R->photon_threshold : d * hs[k] < R->photon_threshold;
+        ev[k] = !cut;
+        delta[k] = cut ? 0.0 : d;
+    }
+    __syncwarp();
 }
 
 // largest j with start[j] <= tk (binary search over a group's tile starts)
@@ -590,6 +660,9 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
     const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
     const bool any_appends = R->any_appends != 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // learned photon-energy sampler: weights after the tables (staged before the first barrier)
+    sfp_mlp::Smem& M = *reinterpret_cast<sfp_mlp::Smem*>(reinterpret_cast<unsigned char*>(s_tab) + R->mlp_off);
+    if (QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) sfp_mlp::stage(M, R->mlp_params);
 
     while (true) {
         __syncthreads();
@@ -612,12 +685,13 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 
         bool alive[ITEMS], ev[ITEMS];
         double x[ITEMS], y[ITEMS], z[ITEMS], ux[ITEMS], uy[ITEMS], uz[ITEMS], tau[ITEMS], delta[ITEMS];
+        double hs[ITEMS], lchi[ITEMS];  // learned sampler only
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
             const long long i = i0 + (long long)k * SFP_TILE;
             alive[k] = (i < N) && (S.pruned[i] == 0);
             ev[k] = false;
-            delta[k] = 0.0;
+            delta[k] = hs[k] = lchi[k] = 0.0;
             x[k] = y[k] = z[k] = ux[k] = uy[k] = uz[k] = tau[k] = 0.0;
             if (alive[k]) {
                 x[k] = S.x[i]; y[k] = S.y[i]; z[k] = S.z[i];
@@ -630,9 +704,10 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
             if (alive[k] && S.radiating) {
                 const long long i = i0 + (long long)k * SFP_TILE;
                 ev[k] = sfp_photon_event<FORM, QED>(R, T, S, I, P, x[k], y[k], z[k], ux[k], uy[k], uz[k], t, step, i,
-                                                    tau[k], delta[k]);
+                                                    tau[k], delta[k], hs[k], lchi[k]);
             }
         }
+        if (QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) sfp_mlp_events<FORM, ITEMS>(R, M, ev, delta, hs, lchi);
         // tile count (k-major block scan); publish and try the look-back
         unsigned int wpre[ITEMS];
 #pragma unroll

@@ -25,7 +25,7 @@ from typing import Sequence
 
 from . import _lib, program
 from .particles import _device, _stream_ptr
-from .simulation import Simulation, resolve_pending_pairs
+from .simulation import Simulation, observe_rates, plan_chunk, resolve_pending_pairs
 
 
 class Ensemble(object):
@@ -38,9 +38,9 @@ class Ensemble(object):
         for s in sims:
             if s.engine != "fused":
                 raise ValueError("ensemble members use the fused engine")
-            if (s.dt, s.photon_threshold, s.form, s.qed_method) != (first.dt, first.photon_threshold, first.form,
-                                                                     first.qed_method):
-                raise ValueError("ensemble members must share dt, photon_threshold, form and QED method")
+            if (s.dt, s.photon_threshold, s.form, s.qed_method, s.sampler) != (
+                    first.dt, first.photon_threshold, first.form, first.qed_method, first.sampler):
+                raise ValueError("ensemble members must share dt, photon_threshold, form, QED method and sampler")
             if s.fields.structure() != first.fields.structure():
                 raise ValueError("ensemble members must share the field structure (parameters may differ)")
             if (s.step, s.t) != (first.step, first.t):
@@ -159,10 +159,13 @@ class Ensemble(object):
         st = _lib.RunState()
         remaining = int(nstep)
         max_chunk = 4 * self.graph_chunk if self.graph_chunk > 0 else 256
+        rates = self.__dict__.setdefault("_rates", {})
         while remaining > 0:
-            chunk = min(remaining, max_chunk)
-            if self._ensure_headroom():
+            grew, fit = plan_chunk(allp, rates, max_chunk)
+            chunk = min(remaining, max_chunk, fit)
+            if self._ensure_headroom() or grew:
                 self._update_run()
+            before = [p.N_buffered for p in allp]
             _lib.check(L.sfp_run_steps(self._run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
             self.kernel_launches += self._launches_per_step() * chunk + 1
@@ -178,6 +181,7 @@ class Ensemble(object):
                     self._update_run()
                     _lib.check(L.sfp_run_clear_halt(self._run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
+            observe_rates(allp, before, done, rates)
             if done == 0 and not halted:
                 raise _lib.SFPError("the step made no progress")
 

@@ -28,6 +28,10 @@ Extra keyword arguments (no reference counterpart):
   p_stages, p_min_blocks -- photon-kernel variant: depth of the copy ring
                  that streams photon state into shared memory and minimum
                  resident blocks per SM;
+  sampler     -- optical depth only: 'table' (the inverse-CDF table, as in
+                 the reference) or 'mlp', the learned photon-energy sampler
+                 (sfparticles_b200.mlp) evaluated on the tensor cores inside
+                 the step;
   engine      -- 'fused' (the persistent step kernels) or 'ops': the
                  reference's own step loop (simulation.py:102-144) over the
                  one-for-one kernels of the C-ABI (float64, materialised
@@ -68,11 +72,46 @@ def resolve_pending_pairs(run, species, update):
     _lib.check(L.sfp_run_resume(run, _stream_ptr()), "sfp_run_resume")
 
 
+def plan_chunk(species, rates, max_chunk):
+    """Size append destinations for the next chunk of device steps from the
+    append rates seen so far (`rates`: id(species) -> particles per step),
+    and return (grew, chunk).  A destination that cannot take a full chunk
+    at 1.25x its rate grows by the reference rule (particles.py:487-500),
+    each growth capped at half its count so memory stays near its use; the
+    chunk is shortened to what then fits.  Buffer sizes do not change
+    results: they only decide how often the device stops for room."""
+    grew = False
+    chunk = max_chunk
+    for p in species:
+        r = rates.get(id(p), 0.0)
+        if r <= 0.0:
+            continue
+        free = p.buffer_size - p.N_buffered
+        want = int(r * max_chunk * 1.25) + 1
+        if free < want:
+            extra = min(want, p.N_buffered // 2 + 1024)
+            if free < extra:
+                p._extend(extra)
+                grew = True
+            free = p.buffer_size - p.N_buffered
+        chunk = min(chunk, max(1, int(free / (1.25 * r))))
+    return grew, chunk
+
+
+def observe_rates(species, before, steps, rates):
+    """Update the append rates from the counts before and after `steps` steps."""
+    if steps <= 0:
+        return
+    for p, n0 in zip(species, before):
+        r = max(0, p.N_buffered - n0) / steps
+        rates[id(p)] = max(r, 0.5 * rates.get(id(p), 0.0))
+
+
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
                  items: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0,
-                 engine: str = "fused") -> None:
+                 engine: str = "fused", sampler: str = "table") -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -93,6 +132,11 @@ class Simulation(object):
         if engine == "ops" and form != "fp64":
             raise ValueError("the 'ops' engine computes in float64 only")
         self.engine = engine
+        if sampler not in ("table", "mlp"):
+            raise ValueError("sampler must be 'table' or 'mlp'")
+        if sampler == "mlp" and engine != "fused":
+            raise ValueError("the learned photon-energy sampler runs in the fused engine")
+        self.sampler = sampler
         self.graph_chunk = int(graph_chunk)
         self.items = int(items)  # massive kernel: particles per thread per tile (0: the form's default)
         self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
@@ -116,6 +160,9 @@ class Simulation(object):
         if len(ods) > 1:
             raise ValueError("all QED species of a simulation must use the same event method")
         self.qed_method = "od" if ods == {True} else "rs"
+        if self.sampler == "mlp" and self.qed_method != "od":
+            raise ValueError("the learned photon-energy sampler replaces the optical-depth table: "
+                             "set SFPARTICLES_OPTICAL_DEPTH=1")
         from .autotune import DEFAULT
         dm, dp = DEFAULT[(self.form, self.qed_method)]
         if self.items <= 0 or self.min_blocks <= 0:
@@ -207,6 +254,11 @@ class Simulation(object):
         cfg.min_blocks = self.min_blocks
         cfg.p_stages = self.p_stages
         cfg.p_min_blocks = self.p_min_blocks
+        if self.sampler == "mlp":
+            from .mlp import PhotonSampler
+            if getattr(self, "_mlp", None) is None:
+                self._mlp = PhotonSampler.trained()
+            cfg.mlp_params = self._mlp.params.data_ptr()
         if self.qed_method == "od":
             cfg.od_photon, cfg.od_pair = device_tables.od_tables(dev)
         else:
@@ -383,14 +435,17 @@ class Simulation(object):
         # the queued chunk is launched as no-op kernels: bound the chunk so a
         # halt wastes at most a few graphs (one host sync per chunk).
         max_chunk = 4 * self.graph_chunk if self.graph_chunk > 0 else 256
+        rates = self.__dict__.setdefault("_rates", {})
         while remaining > 0:
-            chunk = min(remaining, max_chunk)
+            grew, fit = plan_chunk(self.all_particles, rates, max_chunk)
+            chunk = min(remaining, max_chunk, fit)
             if call_back:
                 chunk = 1
             if self.print_every:
                 chunk = min(chunk, self.print_every - (self.step % self.print_every))
-            if self._ensure_headroom():
+            if self._ensure_headroom() or grew:
                 self._update_run(run)
+            before = [p.N_buffered for p in self.all_particles]
             _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
             self.kernel_launches += self._launches_per_step() * chunk + 1
@@ -406,6 +461,7 @@ class Simulation(object):
                     self._update_run(run)
                     _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
+            observe_rates(self.all_particles, before, done, rates)
             if done == 0 and not halted:
                 raise _lib.SFPError("the step made no progress")
             if call_back and done:

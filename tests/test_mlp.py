@@ -1,0 +1,254 @@
+"""The learned photon-energy sampler: its oracle, training kernels, inference
+kernel and what the trained network gains over the table sampler."""
+import ctypes
+import math
+import os
+
+import numpy as np
+import pytest
+
+import mlp_oracle as mo
+import oracle as orc
+
+
+# ------------------------------------------------------------------- oracle
+def test_bf16_rounding_known_values():
+    # bf16 keeps 7 mantissa bits: the spacing at 1 is 2^-7
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, 1.0 + 3 * 2 ** -9, -2.5], dtype=np.float32)
+    # ties go to even: 1 + 2^-8 -> 1, 1 + 3 2^-8 -> 1 + 2^-6; otherwise nearest
+    np.testing.assert_array_equal(mo.bf16_round(x), [1.0, 1.0, 1.0 + 2 ** -6, 1.0, 1.0 + 2 ** -7, -2.5])
+
+
+def test_oracle_gradient_matches_finite_differences():
+    """The oracle's backward pass against central differences of its own loss
+    (weights unrounded, so the loss is smooth)."""
+    rng = np.random.default_rng(0)
+    from sfparticles_b200.mlp import init_params
+    P = init_params(3).astype(np.float64)
+    x = rng.uniform(-1, 1, (64, 2)).astype(np.float32)
+    t = rng.uniform(-1, 1, 64).astype(np.float32)
+    orig = mo.unpack
+
+    def unrounded(P_, round_weights=True):
+        return orig(P_, round_weights=False)
+
+    mo.unpack = unrounded
+    try:
+        P32 = P.astype(np.float32)
+        _, g = mo.loss_and_grad(P32, x, t)
+        idx = rng.choice(mo.NPARAM, 40, replace=False)
+        for k in idx:
+            h = 1e-3
+            Pp, Pm = P32.copy(), P32.copy()
+            Pp[k] += h
+            Pm[k] -= h
+            fd = (mo.loss_and_grad(Pp, x, t)[0] - mo.loss_and_grad(Pm, x, t)[0]) / (float(Pp[k]) - float(Pm[k]))
+            assert abs(fd - g[k]) <= 1e-4 * max(1.0, abs(g[k])), (k, fd, g[k])
+    finally:
+        mo.unpack = orig
+
+
+# ---------------------------------------------------------------------- GPU
+def _gpu():
+    from gpu_helpers import cuda_or_skip
+    cuda_or_skip()
+
+
+@pytest.mark.gpu
+def test_table_sampler_kernel_matches_oracle():
+    """sfp_od_inverse_cdf (the batched table sampler) vs the oracle's
+    restatement of _bisect_interp on the product's photon table."""
+    _gpu()
+    import torch
+    from sfparticles_b200 import mlp
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    tab = orc.make_od_table(d["photon_rate_total"], d["photon_cumulative"], float(d["log_chi_min"]),
+                            float(d["log_chi_delta"]), float(d["log_delta_min"]), float(d["log_delta_delta"]))
+    rng = np.random.default_rng(5)
+    lc = rng.uniform(-3, 3, 4000)
+    u = rng.uniform(0, 1, 4000)
+    got = mlp.sample_table(torch.as_tensor(lc, device="cuda"), torch.as_tensor(u, device="cuda")).cpu().numpy()
+    L = orc.lib()
+    ref = np.array([L.orc_od_bisect(10.0 ** a, r, ctypes.byref(tab)) for a, r in zip(lc, u)])
+    np.testing.assert_allclose(got, ref, rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_training_gradient_matches_oracle():
+    """One fused forward + backward pass of the training kernel vs the float64
+    oracle, same BF16-rounded weights: loss and every gradient block."""
+    _gpu()
+    import torch
+    from sfparticles_b200 import mlp
+    s = mlp.PhotonSampler(mlp.init_params(11))
+    feat, targ = s.make_samples(5000, seed=7)
+    g, loss = s.grad(feat, targ)
+    lo, go = mo.loss_and_grad(s.params.cpu().numpy(), feat.cpu().numpy(), targ.cpu().numpy())
+    assert abs(loss - lo) <= 1e-5 * lo, (loss, lo)
+    g = g.cpu().numpy().astype(np.float64)
+    for name in ("W0", "b0", "W1", "b1", "W2", "b2", "W3", "b3"):
+        a = mo.OFF[name]
+        keys = list(mo.OFF)
+        b = mo.OFF[keys[keys.index(name) + 1]] if name != "b3" else mo.NPARAM
+        err = np.linalg.norm(g[a:b] - go[a:b]) / (np.linalg.norm(go[a:b]) + 1e-30)
+        print(f"grad {name}: relative L2 error {err:.2e}")
+        assert err < 1e-4, (name, err)
+
+
+@pytest.mark.gpu
+def test_inference_kernel_matches_oracle():
+    """Tensor-core inference vs the oracle's forward pass with the same BF16
+    weights and BF16 activations between the layers (hardware tanh, FP32
+    accumulation order and BF16 rounding ties make up the difference)."""
+    _gpu()
+    import torch
+    from sfparticles_b200 import mlp
+    P = mlp.init_params(4)
+    s = mlp.PhotonSampler(P)
+    rng = np.random.default_rng(8)
+    n = 10_007  # not a multiple of the 16-sample warp tile
+    lc = rng.uniform(-3, 3, n)
+    u = rng.uniform(0, 1, n)
+    got = s.sample(torch.as_tensor(lc, device="cuda"), torch.as_tensor(u, device="cuda")).cpu().numpy()
+    ref = mo.forward_infer(P, lc, u)
+    dl = np.abs(np.log10(got) - np.log10(ref))
+    print(f"|log10 delta| difference: max {dl.max():.2e}, 99.9% {np.quantile(dl, 0.999):.2e}")
+    assert np.quantile(dl, 0.999) < 3e-3 and dl.max() < 2e-2
+
+
+@pytest.mark.gpu
+def test_training_reduces_the_loss():
+    """A short run of the training loop (2e6 samples, 2 epochs) lowers the
+    mean squared error by more than 10x from the initial network's."""
+    _gpu()
+    from sfparticles_b200 import mlp
+    s = mlp.PhotonSampler(mlp.init_params(0))
+    feat, targ = s.make_samples(200_000, seed=3)
+    _, l0 = s.grad(feat, targ)
+    s.train(n_samples=2_000_000, batch=16384, epochs=2, lr=3e-3, report_every=50)
+    _, l1 = s.grad(feat, targ)
+    print(f"mse before {l0 / 2e5:.3e} after {l1 / 2e5:.3e}")
+    assert l1 < 0.1 * l0
+
+
+def _ks(a, b):
+    a = np.sort(a)
+    b = np.sort(b)
+    x = np.concatenate([a, b])
+    fa = np.searchsorted(a, x, side="right") / a.size
+    fb = np.searchsorted(b, x, side="right") / b.size
+    return float(np.max(np.abs(fa - fb)))
+
+
+@pytest.mark.gpu
+def test_trained_sampler_spectrum_and_gain_over_the_table():
+    """The trained network (committed weights, else trained here on 1e8
+    table samples) against the table sampler: KS distance and the first three
+    moments of delta at fixed chi, and what it gains: queries per second on
+    5e7 queries with log10 chi ~ U[-3, 0] (the emitters of the small plain
+    config reach chi ~ 0.6) -- against an untrained network's KS distance."""
+    _gpu()
+    import torch
+    from sfparticles_b200 import mlp
+    s = mlp.PhotonSampler.trained(log=print)
+    dev = "cuda"
+    g = torch.Generator(device=dev).manual_seed(12)
+    worst_ks = 0.0
+    for lc0 in (-2.5, -1.0, 0.0, 1.0, 2.5):
+        n = 1_000_000
+        lc = torch.full((n,), lc0, dtype=torch.float64, device=dev)
+        u = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+        dt = mlp.sample_table(lc, u).cpu().numpy()
+        dm = s.sample(lc, u).cpu().numpy()
+        ks = _ks(dm, dt)
+        mom = [float(np.mean(dm ** k) / np.mean(dt ** k) - 1.0) for k in (1, 2, 3)]
+        print(f"log10 chi {lc0:+.1f}: KS {ks:.4f}, moment ratios - 1 {mom[0]:+.4f} {mom[1]:+.4f} {mom[2]:+.4f}")
+        worst_ks = max(worst_ks, ks)
+        assert ks < 0.01, (lc0, ks)
+        # E[delta^k] leans on the rarer hardest photons as k grows
+        assert abs(mom[0]) < 0.01 and abs(mom[1]) < 0.02 and abs(mom[2]) < 0.03, (lc0, mom)
+    # untrained network: the training is what makes it a sampler
+    raw = mlp.PhotonSampler(mlp.init_params(0))
+    lc = torch.full((200_000,), 0.0, dtype=torch.float64, device=dev)
+    u = torch.rand(200_000, dtype=torch.float64, device=dev, generator=g)
+    ks_raw = _ks(raw.sample(lc, u).cpu().numpy(), mlp.sample_table(lc, u).cpu().numpy())
+    print(f"untrained network KS at chi = 1: {ks_raw:.3f}")
+    assert ks_raw > 10 * worst_ks
+    # speed on a 5e7-query batch
+    n = 50_000_000
+    lc = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 3.0 - 3.0
+    u = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    times = {}
+    for name, fn in (("table", lambda: mlp.sample_table(lc, u)), ("mlp", lambda: s.sample(lc, u))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / 3
+    print(f"5e7 queries: table {times['table']:.2f} ms, mlp {times['mlp']:.2f} ms, "
+          f"gain x{times['table'] / times['mlp']:.2f}")
+
+
+def _c1_od_sim(S, n, seed, form, sampler):
+    """The small plain config's beam and pulse (a0 = 50, dt = T0/50) at n
+    electrons, optical-depth method, photons only (the config makes no
+    pairs)."""
+    from sfparticles_b200 import qed
+    from sfparticles_b200.fields import gaussian_laser_pulse
+    C = 299792458.0
+    T0 = 0.8e-6 / C
+    steps = 1500
+    L = C * steps * (T0 / 50) / 2
+    rng = np.random.default_rng(seed)
+    g = 2000 * (1 + 0.01 * rng.normal(size=n))
+    props = (rng.normal(-L, 5e-6, n), rng.normal(0, 1e-6, n), rng.normal(0, 1e-6, n), np.sqrt(g * g - 1),
+             np.zeros(n), np.zeros(n))
+    qed.set_method("od")
+    try:
+        ele = S.Particles("ele", -1, 1, N=n, props=props)
+        pho = S.Particles("pho", 0, 0)
+        ele.set_photon(pho)
+    finally:
+        qed.set_method("rs")
+    ctau = C * 25e-15 / (2 * math.sqrt(math.log(2) / 2))
+    fld = gaussian_laser_pulse(50.0, 3e-6, ctau, direction=-1, x0=L)
+    return S.Simulation(ele, pho, dt=T0 / 50, fields=fld, print_every=None, seed=seed, form=form,
+                        sampler=sampler), steps
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_step_with_learned_sampler_matches_table_spectrum(form):
+    """The small plain config (optical depth, 1e5 electrons, 1500 steps, two
+    seeds) stepped with the learned sampler inside the fused step and with
+    the table: the emitted-photon spectrum (64 log bins above 2 m c^2)
+    differs by <= 2 % relative L1 and the photon number and mean electron
+    energy agree within 3 sigma of the seed-to-seed scatter."""
+    _gpu()
+    import sfparticles_b200 as S
+    from sfparticles_b200 import diagnostics as D
+    res = {}
+    for sampler in ("table", "mlp"):
+        spec, nph, eg = None, [], []
+        for seed in (21, 22):
+            sim, steps = _c1_od_sim(S, 100_000, seed, form, sampler)
+            sim.start(steps)
+            ele, pho = sim.all_particles
+            h, _ = D.photon_spectrum(pho, 64, 2.0, 4000.0)
+            spec = h if spec is None else spec + h
+            nph.append(pho.N_buffered)
+            eg.append(float(np.mean(ele.gamma)))
+        res[sampler] = (spec, np.array(nph, float), np.array(eg))
+    (st, nt, gt), (sm, nm, gm) = res["table"], res["mlp"]
+    l1 = D.spectrum_rel_l1(sm, st)
+    floor = math.sqrt(64.0 / st.sum())
+    print(f"{form}: photons table {nt.sum():.0f} mlp {nm.sum():.0f}; spectrum rel L1 {l1:.4f} "
+          f"(Poisson floor ~{floor:.4f}); <gamma_e> table {gt.mean():.2f} mlp {gm.mean():.2f}")
+    assert l1 <= 0.02, l1
+    assert abs(nm.sum() - nt.sum()) <= 3 * math.sqrt(nt.sum() + nm.sum())
+    assert abs(gm.mean() - gt.mean()) <= 0.01 * gt.mean()
