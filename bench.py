@@ -179,6 +179,201 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
+WORKLOAD_C3 = "learned photon-energy sampler: 5e7 queries per step, log10 chi ~ U[-3,0] (the small plain config's " \
+              "emitters reach chi ~ 0.6), u ~ U(0,1); MLP 2-64-64-64-1 SiLU, BF16 weights, FP32 accumulation"
+MLP_FLOP_PER_QUERY = 2 * (2 * 64 + 2 * 64 * 64 + 64)  # 16768
+
+
+def measured_peak_bf16():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_c3(args):
+    """Learned sampler vs the table sampler on a batch of emission events."""
+    import torch
+    import sfparticles_b200  # noqa: F401 (loads the library)
+    from sfparticles_b200 import mlp
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n = args.queries
+    g = torch.Generator(device=dev).manual_seed(3)
+    lc = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 3.0 - 3.0
+    u = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    s = mlp.PhotonSampler.trained()
+    out = {}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk_summary = None
+    for name, fn in (("table", lambda: mlp.sample_table(lc, u)), ("mlp", lambda: s.sample(lc, u))):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        with ClockSampler(dev.index) as clk:
+            e0.record()
+            for _ in range(args.steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / args.steps
+        if name == "mlp":
+            clk_summary = clk.summary()
+    # end to end through the public API: host arrays in, host delta out
+    hl = lc.cpu().pin_memory()
+    hu = u.cpu().pin_memory()
+    hd = torch.empty(n, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(args.steps):
+        dl = hl.to(dev, non_blocking=True)
+        du = hu.to(dev, non_blocking=True)
+        hd.copy_(s.sample(dl, du), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / args.steps
+    # training throughput of the hand-written kernels (one epoch over 1e7 samples)
+    t = mlp.PhotonSampler(mlp.init_params(0))
+    feat, targ = t.make_samples(10_000_000, seed=5)
+    gbuf = torch.zeros(mlp.NPARAM, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    e0.record()
+    for lo in range(0, 10_000_000, 65536):
+        m = min(65536, 10_000_000 - lo)
+        t.grad(feat[lo:lo + m], targ[lo:lo + m])
+    e1.record()
+    torch.cuda.synchronize()
+    train_sps = 1e7 / (e0.elapsed_time(e1) * 1e-3)
+    # accuracy vs the table at fixed chi
+    acc = {}
+    for lc0 in (-2.5, -1.0, 0.0, 1.0, 2.5):
+        m = 1_000_000
+        a = torch.full((m,), lc0, dtype=torch.float64, device=dev)
+        b = torch.rand(m, dtype=torch.float64, device=dev, generator=g)
+        dt = mlp.sample_table(a, b).cpu().numpy()
+        dm = s.sample(a, b).cpu().numpy()
+        xs = np.concatenate([np.sort(dt), np.sort(dm)])
+        ks = float(np.max(np.abs(np.searchsorted(np.sort(dt), xs, side="right") / m
+                                 - np.searchsorted(np.sort(dm), xs, side="right") / m)))
+        acc[f"log10chi={lc0:+.1f}"] = {"ks": ks, "moment_ratio_minus_1": [
+            float(np.mean(dm ** k) / np.mean(dt ** k) - 1.0) for k in (1, 2, 3)]}
+    peak, peak_kind = measured_peak_bf16()
+    tflops = MLP_FLOP_PER_QUERY * n / (out["mlp"] * 1e-3) / 1e12
+    value = n / (out["mlp"] * 1e-3)
+    line = {"metric": "delta samples/s", "value": value, "unit": "samples/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["mlp"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16/f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD_C3, "queries_per_step": n,
+                       "l2": "inputs 0.8 GB + output 0.4 GB per step, larger than L2 (no flush needed)"},
+            "roofline": {"bound": "tensor", "kernel": "k_mlp_infer", "achieved": tflops, "peak": peak,
+                         "unit": "TFLOP/s", "frac": tflops / peak, "traffic": None, "peak_kind": peak_kind,
+                         "flop_per_query": MLP_FLOP_PER_QUERY},
+            "table_sampler": {"ms_per_step": out["table"], "samples_per_s": n / (out["table"] * 1e-3)},
+            "mlp_over_table_speed": out["table"] / out["mlp"],
+            "training": {"samples_per_s_fwd_bwd": train_sps},
+            "accuracy_vs_table": acc,
+            "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "cpu_baseline": None, "gpu_launches": 2 * (args.steps + args.warmup), "clocks": clk_summary}
+    print(json.dumps(line), flush=True)
+
+
+WORKLOAD_C5 = "spin + radiation-reaction avalanche: 5e6 e- at rest (uniform 2um cube, spin +z) between two " \
+              "counter-propagating circularly polarised Gaussian pulses a0=800 (0.8um, w0 4um, 30fs FWHM; each the sum " \
+              "of two linear pulses, pol 0 / pi/2, cep offset pi/2, amplitude a0/sqrt2), Boris-TBMT spin push, photon " \
+              "emission (optical depth, learned sampler) + recoil + pairs, dt=T0/100, until 2500 steps or 1e9 particles"
+
+
+def make_c5(n, form="fp32", sampler="mlp", seed=0):
+    import sfparticles_b200 as S
+    from sfparticles_b200 import qed
+    from sfparticles_b200.fields import gaussian_laser_pulse
+    rng = np.random.default_rng(seed)
+    qed.set_method("od")
+    try:
+        props = (rng.uniform(-1e-6, 1e-6, n), rng.uniform(-1e-6, 1e-6, n), rng.uniform(-1e-6, 1e-6, n),
+                 np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n), np.ones(n))
+        ele = S.SpinParticles("electron", -1, 1, N=n, props=props)
+        pos = S.SpinParticles("positron", 1, 1)  # pairs are created without spin
+        pho = S.Particles("photon", 0, 0)
+        ele.set_photon(pho)
+        pos.set_photon(pho)
+        pho.set_pair(ele, pos)
+    finally:
+        qed.set_method("rs")
+    ctau = C * 30e-15 / (2 * math.sqrt(math.log(2) / 2))
+    a = 800.0 / math.sqrt(2.0)
+    xm = 10e-6  # the pulse centres start 10 um from the target and meet there after ~33 fs
+    fld = None
+    for d, x0 in ((1, -xm), (-1, xm)):
+        for pol, cep in ((0.0, 0.0), (math.pi / 2, math.pi / 2)):
+            f = gaussian_laser_pulse(a, 4e-6, ctau, direction=d, x0=x0, pol_angle=pol, cep=cep)
+            fld = f if fld is None else fld + f
+    return S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form, sampler=sampler)
+
+
+def run_c5(args):
+    """The avalanche config: particle-steps/s until the step limit or the particle cap."""
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    w = make_c5(1000, args.form)
+    w.run_on_device(args.warmup)
+    w.finish()
+    del w
+    sim = make_c5(args.electrons_c5, args.form)
+    sim._begin()
+    torch.cuda.synchronize()
+    launches0 = sim.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    done = 0
+    with ClockSampler(dev.index) as clk:
+        e0.record()
+        while done < args.steps and sum(p.N_buffered for p in sim.all_particles) < args.particle_cap:
+            k = min(64, args.steps - done)
+            sim.run_on_device(k)
+            done += k
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    counts = {p.name: p.N_buffered for p in sim.all_particles}
+    alive = {p.name: p.Npart for p in sim.all_particles}
+    kms, before, after = sim.time_step_kernel(args.roofline_steps)
+    k_ms = [float(np.mean([q[j] for q in kms])) for j in range(3)] if kms else [0.0, 0.0, 0.0]
+    ps = sim.particle_steps
+    launches = sim.kernel_launches - launches0
+    sim.finish()
+    n_epm = alive["electron"] + alive["positron"]
+    alg_m = n_epm * (BYTES_EPM + 16 + 48)  # + optical depth, + spin (read and written)
+    alg_p = alive["photon"] * (BYTES_PHOTON + 8)  # + optical depth
+    peak, peak_kind = measured_peak_hbm()
+    per_kernel = {
+        "massive": {"avg_ms": k_ms[0], "alg_bytes_per_launch": alg_m,
+                    "achieved_gbs": alg_m / (k_ms[0] * 1e-3) / 1e9 if k_ms[0] else 0.0},
+        "photon": {"avg_ms": k_ms[1], "alg_bytes_per_launch": alg_p,
+                   "achieved_gbs": alg_p / (k_ms[1] * 1e-3) / 1e9 if k_ms[1] else 0.0},
+        "pairs": {"avg_ms": k_ms[2]}}
+    dominant = max(("massive", "photon"), key=lambda k: per_kernel[k]["avg_ms"])
+    dk = per_kernel[dominant]
+    line = {"metric": "particle-steps/s", "value": ps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": done, "warmup": args.warmup, "ms_per_step": ms / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_C5, "form": args.form, "electrons_initial": args.electrons_c5,
+                       "particle_cap": args.particle_cap, "steps_run": done, "final_counts": counts,
+                       "l2": "state larger than L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": dk["achieved_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": dk["achieved_gbs"] / peak, "traffic": None, "peak_kind": peak_kind,
+                         "per_kernel": per_kernel, "launches_timed": len(kms)},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk.summary(),
+            "particle_steps": ps}
+    print(json.dumps(line), flush=True)
+
+
 def make_oracle_sim(n, seed):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as orc
@@ -451,8 +646,13 @@ def main():
     ap.add_argument("--steps", type=int, default=STEPS_FULL)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
-                    help="c2: the scaled cascade (default); c4: 256 batched uneven instances (2000 steps)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the scaled cascade (default); c3: the learned photon-energy sampler on 5e7 "
+                         "queries per step; c4: 256 batched uneven instances (2000 steps); c5: the spin + "
+                         "radiation-reaction avalanche to 1e9 particles")
+    ap.add_argument("--queries", type=int, default=50_000_000, help="c3: queries per step")
+    ap.add_argument("--electrons-c5", type=int, default=5_000_000, help="c5: electrons at rest")
+    ap.add_argument("--particle-cap", type=int, default=1_000_000_000, help="c5: stop at this many particles")
     ap.add_argument("--electrons", type=int, default=10_000_000)
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--compare-electrons", type=int, default=1_000_000)
@@ -474,6 +674,24 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "c3":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "c3",
+                              "unavailable": "the learned-sampler mode runs one GPU, product arm only"}))
+            return
+        if args.steps == STEPS_FULL:
+            args.steps = 20
+        run_c3(args)
+        return
+    if args.workload == "c5":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "c5",
+                              "unavailable": "the avalanche mode runs one GPU, product arm only"}))
+            return
+        if args.steps == STEPS_FULL:
+            args.steps = 2500
+        run_c5(args)
+        return
     if args.workload == "c4":
         if args.impl != "ours" or world != 1:
             print(json.dumps({"impl": args.impl, "workload": "c4",

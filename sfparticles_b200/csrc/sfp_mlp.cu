@@ -340,7 +340,9 @@ __global__ void k_mlp_adam(float* __restrict__ P, const float* __restrict__ g, f
 }
 
 // --------------------------------------------------------------- inference
-// one warp per 16-sample tile (sfp_mlp.cuh), tiles strided over the grid
+// one warp per 16-sample tile (sfp_mlp.cuh), strided over the grid.  (Two
+// tiles per warp share the B-fragment reads but need ~120 registers; the
+// lower occupancy made them slower on this latency-bound kernel.)
 __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ P, const double* __restrict__ lc,
                                                    const double* __restrict__ u, double* __restrict__ out,
                                                    long long n) {

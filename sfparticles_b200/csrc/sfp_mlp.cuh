@@ -8,7 +8,7 @@
 //   W0[64][2] b0[64] W1[64][64] b1[64] W2[64][64] b2[64] W3[64] b3
 // (row j of W = the weights of output unit j).
 //
-// A warp evaluates 16 samples at a time.  The two 64x64 layers run on the
+// A warp evaluates 16 or 32 samples at a time.  The two 64x64 layers run on the
 // tensor cores (mma.sync m16n8k16, BF16 in, FP32 accumulate), and the
 // accumulators of one layer become the A fragments of the next in
 // registers.  Thread (g, t) = (lane / 4, lane % 4) holds rows g and g + 8,
@@ -40,7 +40,12 @@ SFP_DEVICE_INLINE unsigned f2bf(float f) {
 }
 SFP_DEVICE_INLINE float bf2f(unsigned h) { return __uint_as_float(h << 16); }
 SFP_DEVICE_INLINE float bf16r(float f) { return bf2f(f2bf(f)); }
-SFP_DEVICE_INLINE unsigned pack(float lo, float hi) { return f2bf(lo) | (f2bf(hi) << 16); }
+// two floats -> packed BF16 pair (lo in the low half), round to nearest even
+SFP_DEVICE_INLINE unsigned pack(float lo, float hi) {
+    unsigned d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
 
 // all threads of the block; a __syncthreads must follow
 SFP_DEVICE_INLINE void stage(Smem& S, const float* __restrict__ P) {
@@ -85,18 +90,22 @@ SFP_DEVICE_INLINE void mma(float (&d)[4], const unsigned (&a)[4], unsigned b0, u
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// C[nt] = A x W^T for one 64 -> 64 layer (A: four k16 fragments)
-SFP_DEVICE_INLINE void layer(const unsigned short (*W)[WLD], const unsigned (&A)[4][4], float (&C)[8][4], int g,
-                             int t) {
+// C[m][nt] = A[m] x W^T for one 64 -> 64 layer, MT row tiles of 16 (each
+// A[m]: four k16 fragments); every B fragment read serves all MT tiles
+template <int MT>
+SFP_DEVICE_INLINE void layer(const unsigned short (*W)[WLD], const unsigned (&A)[MT][4][4], float (&C)[MT][8][4],
+                             int g, int t) {
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
-        C[nt][0] = C[nt][1] = C[nt][2] = C[nt][3] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < MT; ++m) C[m][nt][0] = C[m][nt][1] = C[m][nt][2] = C[m][nt][3] = 0.0f;
         const unsigned short* row = W[8 * nt + g];
 #pragma unroll
         for (int kc = 0; kc < 4; ++kc) {
             const unsigned b0 = *reinterpret_cast<const unsigned*>(row + 16 * kc + 2 * t);
             const unsigned b1 = *reinterpret_cast<const unsigned*>(row + 16 * kc + 8 + 2 * t);
-            mma(C[nt], A[kc], b0, b1);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) mma(C[m][nt], A[m][kc], b0, b1);
         }
     }
 }
@@ -113,41 +122,57 @@ SFP_DEVICE_INLINE void to_fragments(const float (&C)[8][4], const float* b, unsi
     }
 }
 
-// One 16-row tile, called by all 32 lanes: x0[h], x1[h] are the features of
-// rows g + 8 h; returns the outputs y[h] of those rows (in every lane of the
-// group of four).
-SFP_DEVICE_INLINE void tile16(const Smem& S, const float (&x0)[2], const float (&x1)[2], float (&y)[2]) {
+// MT tiles of 16 rows, called by all 32 lanes: x0[m][h], x1[m][h] are the
+// features of row g + 8 h of tile m; returns the outputs y[m][h] of those
+// rows (in every lane of the group of four).
+template <int MT>
+SFP_DEVICE_INLINE void tiles(const Smem& S, const float (&x0)[MT][2], const float (&x1)[MT][2], float (&y)[MT][2]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    unsigned A[4][4];
+    unsigned A[MT][4][4];
 #pragma unroll
-    for (int kc = 0; kc < 4; ++kc) {
+    for (int m = 0; m < MT; ++m)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int h = r & 1, c = 16 * kc + 2 * t + ((r >> 1) ? 8 : 0);
-            const float z0 = fmaf(S.W0[c][0], x0[h], fmaf(S.W0[c][1], x1[h], S.b0[c]));
-            const float z1 = fmaf(S.W0[c + 1][0], x0[h], fmaf(S.W0[c + 1][1], x1[h], S.b0[c + 1]));
-            A[kc][r] = pack(silu_fast(z0), silu_fast(z1));
+        for (int kc = 0; kc < 4; ++kc) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int h = r & 1, c = 16 * kc + 2 * t + ((r >> 1) ? 8 : 0);
+                const float z0 = fmaf(S.W0[c][0], x0[m][h], fmaf(S.W0[c][1], x1[m][h], S.b0[c]));
+                const float z1 = fmaf(S.W0[c + 1][0], x0[m][h], fmaf(S.W0[c + 1][1], x1[m][h], S.b0[c + 1]));
+                A[m][kc][r] = pack(silu_fast(z0), silu_fast(z1));
+            }
+        }
+    float C[MT][8][4];
+    layer<MT>(S.W1, A, C, g, t);
+#pragma unroll
+    for (int m = 0; m < MT; ++m) to_fragments(C[m], S.b1, A[m], t);
+    layer<MT>(S.W2, A, C, g, t);
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+        y[m][0] = y[m][1] = 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const int c = 8 * nt + 2 * t;
+            y[m][0] = fmaf(S.W3[c], silu_fast(C[m][nt][0] + S.b2[c]), y[m][0]);
+            y[m][0] = fmaf(S.W3[c + 1], silu_fast(C[m][nt][1] + S.b2[c + 1]), y[m][0]);
+            y[m][1] = fmaf(S.W3[c], silu_fast(C[m][nt][2] + S.b2[c]), y[m][1]);
+            y[m][1] = fmaf(S.W3[c + 1], silu_fast(C[m][nt][3] + S.b2[c + 1]), y[m][1]);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            y[m][h] += __shfl_xor_sync(0xffffffffu, y[m][h], 1);
+            y[m][h] += __shfl_xor_sync(0xffffffffu, y[m][h], 2);
+            y[m][h] += S.b3;
         }
     }
-    float C[8][4];
-    layer(S.W1, A, C, g, t);
-    to_fragments(C, S.b1, A, t);
-    layer(S.W2, A, C, g, t);
-    y[0] = y[1] = 0.0f;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        const int c = 8 * nt + 2 * t;
-        y[0] = fmaf(S.W3[c], silu_fast(C[nt][0] + S.b2[c]), y[0]);
-        y[0] = fmaf(S.W3[c + 1], silu_fast(C[nt][1] + S.b2[c + 1]), y[0]);
-        y[1] = fmaf(S.W3[c], silu_fast(C[nt][2] + S.b2[c]), y[1]);
-        y[1] = fmaf(S.W3[c + 1], silu_fast(C[nt][3] + S.b2[c + 1]), y[1]);
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        y[h] += __shfl_xor_sync(0xffffffffu, y[h], 1);
-        y[h] += __shfl_xor_sync(0xffffffffu, y[h], 2);
-        y[h] += S.b3;
-    }
+}
+
+// one 16-row tile (the in-step sampler: a warp's few events)
+SFP_DEVICE_INLINE void tile16(const Smem& S, const float (&x0)[2], const float (&x1)[2], float (&y)[2]) {
+    const float a0[1][2] = {{x0[0], x0[1]}}, a1[1][2] = {{x1[0], x1[1]}};
+    float r[1][2];
+    tiles<1>(S, a0, a1, r);
+    y[0] = r[0][0];
+    y[1] = r[0][1];
 }
 
 }  // namespace sfp_mlp
