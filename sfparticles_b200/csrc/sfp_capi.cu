@@ -331,6 +331,7 @@ __global__ void k_update_tau(double* __restrict__ tau, const double* __restrict_
                              double dt, long long N, const unsigned char* __restrict__ pr, unsigned char* __restrict__ ev,
                              double* __restrict__ delta, sfp_od_table tab, unsigned long long seed,
                              unsigned int stream, unsigned int step) {
+    const double chi_min = pow(10.0, tab.log_chi_min);  // _chi_min, optical_depth.py:14
     GRID_STRIDE(i, N) {
         if (pr[i]) {
             ev[i] = 0;
@@ -338,7 +339,7 @@ __global__ void k_update_tau(double* __restrict__ tau, const double* __restrict_
             continue;
         }
         double tv = tau[i], d = 0.0;
-        const bool e = sfp::od_event(chi[i], ig[i], dt, tv, tab, tab.rate_total, seed, stream, step, i, d);
+        const bool e = sfp::od_event(chi[i], ig[i], dt, tv, tab, tab.rate_total, chi_min, seed, stream, step, i, d);
         tau[i] = tv;
         ev[i] = e ? 1 : 0;
         delta[i] = d;

@@ -514,23 +514,30 @@ SFP_DEVICE_INLINE double od_bisect(double chi, double r_uniform, const sfp_od_ta
 
 // update_tau_e / update_tau_gamma body for one particle (optical_depth.py:42-62)
 // up to the energy draw: true on an event, with `u` the uniform that the
-// inverse CDF maps to delta.
-// Draws: purpose 1 -> (tau reset, tau after event), purpose 2 -> inverse-CDF u.
+// inverse CDF maps to delta.  chi_min = 10^log_chi_min, computed once by the
+// caller (the reference's module constant _chi_min, optical_depth.py:14).
+// Draws, taken only when needed as in the reference (counter-based, so
+// identical to drawing always): purpose 1 -> (tau reset, tau after event),
+// purpose 2 -> inverse-CDF u.
 SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
-                                  const double* rate, unsigned long long seed, unsigned int stream, unsigned int step,
-                                  long long slot, double& u) {
-    const double chi_min = pow(10.0, t.log_chi_min);
+                                  const double* rate, double chi_min, unsigned long long seed, unsigned int stream,
+                                  unsigned int step, long long slot, double& u) {
     if (chi < chi_min) {
         u = 0.0;
         return false;
     }
     const double rtot = od_interp1d(chi, t, rate);
     const double dtau = dt * ig;
-    double ra, rb;
-    uniform2(seed, stream, step, 1u, slot, ra, rb);
-    if (tau == 0.0) tau = -log(1.0 - ra);
+    double ra = 0.0, rb = 0.0;
+    bool drawn = false;
+    if (tau == 0.0) {
+        uniform2(seed, stream, step, 1u, slot, ra, rb);
+        drawn = true;
+        tau = -log(1.0 - ra);
+    }
     tau -= rtot * dtau;
     if (tau < 0.0) {
+        if (!drawn) uniform2(seed, stream, step, 1u, slot, ra, rb);
         double rc, rd;
         uniform2(seed, stream, step, 2u, slot, rc, rd);
         tau = -log(1.0 - rb);
@@ -543,10 +550,10 @@ SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau,
 
 // the whole update with the table's inverse CDF for delta
 SFP_DEVICE_INLINE bool od_event(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
-                                const double* rate, unsigned long long seed, unsigned int stream, unsigned int step,
-                                long long slot, double& delta) {
+                                const double* rate, double chi_min, unsigned long long seed, unsigned int stream,
+                                unsigned int step, long long slot, double& delta) {
     double u;
-    const bool ev = od_event_u(chi, ig, dt, tau, t, rate, seed, stream, step, slot, u);
+    const bool ev = od_event_u(chi, ig, dt, tau, t, rate, chi_min, seed, stream, step, slot, u);
     delta = ev ? od_bisect(chi, u, t) : 0.0;
     return ev;
 }

@@ -305,6 +305,7 @@ struct sfp_qed_smem {
     float inv_dzf;
     float base_maxf;
     double chi_pair_min;  // below: no pair event is possible (z_min > z_max)
+    double od_chi_min_ph, od_chi_min_pa;  // optical depth: 10^log_chi_min of each table
 };
 
 template <int FORM, int QED>
@@ -342,6 +343,8 @@ __device__ __forceinline__ sfp_qed_smem sfp_stage_tables(const sfp_run_dev* __re
     T.base_maxf = (float)(T.zmax * sqrt(T.zmax));
     // pair creation needs z_min = (4/chi)^(2/3) <= z_max: exact cut with margin
     T.chi_pair_min = QED == SFP_QED_REJECTION ? 4.0 / (T.zmax * sqrt(T.zmax)) * (1.0 - 1e-6) : 0.0;
+    T.od_chi_min_ph = QED == SFP_QED_OPTICAL_DEPTH ? pow(10.0, R->od_photon.log_chi_min) : 0.0;
+    T.od_chi_min_pa = QED == SFP_QED_OPTICAL_DEPTH ? pow(10.0, R->od_pair.log_chi_min) : 0.0;
     return T;
 }
 
@@ -373,11 +376,11 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 ev = photon_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
             }
         } else if (R->mlp_params) {
-            ev = od_event_u(chi, ig, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+            ev = od_event_u(chi, ig, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed, S.stream, step, i, d);
             hs = ig;
             lchi = ev ? log10(chi) : 0.0;
         } else {
-            ev = od_event(chi, ig, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+            ev = od_event(chi, ig, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed, S.stream, step, i, d);
         }
         if (ev && !(QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) && d / ig < R->photon_threshold) ev = false;
     } else {
@@ -398,12 +401,13 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 if (ev && dl * g < (float)R->photon_threshold) ev = false;
             }
         } else if (R->mlp_params) {
-            ev = od_event_u((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i,
-                            d);
+            ev = od_event_u((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed,
+                            S.stream, step, i, d);
             hs = (double)g;
             lchi = ev ? log10((double)chi) : 0.0;
         } else {
-            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, I.seed, S.stream, step, i, d);
+            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed,
+                          S.stream, step, i, d);
             if (ev && d * (double)g < R->photon_threshold) ev = false;
         }
         if (!ev) d = 0.0;
@@ -436,7 +440,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                 ev = pair_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
             }
         } else {
-            ev = od_event(chi, ig, dt, tau, R->od_pair, T.od_pa, I.seed, S.stream, step, i, d);
+            ev = od_event(chi, ig, dt, tau, R->od_pair, T.od_pa, T.od_chi_min_pa, I.seed, S.stream, step, i, d);
         }
     } else {
         float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -454,7 +458,8 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                 d = (double)r1;
             }
         } else {
-            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_pair, T.od_pa, I.seed, S.stream, step, i, d);
+            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_pair, T.od_pa, T.od_chi_min_pa, I.seed,
+                          S.stream, step, i, d);
         }
         if (!ev) d = 0.0;
     }
