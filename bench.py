@@ -342,7 +342,9 @@ def run_c5(args):
     ms = e0.elapsed_time(e1)
     counts = {p.name: p.N_buffered for p in sim.all_particles}
     alive = {p.name: p.Npart for p in sim.all_particles}
+    torch.cuda.nvtx.range_push("roofline")  # profilers select these launches by this range
     kms, before, after = sim.time_step_kernel(args.roofline_steps)
+    torch.cuda.nvtx.range_pop()
     k_ms = [float(np.mean([q[j] for q in kms])) for j in range(3)] if kms else [0.0, 0.0, 0.0]
     ps = sim.particle_steps
     launches = sim.kernel_launches - launches0
