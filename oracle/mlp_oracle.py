@@ -80,7 +80,9 @@ def features(log_chi, u):
     """The network's input features, as the kernels compute them (float32)."""
     f0 = (np.asarray(log_chi, dtype=np.float64) / 3.0).astype(np.float32)
     u = np.clip(np.asarray(u, dtype=np.float64), 2.0 ** -53, 1.0 - 2.0 ** -53)
-    f1 = ((np.log(u) - np.log1p(-u)) * 0.125).astype(np.float32)
+    lu = np.log(u.astype(np.float32))
+    lv = np.log((1.0 - u).astype(np.float32))
+    f1 = ((lu - lv) * np.float32(0.125)).astype(np.float32)
     return np.stack([f0, f1], axis=1)
 
 
@@ -91,5 +93,6 @@ def forward_infer(P, log_chi, u):
     a1 = bf16_round(_silu(x @ W0.T + b0)[0])
     a2 = bf16_round(_silu(a1 @ W1.T + b1)[0])
     a3 = _silu(a2 @ W2.T + b2)[0]
-    y = a3 @ W3 + b3
-    return np.clip(10.0 ** (3.0 * (y - 1.0)), 1e-6, 1.0)
+    y = (a3 @ W3 + b3).astype(np.float32)
+    d = np.exp2((y - np.float32(1.0)) * np.float32(3.0 * np.log2(10.0))).astype(np.float64)
+    return np.clip(d, 1e-6, 1.0)

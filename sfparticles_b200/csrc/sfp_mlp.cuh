@@ -65,14 +65,17 @@ SFP_DEVICE_INLINE void stage(Smem& S, const float* __restrict__ P) {
 }
 
 SFP_DEVICE_INLINE float feat_chi(double log_chi) { return (float)(log_chi / 3.0); }
-// u is kept inside [2^-53, 1 - 2^-53] so that the logit stays finite
+// logit(u) / 8 in float32: u is kept inside [2^-53, 1 - 2^-53] so that the
+// logit stays finite, and 1 - u is formed in float64 first so that the tail
+// (u near 1) keeps its relative precision
 SFP_DEVICE_INLINE float feat_u(double u) {
     u = fmin(fmax(u, 0x1p-53), 1.0 - 0x1p-53);
-    return (float)((log(u) - log1p(-u)) * 0.125);
+    return (logf((float)u) - logf((float)(1.0 - u))) * 0.125f;
 }
+// delta = 10^(3 (y - 1)) in float32, clamped to [1e-6, 1]
 SFP_DEVICE_INLINE double delta_of(float y) {
-    const double d = exp10(3.0 * ((double)y - 1.0));
-    return d < 1e-6 ? 1e-6 : (d > 1.0 ? 1.0 : d);
+    const float d = exp2f((y - 1.0f) * (3.0f * 3.32192809488736234787f));  // 3 log2(10)
+    return d < 1e-6f ? 1e-6 : (d > 1.0f ? 1.0 : (double)d);
 }
 
 // SiLU through one hardware tanh: z sigma(z) = z (1 + tanh(z / 2)) / 2
