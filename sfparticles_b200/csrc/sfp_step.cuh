@@ -669,12 +669,16 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
     sfp_mlp::Smem& M = *reinterpret_cast<sfp_mlp::Smem*>(reinterpret_cast<unsigned char*>(s_tab) + R->mlp_off);
     if (QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) sfp_mlp::stage(M, R->mlp_params);
 
+    // thread 0 takes the next tile's ticket while the current tile computes
+    int next_tk = 0;
+    if (threadIdx.x == 0) next_tk = atomicAdd(&st->mticket, 1);
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) {
-            const long long tk = (long long)atomicAdd(&st->mticket, 1);
+            const long long tk = (long long)next_tk;
             s_tile = tk;
             s_pos = tk < n_tiles ? sfp_find_group_pos(R->mtile_start, R->n_mseg, tk) : 0;
+            if (tk < n_tiles) next_tk = atomicAdd(&st->mticket, 1);
         }
         __syncthreads();
         const long long tile = s_tile;
