@@ -616,14 +616,8 @@ def run_ours(args, rank, world):
         torch.cuda.empty_cache()
 
     # max over ranks of the device time; sum of work
-    tot_ps = ps
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        w = torch.tensor([float(ps)], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
-        tot_ps = float(w.item())
+    from sfparticles_b200.shard import reduce_job
+    ms, tot_ps = reduce_job(ms, ps, device=dev)
     peak, peak_kind = measured_peak_hbm()
     dk = per_kernel[dominant]
     for v in per_kernel.values():

@@ -1,0 +1,70 @@
+"""Running one job on several GPUs, one process per GPU.
+
+Particles never interact and the fields are analytic, so a job splits across
+GPUs with no data exchange during the run:
+- one collision's beam is split by particle (``split_counts``);
+- a batch of independent collisions is split by expected work
+  (``assign_instances``).
+
+Each rank then runs its share as an ordinary ``Simulation`` or ``Ensemble``
+with its own Philox key (``rank_seed``). The only collective is the
+reduction of a few scalars after the run (``reduce_job``): the maximum of
+the ranks' device times and the sum of their work. It works with any
+``torch.distributed`` backend: NCCL on GPUs, gloo on CPUs.
+
+This is an extension of the reference, which runs on one device.
+"""
+from __future__ import annotations
+
+from typing import List, Sequence, Tuple
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Philox key of `rank`'s share of a job keyed `base` (64-bit)."""
+    return (int(base) + 0x9E3779B97F4A7C15 * (int(rank) + 1)) & (2 ** 64 - 1)
+
+
+def split_counts(total: int, world: int) -> List[Tuple[int, int]]:
+    """(start, count) of each rank's slice of `total` particles; the first
+    `total % world` ranks take one more."""
+    if world <= 0:
+        raise ValueError("world size must be positive")
+    base, extra = divmod(int(total), int(world))
+    out, start = [], 0
+    for r in range(world):
+        n = base + (1 if r < extra else 0)
+        out.append((start, n))
+        start += n
+    return out
+
+
+def assign_instances(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Instances (by index) for each rank. Longest expected work first, each
+    to the rank with the least work so far; every rank's list stays in
+    instance order."""
+    if world <= 0:
+        raise ValueError("world size must be positive")
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    for lst in out:
+        lst.sort()
+    return out
+
+
+def reduce_job(ms: float, particle_steps: float, device=None) -> Tuple[float, float]:
+    """(max over ranks of `ms`, sum over ranks of `particle_steps`); the
+    values themselves when torch.distributed is not initialised.  Every
+    rank must call it at the same point."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms), float(particle_steps)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    w = torch.tensor([float(particle_steps)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
