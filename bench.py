@@ -376,6 +376,42 @@ def run_c5(args):
     print(json.dumps(line), flush=True)
 
 
+WORKLOAD_OPS = "the reference's step loop over the one-for-one float64 kernels (engine 'ops'): the scaled-cascade " \
+               "beam at the given electron count, from step 0"
+
+
+def run_ops(args):
+    """The plain float64 path on its own: particle-steps/s of the per-op
+    kernels (each launched once per species per step, fields materialised)."""
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    sim = make_sim(args.electrons, 1000, "fp64", engine="ops")
+    for p in sim.all_particles:
+        p._to_gpu()
+    sim._loop_ops(args.warmup, None)
+    torch.cuda.synchronize()
+    ps0 = sim.particle_steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        torch.cuda.nvtx.range_push("ops")  # profilers select these launches by this range
+        e0.record()
+        sim._loop_ops(args.steps, None)
+        e1.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ps = sim.particle_steps - ps0
+    line = {"metric": "particle-steps/s", "value": ps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_OPS, "electrons": args.electrons,
+                       "l2": "80 MB per array at 1e7 electrons, larger than L2 for every kernel"},
+            "roofline": None, "cpu_baseline": None, "e2e": None, "clocks": clk.summary(), "particle_steps": ps}
+    print(json.dumps(line), flush=True)
+
+
 def make_oracle_sim(n, seed):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as orc
@@ -642,10 +678,10 @@ def main():
     ap.add_argument("--steps", type=int, default=STEPS_FULL)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "ops"],
                     help="c2: the scaled cascade (default); c3: the learned photon-energy sampler on 5e7 "
                          "queries per step; c4: 256 batched uneven instances (2000 steps); c5: the spin + "
-                         "radiation-reaction avalanche to 1e9 particles")
+                         "radiation-reaction avalanche to 1e9 particles; ops: the per-op float64 kernels")
     ap.add_argument("--queries", type=int, default=50_000_000, help="c3: queries per step")
     ap.add_argument("--electrons-c5", type=int, default=5_000_000, help="c5: electrons at rest")
     ap.add_argument("--particle-cap", type=int, default=1_000_000_000, help="c5: stop at this many particles")
@@ -678,6 +714,15 @@ def main():
         if args.steps == STEPS_FULL:
             args.steps = 20
         run_c3(args)
+        return
+    if args.workload == "ops":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "ops",
+                              "unavailable": "the per-op mode runs one GPU, product arm only"}))
+            return
+        if args.steps == STEPS_FULL:
+            args.steps = 20
+        run_ops(args)
         return
     if args.workload == "c5":
         if args.impl != "ours" or world != 1:
