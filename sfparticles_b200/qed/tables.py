@@ -22,6 +22,13 @@ in [-3, 2]) and extend it with the same spacing up to log10 chi = 3
 (307 rows), so that chi > 100 is tabulated instead of read past the end.
 Cumulative columns: first entry by quadrature from 0, then the reference's
 left-Riemann accumulation integ[i] = integ[i-1] + P(delta_i)(delta_i - delta_{i-1}).
+
+One deliberate difference: Ai, Ai' and integral Ai are taken as exactly 0
+from z = 108 on (AIRY_ZERO_Z), where their float64 values are 0.  The
+reference evaluates them there with scipy, which returns NaN for z ~ 1e8 and
+above; that leaves its cumulative pair rows for chi_gamma below ~0.43 all NaN
+and its optical-depth pair creation there with a NaN energy fraction.  Every
+finite entry of the reference's tables is unchanged.
 """
 from __future__ import annotations
 
@@ -68,6 +75,23 @@ def int_Ai(z: float) -> float:
     return quad(_Ai, z, np.inf)[0]
 
 
+# Ai(z), Ai'(z) and integral_z^inf Ai are all below half the smallest float64
+# subnormal from z = 108 on (Ai(z) ~ exp(-(2/3) z^1.5) / (2 sqrt(pi) z^0.25),
+# exp(-(2/3) 108^1.5) = 1e-325), so all three are exactly 0.0 in float64
+# there.  scipy's airy returns NaN from z ~ 1e8 on, which the rates reach at
+# delta -> 0 (pair creation for chi_gamma below ~0.43): the reference's
+# generator (optical_depth_tables.py:126-187) keeps those NaNs, and every
+# cumulative pair row below chi_gamma ~ 0.43 comes out NaN.
+AIRY_ZERO_Z = 108.0
+
+
+def _airy_terms(z: float):
+    """(integral_z^inf Ai, Ai'(z)), exactly 0 from AIRY_ZERO_Z on."""
+    if z >= AIRY_ZERO_Z:
+        return 0.0, 0.0
+    return int_Ai(z), _Aip(z)
+
+
 def photon_rate_delta(chi_e: float, delta: float) -> float:
     """dW_gamma/ddelta [1/s] at photon energy fraction delta."""
     if delta == 1.0:
@@ -76,7 +100,8 @@ def photon_rate_delta(chi_e: float, delta: float) -> float:
     chi_gamma = delta * chi_e
     chi_ep = chi_e - chi_gamma
     z = (chi_gamma / chi_e / chi_ep) ** (2 / 3)
-    return factor * (int_Ai(z) + (2.0 / z + chi_gamma * np.sqrt(z)) * _Aip(z))
+    iA, dA = _airy_terms(z)
+    return factor * (iA + (2.0 / z + chi_gamma * np.sqrt(z)) * dA)
 
 
 def pair_rate_delta(chi_gamma: float, delta: float) -> float:
@@ -87,7 +112,8 @@ def pair_rate_delta(chi_gamma: float, delta: float) -> float:
     chi_e = delta * chi_gamma
     chi_ep = chi_gamma - chi_e
     z = (chi_gamma / chi_e / chi_ep) ** (2 / 3)
-    return factor * (int_Ai(z) + (2.0 / z - chi_gamma * np.sqrt(z)) * _Aip(z))
+    iA, dA = _airy_terms(z)
+    return factor * (iA + (2.0 / z - chi_gamma * np.sqrt(z)) * dA)
 
 
 def photon_rate_total(chi_e: float) -> float:

@@ -45,6 +45,37 @@ def test_product_od_table_contains_reference_grid():
     np.testing.assert_array_equal(chi[g["rows"]], g["chi_rows"])
     np.testing.assert_allclose(d["photon_rate_total"][g["rows"]], g["photon_total"], rtol=1e-12)
     np.testing.assert_allclose(d["photon_cumulative"][g["rows"]], g["photon_cum"], rtol=1e-12)
+    np.testing.assert_allclose(d["pair_rate_total"][g["rows"]], g["pair_total"], rtol=1e-12, atol=1e-300)
+    ref = g["pair_cum"]
+    fin = np.isfinite(ref)
+    np.testing.assert_array_equal(d["pair_cumulative"][g["rows"]][fin], ref[fin])
+
+
+def test_pair_table_has_no_nan_rows():
+    """The reference's generator leaves every cumulative pair row below
+    chi_gamma ~ 0.43 NaN (scipy's airy is NaN for z ~ 1e8 and above); the
+    fixture keeps them.  Ours takes the Airy terms as their float64 value 0
+    there: every row finite, non-decreasing, zero exactly where the total
+    rate is zero, and ending at the left-Riemann fraction of the total that
+    the reference's own finite rows end at."""
+    from sfparticles_b200.qed import tables
+    g = golden("ref_od.npz")
+    nan_rows = [k for k in range(len(g["rows"])) if np.isnan(g["pair_cum"][k]).any()]
+    assert nan_rows, "the fixture holds the reference's NaN rows"
+    d = tables.od_tables()
+    pc, tot = d["pair_cumulative"], d["pair_rate_total"]
+    assert np.isfinite(pc).all() and np.isfinite(tot).all()
+    assert (np.diff(pc, axis=1) >= 0).all()
+    np.testing.assert_array_equal(pc.max(axis=1) == 0, tot == 0)
+    # the reference's finite rows nearest below: chi_gamma 0.44 and 0.87
+    ref_frac = np.array([g["pair_cum"][k][-1] / g["pair_total"][k] for k in (nan_rows[-1] + 1, nan_rows[-1] + 2)])
+    fixed = (tot > 0) & (d["chi"] < g["chi_rows"][nan_rows[-1] + 1])
+    assert fixed.sum() > 100
+    frac = pc[fixed, -1] / tot[fixed]
+    assert frac.min() > ref_frac.min() - 1e-3 and frac.max() < ref_frac.max() + 1e-3
+    # the fixed rows, recomputed by the generator, are the shipped ones
+    for k in nan_rows[-2:]:
+        np.testing.assert_array_equal(tables.pair_cumulative(float(g["chi_rows"][k])), pc[g["rows"][k]])
 
 
 def test_oracle_od_sampling_matches_reference_with_same_draws():
