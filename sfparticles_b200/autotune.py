@@ -42,7 +42,7 @@ DEFAULT = {
     ("fp64", "rs"): ((1, 2), (3, 3)),
     ("fp64", "od"): ((1, 2), (3, 3)),
     ("fp32", "rs"): ((2, 3), (3, 4)),
-    ("fp32", "od"): ((1, 3), (3, 4)),
+    ("fp32", "od"): ((2, 2), (3, 3)),
 }
 
 _lock = threading.Lock()

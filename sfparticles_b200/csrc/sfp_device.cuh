@@ -516,17 +516,12 @@ SFP_DEVICE_INLINE double od_bisect(double chi, double r_uniform, const sfp_od_ta
 // up to the energy draw: true on an event, with `u` the uniform that the
 // inverse CDF maps to delta.  chi_min = 10^log_chi_min, computed once by the
 // caller (the reference's module constant _chi_min, optical_depth.py:14).
+// od_tau_step is the part after the total-rate lookup (optical_depth.py:47-62).
 // Draws, taken only when needed as in the reference (counter-based, so
 // identical to drawing always): purpose 1 -> (tau reset, tau after event),
 // purpose 2 -> inverse-CDF u.
-SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
-                                  const double* rate, double chi_min, unsigned long long seed, unsigned int stream,
-                                  unsigned int step, long long slot, double& u) {
-    if (chi < chi_min) {
-        u = 0.0;
-        return false;
-    }
-    const double rtot = od_interp1d(chi, t, rate);
+SFP_DEVICE_INLINE bool od_tau_step(double rtot, double ig, double dt, double& tau, unsigned long long seed,
+                                   unsigned int stream, unsigned int step, long long slot, double& u) {
     const double dtau = dt * ig;
     double ra = 0.0, rb = 0.0;
     bool drawn = false;
@@ -546,6 +541,16 @@ SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau,
     }
     u = 0.0;
     return false;
+}
+
+SFP_DEVICE_INLINE bool od_event_u(double chi, double ig, double dt, double& tau, const sfp_od_table& t,
+                                  const double* rate, double chi_min, unsigned long long seed, unsigned int stream,
+                                  unsigned int step, long long slot, double& u) {
+    if (chi < chi_min) {
+        u = 0.0;
+        return false;
+    }
+    return od_tau_step(od_interp1d(chi, t, rate), ig, dt, tau, seed, stream, step, slot, u);
 }
 
 // the whole update with the table's inverse CDF for delta

@@ -177,4 +177,19 @@ SFP_DEVICE_INLINE float rate_core(float chi_g, float base, const float* __restri
     return iA + (2.0f / z + sgn * chi_g * sqrtf(z)) * dA;
 }
 
+// _linear_interp1d (qed/optical_depth_tables.py:56-66) in float32: the float32
+// form's total-rate lookup (rate: the table staged as float32).  The optical
+// depth it is subtracted from stays float64.
+SFP_DEVICE_INLINE float od_rate(float chi, const sfp_od_table& t, const float* __restrict__ rate) {
+    const float lmin = (float)t.log_chi_min, ldel = (float)t.log_chi_delta, lmax = (float)t.log_chi_max;
+    float lc = log10f(chi);
+    if (lc < lmin) return 0.0f;
+    if (lc > lmax) lc = lmax;
+    int idx = (int)floorf((lc - lmin) / ldel);
+    if (idx > t.chi_N - 2) idx = t.chi_N - 2;
+    if (idx < 0) idx = 0;
+    const float left = lmin + (float)idx * ldel;
+    return rate[idx] + (rate[idx + 1] - rate[idx]) * ((lc - left) / ldel);
+}
+
 }  // namespace sfp32

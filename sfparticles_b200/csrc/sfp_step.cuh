@@ -306,6 +306,8 @@ struct sfp_qed_smem {
     float base_maxf;
     double chi_pair_min;  // below: no pair event is possible (z_min > z_max)
     double od_chi_min_ph, od_chi_min_pa;  // optical depth: 10^log_chi_min of each table
+    const float* od_phf;  // float32 form, optical depth: the total-rate tables as float32
+    const float* od_paf;
 };
 
 template <int FORM, int QED>
@@ -314,6 +316,7 @@ __device__ __forceinline__ sfp_qed_smem sfp_stage_tables(const sfp_run_dev* __re
     T.iAt = T.dAt = s_tab;
     T.iAf = T.dAf = reinterpret_cast<const float*>(s_tab);
     T.od_ph = T.od_pa = s_tab;
+    T.od_phf = T.od_paf = reinterpret_cast<const float*>(s_tab);
     T.zN = 0;
     T.zmax = 0.0;
     if (QED == SFP_QED_REJECTION) {
@@ -335,9 +338,16 @@ __device__ __forceinline__ sfp_qed_smem sfp_stage_tables(const sfp_run_dev* __re
         }
     } else {
         const int n1 = R->od_photon.chi_N, n2 = R->od_pair.chi_N;
-        for (int i = threadIdx.x; i < n1; i += blockDim.x) s_tab[i] = R->od_photon.rate_total[i];
-        for (int i = threadIdx.x; i < n2; i += blockDim.x) s_tab[n1 + i] = R->od_pair.rate_total[i];
-        T.od_pa = s_tab + n1;
+        if (FORM == SFP_FORM_FP64) {
+            for (int i = threadIdx.x; i < n1; i += blockDim.x) s_tab[i] = R->od_photon.rate_total[i];
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) s_tab[n1 + i] = R->od_pair.rate_total[i];
+            T.od_pa = s_tab + n1;
+        } else {
+            float* f = reinterpret_cast<float*>(s_tab);
+            for (int i = threadIdx.x; i < n1; i += blockDim.x) f[i] = (float)R->od_photon.rate_total[i];
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) f[n1 + i] = (float)R->od_pair.rate_total[i];
+            T.od_paf = f + n1;
+        }
     }
     T.inv_dzf = (float)((double)(T.zN - 1) / T.zmax);
     T.base_maxf = (float)(T.zmax * sqrt(T.zmax));
@@ -400,15 +410,20 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 d = (double)dl;
                 if (ev && dl * g < (float)R->photon_threshold) ev = false;
             }
-        } else if (R->mlp_params) {
-            ev = od_event_u((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed,
-                            S.stream, step, i, d);
-            hs = (double)g;
-            lchi = ev ? log10((double)chi) : 0.0;
         } else {
-            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_photon, T.od_ph, T.od_chi_min_ph, I.seed,
-                          S.stream, step, i, d);
-            if (ev && d * (double)g < R->photon_threshold) ev = false;
+            // float32 rate lookup, float64 optical depth
+            double u = 0.0;
+            ev = !((double)chi < T.od_chi_min_ph) &&
+                 od_tau_step((double)sfp32::od_rate(chi, R->od_photon, T.od_phf), 1.0 / (double)g, dt, tau, I.seed,
+                             S.stream, step, i, u);
+            if (R->mlp_params) {
+                d = u;
+                hs = (double)g;
+                lchi = ev ? log10((double)chi) : 0.0;
+            } else {
+                d = ev ? od_bisect((double)chi, u, R->od_photon) : 0.0;
+                if (ev && d * (double)g < R->photon_threshold) ev = false;
+            }
         }
         if (!ev) d = 0.0;
     }
@@ -458,8 +473,12 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                 d = (double)r1;
             }
         } else {
-            ev = od_event((double)chi, 1.0 / (double)g, dt, tau, R->od_pair, T.od_pa, T.od_chi_min_pa, I.seed,
-                          S.stream, step, i, d);
+            // float32 rate lookup, float64 optical depth
+            double u = 0.0;
+            ev = !((double)chi < T.od_chi_min_pa) &&
+                 od_tau_step((double)sfp32::od_rate(chi, R->od_pair, T.od_paf), 1.0 / (double)g, dt, tau, I.seed,
+                             S.stream, step, i, u);
+            d = ev ? od_bisect((double)chi, u, R->od_pair) : 0.0;
         }
         if (!ev) d = 0.0;
     }
