@@ -861,6 +861,15 @@ static int run_upload(sfp_run* r, const sfp_instance* inst, const int64_t* n_buf
 }
 
 // persistent grid of one kernel: resident blocks per SM x SMs
+// the kernel's dynamic shared memory limit, raised to at least `need` bytes
+static cudaError_t raise_dynamic_smem(const void* k, size_t need) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= need) return cudaSuccess;
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
+
 static int persistent_grid(cudaKernel_t k, size_t smem, int fallback_per_sm) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, SFP_TILE_HOST, smem) != cudaSuccess ||
@@ -994,12 +1003,11 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
     const size_t cap = 200 * 1024;
     if (r->smem_m > cap || r->smem_p > cap) return cleanup(fail(SFP_EINVAL, "QED tables too large for shared memory"));
-    if ((r->smem_m > 48 * 1024 && cudaFuncSetAttribute((const void*)r->k_massive,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)r->smem_m) != cudaSuccess) ||
-        (r->smem_p > 48 * 1024 && cudaFuncSetAttribute((const void*)r->k_photon,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)r->smem_p) != cudaSuccess))
+    // always raised, never lowered: the kernels' static shared memory counts
+    // toward the 48 KB a launch gets without it, and runs that share a module
+    // (with and without the learned sampler) need different amounts
+    if (raise_dynamic_smem((const void*)r->k_massive, r->smem_m) != cudaSuccess ||
+        raise_dynamic_smem((const void*)r->k_photon, r->smem_p) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory"));
     r->grid_m = persistent_grid(r->k_massive, r->smem_m, minb);
     r->grid_p = persistent_grid(r->k_photon, r->smem_p, pminb);

@@ -90,12 +90,16 @@ SFP_DEVICE_INLINE uint4 warp_sum_u4(uint4 v) {
 
 // Asynchronous 16-byte global -> shared copies (cp.async, one per thread,
 // L2 only); `src_bytes` < 16 zero-fills the rest and reads only that many.
+// Issue and commit carry no "memory" clobber, so values the compiler holds in
+// registers survive them; the destination's earlier readers are ordered by
+// the caller's __syncwarp() before the issue (volatile asm is not moved across
+// it), and the data is read only after cp_async_wait, which is a clobber.
 SFP_DEVICE_INLINE void cp_async16(void* smem_dst, const void* gsrc, unsigned int src_bytes) {
     const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
     const unsigned long long g = (unsigned long long)__cvta_generic_to_global(gsrc);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(src_bytes) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(src_bytes));
 }
-SFP_DEVICE_INLINE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+SFP_DEVICE_INLINE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 SFP_DEVICE_INLINE void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -838,44 +842,52 @@ struct sfp_photon_ring {
     static constexpr int STAGE_BYTES = NC * 32 * 8 + 32;             // + the 32 pruned flags
 };
 
-SFP_DEVICE_INLINE const double* sfp_ring_src(const sfp_segment& S, int c) {
+// A warp's tile descriptor in shared memory: each array of the tile's
+// segment, offset to the tile's first photon (NULL where the segment has no
+// such array).  Slots 0-5 x..uz, 6 tau, 7 the pruned flags, 8 pair delta.
+constexpr int SFP_DESC_TAU = 6, SFP_DESC_PRUNED = 7, SFP_DESC_DELTA = 8, SFP_DESC_N = 9;
+
+SFP_DEVICE_INLINE char* sfp_desc_slot(const sfp_segment& S, int c, long long base) {
     switch (c) {
-        case 0: return S.x;
-        case 1: return S.y;
-        case 2: return S.z;
-        case 3: return S.ux;
-        case 4: return S.uy;
-        case 5: return S.uz;
-        default: return S.tau;
+        case 0: return reinterpret_cast<char*>(S.x + base);
+        case 1: return reinterpret_cast<char*>(S.y + base);
+        case 2: return reinterpret_cast<char*>(S.z + base);
+        case 3: return reinterpret_cast<char*>(S.ux + base);
+        case 4: return reinterpret_cast<char*>(S.uy + base);
+        case 5: return reinterpret_cast<char*>(S.uz + base);
+        case SFP_DESC_TAU: return S.tau ? reinterpret_cast<char*>(S.tau + base) : nullptr;
+        case SFP_DESC_PRUNED: return reinterpret_cast<char*>(S.pruned + base);
+        default: return S.delta ? reinterpret_cast<char*>(S.delta + base) : nullptr;
     }
 }
 
-// copies of sub-step `sub` (photons base + 32 sub .. + 31) into one stage:
-// component c of photons 2p, 2p+1 -> dst + 256 c + 16 p; flags -> dst + 256 NC.
-// Entries at or past N are zero-filled and not read.  One commit group.
+// copies of sub-step `sub` (tile photons 32 sub .. + 31) into one stage: copy
+// c is component c/16 of photons 2(c%16), +1 (c < 16 NC) or 16 pruned flags,
+// always to dst + 16 c, so components land at dst + 256 comp and the flags at
+// dst + 256 NC.  `left` = photons of the segment from the tile's first on;
+// entries past them are zero-filled and not read.  One commit group.
 template <int QED>
-__device__ __forceinline__ void sfp_ring_issue(const sfp_segment& S, long long base, int sub, long long N,
-                                               unsigned char* dst, int lane) {
+__device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long long left, unsigned char* dst,
+                                               int lane) {
     constexpr int NC = sfp_photon_ring<QED>::NC;
     constexpr int NCOPY = NC * 16 + 2;
-    const long long i0 = base + (long long)sub * 32;
+    const bool full = left >= (long long)(sub + 1) * 32;  // warp-uniform: no copy is short
 #pragma unroll
     for (int k = 0; k < (NCOPY + 31) / 32; ++k) {
         const int c = lane + 32 * k;
         if (c < NC * 16) {
-            const int comp = c >> 4, pair = c & 15;
-            const long long j = i0 + 2 * pair;
-            const long long left = N - j;
-            const double* src = sfp_ring_src(S, comp);
-            unsigned int nb = left >= 2 ? 16u : (left == 1 ? 8u : 0u);
+            const int e = sub * 32 + 2 * (c & 15);
+            const char* src = D[c >> 4];
+            unsigned int nb = 16u;
+            if (!full) nb = left - e >= 2 ? 16u : (left - e == 1 ? 8u : 0u);
             if (!src) nb = 0u;  // no optical depth array on this segment
-            sfp::cp_async16(dst + comp * 256 + pair * 16, nb ? (const void*)(src + j) : (const void*)S.x, nb);
+            sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + (size_t)e * 8) : (const void*)D[0], nb);
         } else if (c < NCOPY) {
-            const int h = c - NC * 16;
-            const long long j = i0 + 16 * h;
-            const long long left = N - j;
-            const unsigned int nb = left >= 16 ? 16u : (left > 0 ? (unsigned int)left : 0u);
-            sfp::cp_async16(dst + NC * 256 + h * 16, nb ? (const void*)(S.pruned + j) : (const void*)S.pruned, nb);
+            const int e = sub * 32 + 16 * (c - NC * 16);
+            const char* src = D[SFP_DESC_PRUNED];
+            unsigned int nb = 16u;
+            if (!full) nb = left - e >= 16 ? 16u : (left - e > 0 ? (unsigned int)(left - e) : 0u);
+            sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + e) : (const void*)src, nb);
         }
     }
     sfp::cp_async_commit();
@@ -898,6 +910,8 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
+    __shared__ char* s_desc[SFP_TILE / 32][SFP_DESC_N];
+    char* const* D = s_desc[warp];
 
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&st->pticket, 1);
@@ -916,40 +930,47 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             tile = __shfl_sync(0xffffffffu, tk, 0);
             continue;
         }
+        const long long left = N - base;
+        const bool bw = S.bw != 0, push = S.push != 0;
+        __syncwarp();  // the previous tile's lanes are done with its descriptor and stages
+        if (lane < SFP_DESC_N) s_desc[warp][lane] = sfp_desc_slot(S, lane, base);
+        __syncwarp();
         unsigned int cnt = 0;
 #pragma unroll
-        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<QED>(S, base, k, N, ring + k * SB, lane);
+        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<QED>(D, k, left, ring + k * SB, lane);
 #pragma unroll 1
         for (int sub = 0; sub < SFP_PHOTON_WSUB; ++sub) {
             __syncwarp();  // every lane has read the stage about to be refilled
             const int nsub = sub + STAGES - 1;
-            if (nsub < SFP_PHOTON_WSUB) sfp_ring_issue<QED>(S, base, nsub, N, ring + (nsub % STAGES) * SB, lane);
+            if (nsub < SFP_PHOTON_WSUB) sfp_ring_issue<QED>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
             else cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncwarp();  // the stage of `sub` is complete for the whole warp
             const unsigned char* stg = ring + (sub % STAGES) * SB;
             const double* sd = reinterpret_cast<const double*>(stg);
-            const long long i = base + (long long)sub * 32 + lane;
-            const bool alive = (i < N) && stg[NC * 256 + lane] == 0;
+            const int e = sub * 32 + lane;  // photon index from the tile's first
+            const long long i = base + e;
+            const bool alive = e < left && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
             double tau = QED == SFP_QED_OPTICAL_DEPTH ? sd[192 + lane] : 0.0;
             bool ev = false;
             double delta = 0.0;
-            if (alive && S.bw)
+            if (alive && bw)
                 ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
             if (ev) {
                 // converted photons are pruned, not pushed (cpu.py:190); 2 marks this step's events
-                S.pruned[i] = 2;
-                S.delta[i] = delta;
-            } else if (alive && S.push) {
+                reinterpret_cast<unsigned char*>(D[SFP_DESC_PRUNED])[e] = 2;
+                reinterpret_cast<double*>(D[SFP_DESC_DELTA])[e] = delta;
+            } else if (alive && push) {
                 if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
                 else push_photon32(x, y, z, ux, uy, uz, dt);
-                S.x[i] = x;
-                S.y[i] = y;
-                S.z[i] = z;
+                reinterpret_cast<double*>(D[0])[e] = x;
+                reinterpret_cast<double*>(D[1])[e] = y;
+                reinterpret_cast<double*>(D[2])[e] = z;
             }
-            if (QED == SFP_QED_OPTICAL_DEPTH && alive && S.bw && S.tau) S.tau[i] = tau;
+            if (QED == SFP_QED_OPTICAL_DEPTH && alive && bw && D[SFP_DESC_TAU])
+                reinterpret_cast<double*>(D[SFP_DESC_TAU])[e] = tau;
             cnt += __popc(__ballot_sync(0xffffffffu, ev));
         }
         if (lane == 0) {
