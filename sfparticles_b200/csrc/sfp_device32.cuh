@@ -49,7 +49,11 @@ SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, u
 
 // ---- field presets (same parameter blocks as the float64 forms) ----------
 // gaussian_laser_pulse (fields.py:152-168); the curvature term k0 r^2 / (2 Rx)
-// is written as k0 r^2 x / (2 (x^2 + zR^2)), finite at x = 0.
+// is written as k0 r^2 x / (2 (x^2 + zR^2)) = (k0 / (2 zR^2)) r^2 x / q with
+// q = 1 + (x/zR)^2, finite at x = 0, and r^2 / w(x)^2 as (1/w0^2) r^2 / q.
+// Slots 10-15 of the block hold float32 constants in pairs (fields.py,
+// _pack_float32): E0, k0, 1/zR, k0/(2 zR^2), 1/w0^2, 1/kc^2, direction/c,
+// cep, cos(pol), sin(pol), k0/(4 zR), kc = k0 ctau.  1/q is rsqrt(q)^2.
 // |phi| / kc beyond which a Gaussian envelope exp(-(phi/kc)^2) is exactly 0
 // in float32, denormals included: sqrt(110), with exp(-104) already below
 // half the smallest denormal
@@ -57,34 +61,34 @@ constexpr float kFieldCut32 = 10.5f;
 
 SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
                                       float F[6]) {
-    const float E0 = (float)P[0], k0 = (float)P[1], zR = (float)P[2], w0 = (float)P[3], ctau = (float)P[4];
+    const float* __restrict__ G = reinterpret_cast<const float*>(P + 10);
+    const float E0 = G[0], k0 = G[1], inv_zR = G[2], cq = G[3], inv_w02 = G[4], inv_kc2 = G[5], dirc = G[6];
+    const float cep = G[7], cp = G[8], sp = G[9], cut_r = G[10], kc = G[11];
     const double dir = P[5], x0 = P[6];
-    const float cep = (float)P[7], cp = (float)P[8], sp = (float)P[9];
     const float xf = (float)x, yf = (float)y, zf = (float)z;
     const float xr = (float)((x - x0) - (dir * sfp::kC) * t);
     const float r2 = yf * yf + zf * zf;
-    // |phi| >= |k0 xr| - k0 r2 / (4 zR) - pi/2 (as in the float64 form):
+    // |phi| >= k0 |xr| - k0 r2 / (4 zR) - pi/2 (as in the float64 form):
     // beyond kFieldCut32 kc the envelope is exactly 0, and so is the field
-    if (4.0f * zR * fabsf(k0 * xr) - k0 * r2 - 6.2832f * zR > 4.0f * zR * kFieldCut32 * (k0 * ctau)) {
+    if (k0 * fabsf(xr) - cut_r * r2 - 1.5708f > kFieldCut32 * kc) {
         for (int k = 0; k < 6; ++k) F[k] = 0.0f;
         return;
     }
-    const float xz = xf / zR;
+    const float xz = xf * inv_zR;
     const float q = 1.0f + xz * xz;
-    const float wx2 = (w0 * w0) * q;
+    const float rs = rsqrtf(q);
+    const float rq = rs * rs;
     const float gouy = atanf(xz);
-    const float phi = k0 * xr + (k0 * r2 * xf) / (2.0f * (xf * xf + zR * zR)) - gouy;
-    const float kc = k0 * ctau;
-    const float env = __expf(-(r2 / wx2 + (phi * phi) / (kc * kc)));
-    const float E = E0 * cos_r(phi + cep) * rsqrtf(q) * env;
+    const float phi = k0 * xr + (cq * r2) * (xf * rq) - gouy;
+    const float env = __expf(-((r2 * inv_w02) * rq + (phi * phi) * inv_kc2));
+    const float E = E0 * cos_r(phi + cep) * rs * env;
     const float Ey = E * cp, Ez = E * sp;
-    const float d = (float)dir;
     F[0] = 0.0f;
     F[1] = Ey;
     F[2] = Ez;
     F[3] = 0.0f;
-    F[4] = -Ez * (d / kCf);
-    F[5] = Ey * (d / kCf);
+    F[4] = -Ez * dirc;
+    F[5] = Ey * dirc;
 }
 
 // simple_laser_pulse (fields.py:102-116)

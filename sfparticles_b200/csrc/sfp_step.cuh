@@ -464,25 +464,31 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
     } else {
         float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (S.push) sfp_field_program32(x, y, z, t, P, F);
-        const float g = sfp32::gamma_of(ux, uy, uz, true);
-        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
-        if (QED == SFP_QED_REJECTION) {
-            if (chi > 0.0f && !((double)chi < T.chi_pair_min)) {
-                float r1, r2;
-                sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
-                const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
-                const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
-                const float W = kRate * sfp32::rate_core(chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, -1.0f);
-                ev = r2 < W * ((float)dt / g);
-                d = (double)r1;
+        // in a zero field (outside every pulse: the far-field cut) chi is
+        // exactly 0, so neither method can create a pair or change tau
+        const bool field = F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f || F[5] != 0.f;
+        if (field) {
+            const float g = sfp32::gamma_of(ux, uy, uz, true);
+            const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+            if (QED == SFP_QED_REJECTION) {
+                if (chi > 0.0f && !((double)chi < T.chi_pair_min)) {
+                    float r1, r2;
+                    sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+                    const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
+                    const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
+                    const float W =
+                        kRate * sfp32::rate_core(chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, -1.0f);
+                    ev = r2 < W * ((float)dt / g);
+                    d = (double)r1;
+                }
+            } else {
+                // float32 rate lookup, float64 optical depth
+                double u = 0.0;
+                ev = !((double)chi < T.od_chi_min_pa) &&
+                     od_tau_step((double)sfp32::od_rate(chi, R->od_pair, T.od_paf), 1.0 / (double)g, dt, tau, I.seed,
+                                 S.stream, step, i, u);
+                d = ev ? od_bisect((double)chi, u, R->od_pair) : 0.0;
             }
-        } else {
-            // float32 rate lookup, float64 optical depth
-            double u = 0.0;
-            ev = !((double)chi < T.od_chi_min_pa) &&
-                 od_tau_step((double)sfp32::od_rate(chi, R->od_pair, T.od_paf), 1.0 / (double)g, dt, tau, I.seed,
-                             S.stream, step, i, u);
-            d = ev ? od_bisect((double)chi, u, R->od_pair) : 0.0;
         }
         if (!ev) d = 0.0;
     }

@@ -159,6 +159,15 @@ def _preset(kind: str, params: List[float]) -> Fields:
     return Fields(_tree=_Term(kind, params))
 
 
+def _pack_float32(values: List[float]) -> List[float]:
+    """float64 parameter slots holding float32 values in pairs (little
+    endian: value 2j in the low half of slot j).  Finite float32 values never
+    pack into a NaN or infinity."""
+    import struct
+    v = list(values) + [0.0] * (len(values) % 2)
+    return [struct.unpack("<d", struct.pack("<ff", v[j], v[j + 1]))[0] for j in range(0, len(v), 2)]
+
+
 def _check_direction(direction):
     assert direction == 1 or direction == -1, "direction must be +1 (+x) or -1 (-x)"
 
@@ -192,7 +201,13 @@ def gaussian_laser_pulse(a0, w0, ctau, direction=1, x0=0.0, l0=0.8e-6, pol_angle
     zR = PI * w0 ** 2 / l0
     a0_norm = E_CHARGE / (M_E * C * omega0)
     E0 = a0 / a0_norm
-    f = _preset(KIND_GAUSSIAN, [E0, k0, zR, w0, ctau, direction, x0, cep, math.cos(pol_angle), math.sin(pol_angle)])
+    cp, sp = math.cos(pol_angle), math.sin(pol_angle)
+    kc = k0 * ctau
+    # slots 10-15: the float32 form's constants, two float32 per slot, so that
+    # its per-particle evaluation converts and divides nothing
+    f32 = [E0, k0, 1.0 / zR, k0 / (2.0 * zR * zR), 1.0 / (w0 * w0), 1.0 / (kc * kc), direction / C, cep, cp, sp,
+           k0 / (4.0 * zR), kc]
+    f = _preset(KIND_GAUSSIAN, [E0, k0, zR, w0, ctau, direction, x0, cep, cp, sp] + _pack_float32(f32))
     f.field_func_input = ("gaussian_laser_pulse", dict(a0=a0, w0=w0, ctau=ctau, direction=direction, x0=x0, l0=l0,
                                                        pol_angle=pol_angle, cep=cep))
     return f
