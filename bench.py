@@ -48,7 +48,7 @@ BYTES_PTILE = 4     # photon-tile event counter read by the pairs kernel (one pe
 # DRAM bytes (read + write, ncu) / algorithmic bytes of one launch, from an ncu capture of the same
 # cascade at 1e6 electrons at its final state (2.8 GB of photon state, larger than L2, so traffic
 # scales with the units processed).  Only kernels whose state exceeds L2 in that capture are listed.
-NCU_TRAFFIC_RATIO = {"photon": 2.801e9 / 2.806e9}
+NCU_TRAFFIC_RATIO = {"photon": 2.768e9 / 2.806e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
