@@ -16,10 +16,13 @@ reference's Python orchestration on top of it:
   ``:433-473``, ``_push_momentum`` ``:244-281`` / ``:575-604``, ``_prune``);
 * the step loop: ``simulation.py:102-144``.
 
-Conventions where the reference is undefined (documented in DESIGN.md):
-appended slots start with zero spin and zero optical depth (the reference
-copies stale values cyclically via ``numpy.resize``); random draws come from
-the keyed Philox stream shared with the GPU instead of Numba's MT19937.
+Conventions where the reference is undefined: appended slots start with zero
+spin and zero optical depth (the reference copies stale values cyclically via
+``numpy.resize``); random draws come from the keyed Philox stream shared with
+the GPU instead of Numba's MT19937.  Optical-depth tables are passed in
+(``make_od_table``); the tests pass the ones sfparticles_b200.qed.tables
+ships, whose pair rows below chi_gamma ~ 0.43 are finite where the
+reference's generator leaves them NaN.
 """
 from __future__ import annotations
 

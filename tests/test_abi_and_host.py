@@ -158,3 +158,22 @@ def test_use_gpu_zero_is_refused(monkeypatch):
     r = subprocess.run([sys.executable, "-c", "import sfparticles_b200"], env={**os.environ, "SFPARTICLES_USE_GPU": "0"},
                        capture_output=True, text=True, cwd=REPO)
     assert r.returncode != 0 and "GPU implementation" in r.stderr
+
+
+def test_gaussian_float32_block():
+    """gaussian_laser_pulse: slots 0-9 are the float64 parameters; slots 10-15
+    pack the float32 form's derived constants two per slot, each the float64
+    value rounded once to float32, and none packs into a NaN or infinity."""
+    import math
+    from sfparticles_b200.constants import C, PI
+    a0, w0, ctau, d, x0, l0, pol, cep = 150.0, 4e-6, 7e-6, -1, 3e-5, 0.8e-6, 0.7, 0.25
+    p = fields.gaussian_laser_pulse(a0, w0, ctau, direction=d, x0=x0, l0=l0, pol_angle=pol, cep=cep).params()
+    assert p.size == _lib.SFP_FIELD_PARAMS and np.isfinite(p).all()
+    k0, zR = 2 * PI / l0, PI * w0 ** 2 / l0
+    E0 = a0 / (e / (m_e * C * (2 * PI * C / l0)))
+    np.testing.assert_array_equal(p[:10], [E0, k0, zR, w0, ctau, d, x0, cep, math.cos(pol), math.sin(pol)])
+    kc = k0 * ctau
+    want = np.array([E0, k0, 1 / zR, k0 / (2 * zR * zR), 1 / (w0 * w0), 1 / (kc * kc), d / C, cep, math.cos(pol),
+                     math.sin(pol), k0 / (4 * zR), kc], dtype=np.float32)
+    got = np.frombuffer(np.ascontiguousarray(p[10:16]).tobytes(), dtype="<f4")
+    np.testing.assert_array_equal(got, want)

@@ -175,3 +175,21 @@ def test_oracle_c1_cascade_statistics_match_reference():
     # spectrum-level agreement: relative L1 of the mean spectra
     l1 = np.abs(rh.mean(0) - oh.mean(0)).sum() / rh.mean(0).sum()
     assert l1 < 0.03, l1
+
+
+def test_pair_delta_finite_where_the_reference_table_is_nan():
+    """Pair energy fractions drawn by the oracle's inverse CDF (the
+    reference's _bisect_interp) from the shipped pair table are finite and in
+    (0, 1] for chi_gamma between the first non-zero row and 0.43, where the
+    reference's own table rows are NaN."""
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    tab = orc.make_od_table(d["pair_rate_total"], d["pair_cumulative"], float(d["log_chi_min"]),
+                            float(d["log_chi_delta"]), float(d["log_delta_min"]), float(d["log_delta_delta"]))
+    L = orc.lib()
+    chi0 = float(d["chi"][np.nonzero(d["pair_rate_total"] > 0)[0][0]])
+    rng = np.random.default_rng(7)
+    chis = 10.0 ** rng.uniform(np.log10(chi0), np.log10(0.43), 400)
+    us = rng.uniform(0.0, 1.0, 400)
+    dl = np.array([L.orc_od_bisect(c, u, ctypes.byref(tab)) for c, u in zip(chis, us)])
+    assert np.isfinite(dl).all() and (dl > 0).all() and (dl <= 1.0).all()
