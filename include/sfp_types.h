@@ -36,11 +36,16 @@ typedef uint8_t sfp_u8;
 
 /* arithmetic forms of the fused step */
 #define SFP_FORM_FP64 0  /* plain float64, the reference's arithmetic        */
-#define SFP_FORM_FP32 1  /* float32 push, float64 gamma/|u| when gamma>1e4,
-                            Kahan position, float64 optical depth            */
+#define SFP_FORM_FP32 1  /* float32 arithmetic on float64 state: float32
+                            increments accumulated in float64, float64
+                            gamma when gamma>1e4, float64 optical depth      */
 
 #define SFP_MAX_CHANNELS 4  /* distinct append destinations per instance */
-#define SFP_FIELD_PARAMS 16 /* doubles per preset term                   */
+#define SFP_FIELD_PARAMS 16 /* doubles per preset term; each preset's layout
+                               is written by sfparticles_b200/fields.py (the
+                               Gaussian pulse: slots 0-9 its float64
+                               parameters, 10-15 float32 constants for the
+                               float32 form, two per slot)                    */
 
 /* One particle species of one collision instance: the reference's Particles
  * attribute arrays (particles.py:87-146) as device pointers. */
