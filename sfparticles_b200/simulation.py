@@ -145,6 +145,7 @@ class Simulation(object):
         self.particle_steps = 0  # sum over executed steps of all species' N_buffered
         self.kernel_launches = 0  # libsfp kernels launched by start()/run_on_device()
         self._run = None
+        self._trajectories = []
 
         for p in all_particles:
             if p.bw:
@@ -169,6 +170,21 @@ class Simulation(object):
             self.items, self.min_blocks = dm
         if self.p_stages <= 0 or self.p_min_blocks <= 0:
             self.p_stages, self.p_min_blocks = dp
+
+    def record(self, species: Particles, index, every: int = 1, attrs=None):
+        """Record `attrs` of the buffer slots `index` of `species` after every
+        `every`-th step, on the device (sfparticles_b200.trajectory); returns
+        the Trajectory, whose numpy() gives the records."""
+        from .trajectory import Trajectory
+        assert species in self.all_particles, f"{species.name} not included in simulation."
+        tr = Trajectory(species, index, every, attrs)
+        self._trajectories.append(tr)
+        return tr
+
+    def _record(self):
+        for tr in self._trajectories:
+            if tr.due(self.step):
+                tr.capture(self.step)
 
     # ------------------------------------------------------------------
     def _index(self, p):
@@ -320,6 +336,7 @@ class Simulation(object):
                 call_back(self.step)
             self.t += dt
             self.step += 1
+            self._record()
             if self.print_every and self.step % self.print_every == 0 and self.progress_bar is not None:
                 self.progress_bar.update(self.print_every)
 
@@ -443,6 +460,8 @@ class Simulation(object):
                 chunk = 1
             if self.print_every:
                 chunk = min(chunk, self.print_every - (self.step % self.print_every))
+            for tr in self._trajectories:
+                chunk = min(chunk, tr.steps_to_next(self.step))
             if self._ensure_headroom() or grew:
                 self._update_run(run)
             before = [p.N_buffered for p in self.all_particles]
@@ -461,6 +480,8 @@ class Simulation(object):
                     self._update_run(run)
                     _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
+            if done:
+                self._record()
             observe_rates(self.all_particles, before, done, rates)
             if done == 0 and not halted:
                 raise _lib.SFPError("the step made no progress")
