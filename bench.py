@@ -587,7 +587,11 @@ def run_ours(args, rank, world):
         wall = time.perf_counter() - t0
         ms2 = e0.elapsed_time(e1)
         d2h = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
-        e2e = dict(value=sim2.particle_steps / (max(ms2, wall * 1e3) * 1e-3), unit="particle-steps/s",
+        # whole job: the slowest rank's time, every rank's work and copies
+        from sfparticles_b200.shard import reduce_job, sum_over_ranks
+        ms2, ps2 = reduce_job(max(ms2, wall * 1e3), sim2.particle_steps, device=dev)
+        h2d, d2h = sum_over_ranks([h2d, d2h], device=dev)
+        e2e = dict(value=ps2 / (ms2 * 1e-3), unit="particle-steps/s",
                    h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
                    wall_s=wall)
         del sim2

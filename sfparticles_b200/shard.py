@@ -9,7 +9,8 @@ GPUs with no data exchange during the run:
 Each rank then runs its share as an ordinary ``Simulation`` or ``Ensemble``
 with its own Philox key (``rank_seed``). The only collective is the
 reduction of a few scalars after the run (``reduce_job``): the maximum of
-the ranks' device times and the sum of their work. It works with any
+the ranks' device times and the sum of their work (``sum_over_ranks`` for
+other totals, such as bytes copied). It works with any
 ``torch.distributed`` backend: NCCL on GPUs, gloo on CPUs.
 
 This is an extension of the reference, which runs on one device.
@@ -53,6 +54,19 @@ def assign_instances(costs: Sequence[float], world: int) -> List[List[int]]:
     for lst in out:
         lst.sort()
     return out
+
+
+def sum_over_ranks(values: Sequence[float], device=None) -> List[float]:
+    """Each of `values` summed over the ranks (one all-reduce); the values
+    themselves when torch.distributed is not initialised.  Every rank must
+    call it at the same point with the same number of values."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
 
 
 def reduce_job(ms: float, particle_steps: float, device=None) -> Tuple[float, float]:

@@ -63,7 +63,8 @@ def _rank(rank, world, port, out):
         sim.run(20)
         ms = 10.0 + rank  # stands in for a device time
         got = shard.reduce_job(ms, sim.particle_steps)
-        out[rank] = (got, sim.particle_steps, pho.N_buffered)
+        sums = shard.sum_over_ranks([rank + 1, 0.5 * pho.N_buffered])
+        out[rank] = (got, sim.particle_steps, pho.N_buffered, sums)
     finally:
         dist.destroy_process_group()
 
@@ -85,11 +86,14 @@ def test_two_gloo_ranks_reduce_time_and_work():
             assert p.exitcode == 0, p.exitcode
         res = dict(out)
     total = sum(res[r][1] for r in range(world))
+    photons = sum(res[r][2] for r in range(world))
     for r in range(world):
-        (ms, ps), _, _ = res[r]
+        (ms, ps), _, _, sums = res[r]
         assert ms == 11.0 and ps == total
+        assert sums == [3.0, 0.5 * photons]
     assert res[0][1] > 0 and res[1][1] > 0
 
 
 def test_reduce_job_without_a_process_group_is_the_identity():
     assert shard.reduce_job(3.5, 42) == (3.5, 42.0)
+    assert shard.sum_over_ranks([1, 2.5]) == [1.0, 2.5]
