@@ -1,0 +1,74 @@
+"""Buffer-growth planning of the device loop, on host species: the
+reference's growth rule (particles.py:487-500) applied ahead of a chunk of
+device steps from the observed append rates (simulation.plan_chunk,
+observe_rates) and the one-step worst case for photon destinations
+(Simulation._ensure_headroom)."""
+import numpy as np
+
+import sfparticles_b200 as S
+from sfparticles_b200.fields import static_field
+from sfparticles_b200.simulation import observe_rates, plan_chunk
+
+
+def _species(n, name="pho"):
+    m = 0 if name == "pho" else 1
+    props = tuple(np.ones(n) for _ in range(6)) if m else tuple(np.ones(n) * (k + 1) for k in range(6))
+    return S.Particles(name, 0 if m == 0 else -1, m, N=n, props=props)
+
+
+def test_no_rate_no_growth_full_chunk():
+    p = _species(100)
+    assert plan_chunk([p], {}, 256) == (False, 256)
+    assert p.buffer_size == 100
+
+
+def test_growth_by_the_reference_rule_capped_at_half_the_count():
+    p = _species(1000)
+    rates = {id(p): 10.0}
+    grew, chunk = plan_chunk([p], rates, 256)
+    # want 1.25 * 10 * 256 + 1 = 3201, capped at 1000 // 2 + 1024 = 1524: the reference rule
+    # grows by N_buffered // 4 + N_new = 250 + 1524
+    assert grew and p.buffer_size == 1000 + 250 + 1524
+    assert chunk == int(1774 / 12.5)
+    assert np.all(p._arr["_to_be_pruned"][1000:]) and np.all(p._arr["x"][1000:] == 0)
+    assert np.array_equal(p._arr["ux"][:1000], np.full(1000, 4.0))
+
+
+def test_enough_room_keeps_the_buffers_and_bounds_the_chunk():
+    p = _species(100)
+    p._extend(5000)  # free room
+    size = p.buffer_size
+    grew, chunk = plan_chunk([p], {id(p): 4.0}, 256)
+    assert not grew and p.buffer_size == size
+    assert chunk == min(256, int((size - 100) / 5.0))
+
+
+def test_a_capped_growth_shortens_the_chunk():
+    """b's growth is capped at N // 2 + 1024, below a chunk's worth at its
+    rate, so b sets the chunk; a has room for a full one."""
+    a, b = _species(100), _species(100)
+    a._extend(100_000)
+    grew, chunk = plan_chunk([a, b], {id(a): 1.0, id(b): 10.0}, 1000)
+    assert grew and b.buffer_size == 100 + 25 + (100 // 2 + 1024)
+    assert chunk == int((b.buffer_size - 100) / 12.5) < 1000
+
+
+def test_observed_rates_decay_by_half_at_most():
+    p = _species(10)
+    rates = {}
+    observe_rates([p], [0], 5, rates)
+    assert rates[id(p)] == 2.0
+    observe_rates([p], [10], 5, rates)  # no appends: the rate halves
+    assert rates[id(p)] == 1.0
+    observe_rates([p], [10], 0, rates)  # no steps: unchanged
+    assert rates[id(p)] == 1.0
+
+
+def test_photon_destinations_hold_one_step_of_worst_case_emission():
+    ele = _species(300, "ele")
+    pho = S.Particles("pho", 0, 0)
+    ele.set_photon(pho)
+    sim = S.Simulation(ele, pho, dt=1e-17, fields=static_field(), print_every=None)
+    assert sim._ensure_headroom()
+    assert pho.buffer_size - pho.N_buffered >= ele.N_buffered
+    assert not sim._ensure_headroom()
