@@ -32,7 +32,6 @@ finite entry of the reference's tables is unchanged.
 """
 from __future__ import annotations
 
-import math
 import os
 import time
 

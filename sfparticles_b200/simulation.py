@@ -46,11 +46,10 @@ import os
 from time import perf_counter_ns
 from typing import Callable
 
-import numpy as np
 
 from . import _lib, program, qed
 from .fields import Fields
-from .particles import Particles, RadiationReactionType, _RR_CODE, _device, _random_seed, _stream_ptr
+from .particles import Particles, _RR_CODE, _device, _random_seed, _stream_ptr
 
 try:
     from tqdm.autonotebook import tqdm

@@ -37,7 +37,6 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_reports_errors_without_a_device():
-    import ctypes
     L = _lib.load()
     rc = L.sfp_bool_sum(None, 10, None, None)
     assert rc != 0 and b"NULL" in L.sfp_last_error()

@@ -9,7 +9,6 @@ event decisions are compared exactly.
 """
 import ctypes
 import json
-import math
 import os
 
 import numpy as np

@@ -163,7 +163,6 @@ def test_pair_number(S):
 # ---- tests/test_pusher.py ---------------------------------------------------
 
 def test_boris_gyration_conserves_momentum(S):
-    import ctypes
     from sfparticles_b200 import _lib
     from sfparticles_b200.constants import C, E_CHARGE, M_E, PI
     r = 1e-6

@@ -4,7 +4,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 
 from sfparticles_b200 import shard
 
