@@ -20,7 +20,8 @@ What is recorded, and from which reference code:
                       so orchestration order, appends, recoil and child pushes
                       are the reference's own
 * ref_od.npz       -- optical-depth table rows from the reference generators and
-                      the inverse-CDF / rate interpolation (py_func) on them
+                      the inverse-CDF / rate interpolation (py_func) on them, for
+                      the photon rows and the finite pair rows
 * ref_stats.json   -- un-injected reference runs (Numba's own RNG) for
                       statistical comparison
 
@@ -434,10 +435,24 @@ def gen_od():
             bis.append(odt._bisect_interp.py_func(c, ph_cum))
         finally:
             g["np"] = saved
+    # the same pieces on the pair rows, at chi whose two bracketing rows are
+    # finite (the reference's rows below chi_gamma ~ 0.43 are NaN)
+    first = int(np.nonzero(np.isfinite(pa_cum).all(axis=1))[0][0])
+    chis_p = 10 ** rng.uniform(lo + sub_delta * first, lo + sub_delta * (sub_N - 1) - 1e-9, 1000)
+    rs_p = rng.random(1000)
+    interp_p = np.array([odt._linear_interp1d.py_func(c, pa_tot) for c in chis_p])
+    bis_p = []
+    for c, r in zip(chis_p, rs_p):
+        g["np"] = _NP([r])
+        try:
+            bis_p.append(odt._bisect_interp.py_func(c, pa_cum))
+        finally:
+            g["np"] = saved
     np.savez(out("ref_od.npz"), chi_rows=chi_all[rows], rows=rows, photon_total=ph_tot, pair_total=pa_tot,
              photon_cum=ph_cum, pair_cum=pa_cum, sub_log_chi_min=lo, sub_log_chi_delta=sub_delta,
              log_delta_min=float(ldm), log_delta_delta=(0 - ldm) / (delta_N - 1),
-             q_chi=chis, q_r=rs_, q_interp=interp, q_bisect=np.array(bis))
+             q_chi=chis, q_r=rs_, q_interp=interp, q_bisect=np.array(bis),
+             q_chi_pair=chis_p, q_r_pair=rs_p, q_interp_pair=interp_p, q_bisect_pair=np.array(bis_p))
 
 
 # ---------------------------------------------------------------------------

@@ -89,6 +89,21 @@ def test_oracle_od_sampling_matches_reference_with_same_draws():
     np.testing.assert_allclose(bis, g["q_bisect"], rtol=1e-13)
 
 
+def test_oracle_pair_od_sampling_matches_reference_with_same_draws():
+    """The same pinning on the pair rows: the reference's _linear_interp1d and
+    _bisect_interp on its own pair table, at chi_gamma whose bracketing rows
+    are finite (0.45 to 100), against the oracle's with the same draws."""
+    g = golden("ref_od.npz")
+    tab = orc.make_od_table(g["pair_total"], g["pair_cum"], float(g["sub_log_chi_min"]),
+                            float(g["sub_log_chi_delta"]), float(g["log_delta_min"]), float(g["log_delta_delta"]))
+    L = orc.lib()
+    interp = np.array([L.orc_od_interp1d(c, ctypes.byref(tab)) for c in g["q_chi_pair"]])
+    np.testing.assert_allclose(interp, g["q_interp_pair"], rtol=1e-14)
+    bis = np.array([L.orc_od_bisect(c, r, ctypes.byref(tab)) for c, r in zip(g["q_chi_pair"], g["q_r_pair"])])
+    np.testing.assert_allclose(bis, g["q_bisect_pair"], rtol=1e-13)
+    assert np.isfinite(bis).all()
+
+
 def _stats():
     with open(os.path.join(GOLDEN, "ref_stats.json")) as f:
         return json.load(f)
