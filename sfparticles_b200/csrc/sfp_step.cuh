@@ -837,7 +837,9 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 // ticket and streams them 32 at a time through a ring of STAGES shared-
 // memory stages filled with cp.async, so the state of the next sub-steps is
 // in flight while the current one computes; after the QED tables are staged
-// no block barrier is taken.  Per photon: the pair event at t; a converted
+// no block barrier is taken.  The copies and the stores address the tile
+// through a per-warp descriptor of its arrays in shared memory, written once
+// per tile (sfp_desc_slot).  Per photon: the pair event at t; a converted
 // photon is marked (pruned = 2, not pushed) and its delta stored for the
 // pairs kernel; every other alive photon is pushed.  The warp's event count
 // goes to its tile's counter and is added to its super-tile's.
