@@ -242,6 +242,17 @@ class _QueueRandom:
         return v
 
 
+class _NP:
+    """Stands in for the `np` module inside the reference's _bisect_interp:
+    np.random.rand() serves the given draws, everything else is numpy."""
+
+    def __init__(self, r):
+        self.random = _QueueRandom(r)
+
+    def __getattr__(self, k):
+        return getattr(np, k)
+
+
 def run_rs_injected(photon, inv_gamma, chi, dt, N, pruned, event, delta, seed, stream, step):
     """Call the reference sampler body with the oracle's keyed Philox draws."""
     from sfparticles.qed import rejection_sampling as rs
@@ -419,13 +430,6 @@ def gen_od():
     chis = 10 ** rng.uniform(lo, lo + sub_delta * (sub_N - 1) - 1e-9, 2000)
     rs_ = rng.random(2000)
 
-    class _NP:
-        def __init__(self, r):
-            self.random = _QueueRandom(r)
-
-        def __getattr__(self, k):
-            return getattr(np, k)
-
     interp = np.array([odt._linear_interp1d.py_func(c, ph_tot) for c in chis])
     bis = []
     saved = g["np"]
@@ -453,6 +457,147 @@ def gen_od():
              log_delta_min=float(ldm), log_delta_delta=(0 - ldm) / (delta_N - 1),
              q_chi=chis, q_r=rs_, q_interp=interp, q_bisect=np.array(bis),
              q_chi_pair=chis_p, q_r_pair=rs_p, q_interp_pair=interp_p, q_bisect_pair=np.array(bis_p))
+
+
+# ---------------------------------------------------------------------------
+# Whole optical-depth runs.  The reference picks the method when it is
+# imported (qed/__init__.py), so they run in a child process with
+# SFPARTICLES_OPTICAL_DEPTH=1, from a scratch copy of the reference package
+# in which the rate tables are written as optical_depth_tables.h5 (served by
+# the h5py stand-in).  The tables are the reference grid (rows 0-255,
+# log10 chi in [-3, 2]) of sfparticles_b200's shipped tables, which equal the
+# reference generator's rows wherever those are finite.  Both cases keep chi
+# below 100 (the reference's interpolation reads past its last row above it)
+# and give no appended particle an optical depth, where the reference copies
+# stale values cyclically (numpy.resize) and the oracle starts at zero.
+OD_SIM_CASES = {
+    # electrons emit by optical depth, with recoil, in a laser pulse; photons make no pairs
+    "od_emission": dict(kind="od", n_e=48, gamma0=4000.0, a0=600.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 100, steps=260,
+                        field="gaussian", lead=1.2e-6, seed=31, thr=2.0),
+    # photons convert to pairs by optical depth in a static field; the pairs do not radiate
+    "od_pairs": dict(kind="od", n_g=2000, gamma_lo=3000.0, gamma_hi=30000.0, chi_ref=1.5, gamma_ref=1e4,
+                     dt=1.5e-15, steps=40, seed=32, thr=2.0),
+}
+
+
+def _od_injected(kind, sim, species, seed):
+    """update_tau_e / update_tau_gamma of the reference (their Python bodies,
+    one particle per call) fed the oracle's keyed draws: purpose 1 gives the
+    reset draw (used when tau == 0) and the draw after an event, purpose 2
+    the inverse-CDF draw of _bisect_interp."""
+    from sfparticles.qed import optical_depth as od
+    from sfparticles.qed import optical_depth_tables as odt
+    fn = (od.update_tau_e if kind == "e" else od.update_tau_gamma).py_func
+    name = "photon_delta_from_chi_delta_table" if kind == "e" else "pair_delta_from_chi_delta_table"
+    table = odt._integral_photon_prob_along_delta if kind == "e" else odt._integral_pair_prob_along_delta
+    G, T = fn.__globals__, odt.__dict__
+
+    def run(tau, inv_gamma, chi, dt, N, pruned, event, delta):
+        stream = next(i for i, p in enumerate(species) if getattr(p, "tau", None) is tau)
+        slots = np.arange(N)
+        ra = orc.uniform2(seed, stream, sim.step, 1, slots)
+        rb = orc.uniform2(seed, stream, sim.step, 2, slots)
+        saved = G["random"], G[name], T["np"]
+
+        def draw(c, r):
+            T["np"] = _NP([r])
+            try:
+                return odt._bisect_interp.py_func(c, table)
+            finally:
+                T["np"] = saved[2]
+
+        try:
+            for ip in range(N):
+                G["random"] = _QueueRandom(np.array(([ra[ip, 0]] if tau[ip] == 0.0 else []) + [ra[ip, 1]]))
+                G[name] = lambda c, r=rb[ip, 0]: draw(c, r)
+                fn(tau[ip:ip + 1], inv_gamma[ip:ip + 1], chi[ip:ip + 1], dt, 1, pruned[ip:ip + 1],
+                   event[ip:ip + 1], delta[ip:ip + 1])
+        finally:
+            G["random"], G[name] = saved[0], saved[1]
+
+    return run
+
+
+def od_pairs_initial(case, rng):
+    """Photons along +x at the origin, energies log-uniform."""
+    n = case["n_g"]
+    g = np.exp(rng.uniform(math.log(case["gamma_lo"]), math.log(case["gamma_hi"]), n))
+    return [np.zeros(n), np.zeros(n), np.zeros(n), g, np.zeros(n), np.zeros(n)]
+
+
+def od_pairs_bz(case):
+    """Static B_z that gives chi_ref to a photon of gamma_ref moving along x."""
+    from scipy.constants import c, e, hbar, m_e
+    return case["chi_ref"] * m_e ** 2 * c ** 2 / e / hbar / case["gamma_ref"]
+
+
+def _od_sims_child():
+    import sfparticles
+    from sfparticles import fields as F
+    from sfparticles import particles as P
+    assert P._use_optical_depth
+    saved = P.update_tau_e, P.update_tau_gamma
+    for name, case in OD_SIM_CASES.items():
+        rng = np.random.default_rng(sum(map(ord, name)))
+        seed = case["seed"]
+        if name == "od_emission":
+            props, _ = sim_initial(case, rng)
+            terms, comb = sim_field_spec(case)
+            fld = getattr(F, terms[0][0])(**terms[0][1])
+            ele = sfparticles.Particles("ele", -1, 1, N=case["n_e"], props=tuple(np.array(a) for a in props))
+            pho = sfparticles.Particles("pho", 0, 0)
+            ele.set_photon(pho)
+            species = [ele, pho]
+            dt = 0.8e-6 / 299792458.0 * case["dt_T0"]
+        else:
+            props = od_pairs_initial(case, rng)
+            terms, comb = [("static_field", dict(Bz=od_pairs_bz(case)))], 0
+            fld = F.static_field(Bz=od_pairs_bz(case))
+            pho = sfparticles.Particles("pho", 0, 0, N=case["n_g"], props=tuple(np.array(a) for a in props))
+            ele = sfparticles.Particles("ele", -1, 1)
+            pos = sfparticles.Particles("pos", 1, 1)
+            pho.set_pair(ele, pos)
+            species = [ele, pos, pho]
+            dt = case["dt"]
+        sim = sfparticles.Simulation(*species, dt=dt, fields=fld, print_every=None, photon_threshold=case["thr"])
+        P.update_tau_e = _od_injected("e", sim, species, seed)
+        P.update_tau_gamma = _od_injected("g", sim, species, seed)
+        t0 = time.time()
+        try:
+            sim.start(case["steps"])
+        finally:
+            P.update_tau_e, P.update_tau_gamma = saved
+        res = {"case": json.dumps(case), "field_terms": json.dumps(terms), "field_comb": json.dumps(comb),
+               "dt": dt, "init": np.stack(props)}
+        for i, p in enumerate(species):
+            res[f"s{i}_state"] = np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+            res[f"s{i}_name"] = p.name
+        res["n_species"] = len(species)
+        np.savez(out(f"ref_sim_{name}.npz"), **res)
+        print(f"  sim {name}: {[p.N_buffered for p in species]} in {time.time() - t0:.1f}s")
+
+
+def gen_od_sims():
+    """Prepare the scratch reference copy with its OD tables and run the child."""
+    import shutil
+    import subprocess
+    sys.path.insert(0, REPO)
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    n = 256
+    with tempfile.TemporaryDirectory() as tmp:
+        shutil.copytree(os.path.join(REF, "sfparticles"), os.path.join(tmp, "sfparticles"),
+                        ignore=shutil.ignore_patterns("__pycache__"))
+        with open(os.path.join(tmp, "sfparticles", "qed", "optical_depth_tables.h5"), "wb") as f:
+            np.savez(f, photon_prob_rate_total=d["photon_rate_total"][:n], pair_prob_rate_total=d["pair_rate_total"][:n],
+                     integral_photon_prob_along_delta=d["photon_cumulative"][:n],
+                     integral_pair_prob_along_delta=d["pair_cumulative"][:n],
+                     attr_chi_N=np.int64(n), attr_log_chi_range=np.array([-3.0, 2.0]),
+                     attr_log_chi_delta=np.float64(d["log_chi_delta"]), attr_delta_N=np.int64(1024),
+                     attr_log_delta_range=np.array([float(d["log_delta_min"]), 0.0]),
+                     attr_log_delta_delta=np.float64(d["log_delta_delta"]))
+        env = dict(os.environ, SFPARTICLES_OPTICAL_DEPTH="1", SFP_REFERENCE=tmp)
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--od-child"], env=env, check=True)
 
 
 # ---------------------------------------------------------------------------
@@ -516,12 +661,16 @@ def gen_stats():
 
 
 PARTS = dict(tables=gen_tables, pushers=gen_pushers, fields=gen_fields, rates=gen_rates, rs_events=gen_rs_events,
-             sims=gen_sims, od=gen_od, stats=gen_stats)
+             sims=gen_sims, od=gen_od, od_sims=gen_od_sims, stats=gen_stats)
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*", default=None)
+    ap.add_argument("--od-child", action="store_true", help=argparse.SUPPRESS)
     a = ap.parse_args()
+    if a.od_child:
+        _od_sims_child()
+        sys.exit(0)
     for k, fn in PARTS.items():
         if a.only and k not in a.only:
             continue

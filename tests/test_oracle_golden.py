@@ -213,6 +213,53 @@ def oracle_case_sim(g):
     return case, sim, species
 
 
+def oracle_od_case_sim(g):
+    """Rebuild a whole optical-depth fixture case on the oracle, with the
+    shipped tables (the fixture ran the reference on their first 256 rows,
+    its own chi grid)."""
+    from sfparticles_b200.qed import tables
+    case = json.loads(str(g["case"]))
+    d = tables.od_tables()
+    tabs = [orc.make_od_table(d[f"{k}_rate_total"], d[f"{k}_cumulative"], float(d["log_chi_min"]),
+                              float(d["log_chi_delta"]), float(d["log_delta_min"]), float(d["log_delta_delta"]))
+            for k in ("photon", "pair")]
+    (nm, kw), = json.loads(str(g["field_terms"]))
+    terms = getattr(orc, nm)(**kw)
+    init = [np.ascontiguousarray(a) for a in g["init"]]
+    if "n_e" in case:
+        ele = orc.Species("ele", -1, 1, N=case["n_e"], props=init)
+        pho = orc.Species("pho", 0, 0)
+        ele.set_photon(pho, od=True)
+        species = [ele, pho]
+    else:
+        ele, pos = orc.Species("ele", -1, 1), orc.Species("pos", 1, 1)
+        pho = orc.Species("pho", 0, 0, N=case["n_g"], props=init)
+        pho.set_pair(ele, pos, od=True)
+        species = [ele, pos, pho]
+    sim = orc.OracleSim(species, float(g["dt"]), terms, ("od", tabs[0], tabs[1]), seed=case["seed"],
+                        photon_threshold=case["thr"])
+    return case, sim, species
+
+
+@pytest.mark.parametrize("name", ["od_emission", "od_pairs"])
+def test_whole_optical_depth_simulation_matches_reference(name):
+    """Reference Simulation.start in its optical-depth mode (its update_tau_e /
+    update_tau_gamma and _bisect_interp fed the oracle's Philox draws) vs the
+    oracle step loop: photon emission with recoil in a laser pulse, and pair
+    creation by photons in a static field."""
+    g = golden(f"ref_sim_{name}.npz")
+    case, sim, species = oracle_od_case_sim(g)
+    sim.run(case["steps"])
+    assert len(species) == int(g["n_species"])
+    for i, p in enumerate(species):
+        p.prune()
+        got = np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+        ref = g[f"s{i}_state"]
+        assert got.shape == ref.shape, (p.name, got.shape, ref.shape)
+        assert ref.shape[1] > 0, p.name
+        np.testing.assert_array_equal(got, ref, err_msg=p.name)
+
+
 @pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "CLL_focused", "push_only"])
 def test_whole_simulation_matches_reference(name):
     """Reference Simulation.start (its own orchestration, growth, appends and
