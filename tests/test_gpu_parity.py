@@ -265,6 +265,48 @@ def test_fused_step_matches_oracle(name):
     assert sim.particle_steps > 0
 
 
+@pytest.mark.parametrize("name", ["od_emission", "od_pairs"])
+def test_fused_optical_depth_matches_oracle_and_reference(name):
+    """Optical-depth runs (emission with recoil in a laser pulse; pair creation
+    by photons in a static field): the fused float64 step vs the oracle and vs
+    the reference's own Simulation.start fed the same keyed draws."""
+    cuda_or_skip()
+    import sfparticles_b200 as S
+    from sfparticles_b200 import qed
+    from test_oracle_golden import oracle_od_case_sim
+    g = golden(f"ref_sim_{name}.npz")
+    case = json.loads(str(g["case"]))
+    init = tuple(np.array(a) for a in g["init"])
+    qed.set_method("od")
+    try:
+        if "n_e" in case:
+            ele = S.Particles("ele", -1, 1, N=case["n_e"], props=init)
+            pho = S.Particles("pho", 0, 0)
+            ele.set_photon(pho)
+            species = [ele, pho]
+        else:
+            ele, pos = S.Particles("ele", -1, 1), S.Particles("pos", 1, 1)
+            pho = S.Particles("pho", 0, 0, N=case["n_g"], props=init)
+            pho.set_pair(ele, pos)
+            species = [ele, pos, pho]
+    finally:
+        qed.set_method("rs")
+    sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
+                       photon_threshold=case["thr"], seed=case["seed"])
+    sim.start(case["steps"])
+    _, osim, ospecies = oracle_od_case_sim(g)
+    osim.run(case["steps"])
+    keys = ("x", "y", "z", "ux", "uy", "uz")
+    for i, (p, o) in enumerate(zip(species, ospecies)):
+        o.prune()
+        got = np.stack([getattr(p, k) for k in keys])
+        ref = np.stack([getattr(o, k) for k in keys])
+        assert got.shape == ref.shape == g[f"s{i}_state"].shape, (p.name, got.shape, ref.shape)
+        assert got.shape[1] > 0, p.name
+        assert _rel(got, ref) < RTOL_RUN, (p.name, _rel(got, ref))
+        assert _rel(got, g[f"s{i}_state"]) < RTOL_RUN, (p.name, _rel(got, g[f"s{i}_state"]))
+
+
 @pytest.mark.parametrize("name", ["spin_LL", "CLL_focused", "push_only"])
 def test_fused_deterministic_push_matches_reference(name):
     """Emission off: the GPU run vs the reference's own Simulation.start, 1e-10."""
