@@ -474,6 +474,9 @@ OD_SIM_CASES = {
     # electrons emit by optical depth, with recoil, in a laser pulse; photons make no pairs
     "od_emission": dict(kind="od", n_e=48, gamma0=4000.0, a0=600.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 100, steps=260,
                         field="gaussian", lead=1.2e-6, seed=31, thr=2.0),
+    # the same with Thomas-BMT spin (the avalanche's electrons)
+    "od_spin_emission": dict(kind="od", n_e=32, gamma0=3000.0, a0=300.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 100,
+                             steps=200, field="gaussian", lead=1.0e-6, seed=33, thr=1.0, spin=True),
     # photons convert to pairs by optical depth in a static field; the pairs do not radiate
     "od_pairs": dict(kind="od", n_g=2000, gamma_lo=3000.0, gamma_hi=30000.0, chi_ref=1.5, gamma_ref=1e4,
                      dt=1.5e-15, steps=40, seed=32, thr=2.0),
@@ -540,11 +543,19 @@ def _od_sims_child():
     for name, case in OD_SIM_CASES.items():
         rng = np.random.default_rng(sum(map(ord, name)))
         seed = case["seed"]
-        if name == "od_emission":
-            props, _ = sim_initial(case, rng)
+        spin = None
+        if "n_e" in case:
+            props, spin = sim_initial(case, rng)
             terms, comb = sim_field_spec(case)
             fld = getattr(F, terms[0][0])(**terms[0][1])
-            ele = sfparticles.Particles("ele", -1, 1, N=case["n_e"], props=tuple(np.array(a) for a in props))
+            if case.get("spin"):
+                # SpinParticles cannot take props in the reference: set the state after construction
+                ele = sfparticles.SpinParticles("ele", -1, 1, N=case["n_e"])
+                ele.x, ele.y, ele.z, ele.ux, ele.uy, ele.uz = [np.array(a) for a in props]
+                ele.inv_gamma = 1 / np.sqrt(1 + ele.ux ** 2 + ele.uy ** 2 + ele.uz ** 2)
+                ele.sx, ele.sy, ele.sz = [np.array(a) for a in spin]
+            else:
+                ele = sfparticles.Particles("ele", -1, 1, N=case["n_e"], props=tuple(np.array(a) for a in props))
             pho = sfparticles.Particles("pho", 0, 0)
             ele.set_photon(pho)
             species = [ele, pho]
@@ -569,8 +580,11 @@ def _od_sims_child():
             P.update_tau_e, P.update_tau_gamma = saved
         res = {"case": json.dumps(case), "field_terms": json.dumps(terms), "field_comb": json.dumps(comb),
                "dt": dt, "init": np.stack(props)}
+        if case.get("spin"):
+            res["spin_init"] = np.stack(spin)
         for i, p in enumerate(species):
-            res[f"s{i}_state"] = np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+            keys = ["x", "y", "z", "ux", "uy", "uz"] + (["sx", "sy", "sz"] if hasattr(p, "sx") else [])
+            res[f"s{i}_state"] = np.stack([getattr(p, k) for k in keys])
             res[f"s{i}_name"] = p.name
         res["n_species"] = len(species)
         np.savez(out(f"ref_sim_{name}.npz"), **res)

@@ -265,7 +265,7 @@ def test_fused_step_matches_oracle(name):
     assert sim.particle_steps > 0
 
 
-@pytest.mark.parametrize("name", ["od_emission", "od_pairs"])
+@pytest.mark.parametrize("name", ["od_emission", "od_spin_emission", "od_pairs"])
 def test_fused_optical_depth_matches_oracle_and_reference(name):
     """Optical-depth runs (emission with recoil in a laser pulse; pair creation
     by photons in a static field): the fused float64 step vs the oracle and vs
@@ -280,7 +280,11 @@ def test_fused_optical_depth_matches_oracle_and_reference(name):
     qed.set_method("od")
     try:
         if "n_e" in case:
-            ele = S.Particles("ele", -1, 1, N=case["n_e"], props=init)
+            if case.get("spin"):
+                ele = S.SpinParticles("ele", -1, 1, N=case["n_e"],
+                                      props=init + tuple(np.array(a) for a in g["spin_init"]))
+            else:
+                ele = S.Particles("ele", -1, 1, N=case["n_e"], props=init)
             pho = S.Particles("pho", 0, 0)
             ele.set_photon(pho)
             species = [ele, pho]
@@ -296,9 +300,9 @@ def test_fused_optical_depth_matches_oracle_and_reference(name):
     sim.start(case["steps"])
     _, osim, ospecies = oracle_od_case_sim(g)
     osim.run(case["steps"])
-    keys = ("x", "y", "z", "ux", "uy", "uz")
     for i, (p, o) in enumerate(zip(species, ospecies)):
         o.prune()
+        keys = ["x", "y", "z", "ux", "uy", "uz"] + (["sx", "sy", "sz"] if o.spin else [])
         got = np.stack([getattr(p, k) for k in keys])
         ref = np.stack([getattr(o, k) for k in keys])
         assert got.shape == ref.shape == g[f"s{i}_state"].shape, (p.name, got.shape, ref.shape)

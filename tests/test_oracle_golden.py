@@ -227,7 +227,9 @@ def oracle_od_case_sim(g):
     terms = getattr(orc, nm)(**kw)
     init = [np.ascontiguousarray(a) for a in g["init"]]
     if "n_e" in case:
-        ele = orc.Species("ele", -1, 1, N=case["n_e"], props=init)
+        spin = bool(case.get("spin"))
+        ele = orc.Species("ele", -1, 1, N=case["n_e"], props=init, spin=spin,
+                          spin_props=[np.ascontiguousarray(a) for a in g["spin_init"]] if spin else None)
         pho = orc.Species("pho", 0, 0)
         ele.set_photon(pho, od=True)
         species = [ele, pho]
@@ -241,19 +243,20 @@ def oracle_od_case_sim(g):
     return case, sim, species
 
 
-@pytest.mark.parametrize("name", ["od_emission", "od_pairs"])
+@pytest.mark.parametrize("name", ["od_emission", "od_spin_emission", "od_pairs"])
 def test_whole_optical_depth_simulation_matches_reference(name):
     """Reference Simulation.start in its optical-depth mode (its update_tau_e /
     update_tau_gamma and _bisect_interp fed the oracle's Philox draws) vs the
-    oracle step loop: photon emission with recoil in a laser pulse, and pair
-    creation by photons in a static field."""
+    oracle step loop: photon emission with recoil in a laser pulse, without
+    and with Thomas-BMT spin, and pair creation by photons in a static field."""
     g = golden(f"ref_sim_{name}.npz")
     case, sim, species = oracle_od_case_sim(g)
     sim.run(case["steps"])
     assert len(species) == int(g["n_species"])
     for i, p in enumerate(species):
         p.prune()
-        got = np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+        keys = ["x", "y", "z", "ux", "uy", "uz"] + (["sx", "sy", "sz"] if p.spin else [])
+        got = np.stack([getattr(p, k) for k in keys])
         ref = g[f"s{i}_state"]
         assert got.shape == ref.shape, (p.name, got.shape, ref.shape)
         assert ref.shape[1] > 0, p.name
