@@ -703,7 +703,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--roofline-steps", type=int, default=8)
-    ap.add_argument("--cpu-electrons", type=int, default=10_000)
+    ap.add_argument("--cpu-electrons", type=int, default=20_000)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
@@ -776,7 +776,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, steps, ps, dt = cpu_sample(args.cpu_electrons, STEPS_FULL, args.cpu_budget, 1)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": omp_threads(), "kind": "port",
-               "sample": f"{args.cpu_electrons} e- of the same cascade (1/1000 of the beam), first {steps} steps, "
+               "sample": f"{args.cpu_electrons} e- of the same cascade (1/{args.electrons // args.cpu_electrons} of "
+                         f"the beam), first {steps} steps, "
                          f"{ps:.3g} particle-steps in {dt:.1f}s"}
 
     r = run_ours(args, rank, world)
