@@ -301,6 +301,10 @@ SIM_CASES = {
     # deterministic Landau-Lifshitz + spin, no emission
     "spin_LL": dict(kind="det", n_e=32, gamma0=2000.0, a0=200.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
                     field="gaussian", lead=3e-6, spin=True, rr="LL", pairs=False, seed=0, thr=2.0),
+    # spin with RR=CLL: the reference's spin push has no CLL branch (particles.py:596-604),
+    # so this is the plain Boris-TBMT push
+    "spin_CLL": dict(kind="det", n_e=32, gamma0=2000.0, a0=200.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
+                     field="gaussian", lead=3e-6, spin=True, rr="CLL", pairs=False, seed=0, thr=2.0),
     # deterministic quantum-corrected LL with a focused pulse
     "CLL_focused": dict(kind="det", n_e=32, gamma0=1500.0, a0=150.0, w0=2.5e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
                         field="focused", lead=3e-6, spin=False, rr="CLL", pairs=False, seed=0, thr=2.0),

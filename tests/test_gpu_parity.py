@@ -248,7 +248,7 @@ def _oracle_case(g):
     return species
 
 
-@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "CLL_focused", "push_only"])
+@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "spin_CLL", "CLL_focused", "push_only"])
 def test_fused_step_matches_oracle(name):
     """Fused Simulation.start on the GPU vs the oracle step loop, same Philox
     keys: identical particle counts and order, states within tolerance."""
@@ -311,7 +311,7 @@ def test_fused_optical_depth_matches_oracle_and_reference(name):
         assert _rel(got, g[f"s{i}_state"]) < RTOL_RUN, (p.name, _rel(got, g[f"s{i}_state"]))
 
 
-@pytest.mark.parametrize("name", ["spin_LL", "CLL_focused", "push_only"])
+@pytest.mark.parametrize("name", ["spin_LL", "spin_CLL", "CLL_focused", "push_only"])
 def test_fused_deterministic_push_matches_reference(name):
     """Emission off: the GPU run vs the reference's own Simulation.start, 1e-10."""
     cuda_or_skip()
