@@ -305,6 +305,12 @@ SIM_CASES = {
     # so this is the plain Boris-TBMT push
     "spin_CLL": dict(kind="det", n_e=32, gamma0=2000.0, a0=200.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
                      field="gaussian", lead=3e-6, spin=True, rr="CLL", pairs=False, seed=0, thr=2.0),
+    # Landau-Lifshitz without spin, through the plane-wave-like pulse (Gaussian in time)
+    "simple_LL": dict(kind="det", n_e=32, gamma0=2000.0, a0=150.0, w0=3e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
+                      field="simple", t_order=2, lead=3e-6, spin=False, rr="LL", pairs=False, seed=0, thr=2.0),
+    # emission off through the same pulse with a fourth-order temporal envelope
+    "simple_t4": dict(kind="det", n_e=32, gamma0=500.0, a0=20.0, w0=3e-6, ctau=6e-6, dt_T0=1 / 50, steps=300,
+                      field="simple", t_order=4, lead=4e-6, spin=False, rr="NONE", pairs=False, seed=0, thr=2.0),
     # deterministic quantum-corrected LL with a focused pulse
     "CLL_focused": dict(kind="det", n_e=32, gamma0=1500.0, a0=150.0, w0=2.5e-6, ctau=5e-6, dt_T0=1 / 50, steps=300,
                         field="focused", lead=3e-6, spin=False, rr="CLL", pairs=False, seed=0, thr=2.0),
@@ -339,6 +345,9 @@ def sim_field_spec(case):
         return [("gaussian_laser_pulse", dict(a0=a, w0=w0, ctau=ctau, direction=-1, x0=x0, pol_angle=0.0)),
                 ("gaussian_laser_pulse", dict(a0=a, w0=w0, ctau=ctau, direction=-1, x0=x0, pol_angle=math.pi / 2,
                                               cep=math.pi / 2))], [0, 1]
+    if case["field"] == "simple":
+        return [("simple_laser_pulse", dict(a0=a0, w0=w0, ctau=ctau, t_order=case["t_order"], direction=-1,
+                                            x0=x0))], 0
     raise ValueError(case["field"])
 
 

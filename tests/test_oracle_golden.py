@@ -263,7 +263,8 @@ def test_whole_optical_depth_simulation_matches_reference(name):
         np.testing.assert_array_equal(got, ref, err_msg=p.name)
 
 
-@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "spin_CLL", "CLL_focused", "push_only"])
+@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "spin_CLL", "simple_LL", "simple_t4",
+                                  "CLL_focused", "push_only"])
 def test_whole_simulation_matches_reference(name):
     """Reference Simulation.start (its own orchestration, growth, appends and
     pushes; samplers fed the oracle's Philox draws) vs the oracle step loop."""
