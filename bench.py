@@ -43,8 +43,11 @@ BYTES_EPM = 97      # pushed e+-: x,y,z,ux,uy,uz read + written (96) + alive fla
 BYTES_PHOTON = 73   # pushed photon: x,y,z,ux,uy,uz read (48) + flag (1) + x,y,z written (24)
 BYTES_DEAD = 1      # pruned slot: flag read
 BYTES_APPEND = 49   # appended particle: x,y,z,ux,uy,uz + flag written
-BYTES_PAIR = 155    # pair event in the pairs kernel: parent state + delta read (56), flag (1), e- and e+ written (98)
-BYTES_PTILE = 4     # photon-tile event counter read by the pairs kernel (one per 1024 photons)
+BYTES_EMIT_MARK = 9  # emitter in the massive kernel: delta (8) + mark (1) written instead of its state
+BYTES_EMIT = 154    # emitter in the appends kernel: parent state + delta read (56), photon written (49), parent
+                    # state + flag written (49)
+BYTES_PAIR = 155    # pair event in the appends kernel: parent state + delta read (56), flag (1), e- and e+
+                    # written (98)
 # DRAM bytes (read + write, ncu) / algorithmic bytes of one launch, from an ncu capture of the same
 # cascade at 1e6 electrons at its final state (2.8 GB of photon state, larger than L2, so traffic
 # scales with the units processed).  Only kernels whose state exceeds L2 in that capture are listed.
@@ -52,6 +55,14 @@ NCU_TRAFFIC_RATIO = {"photon": 2.768e9 / 2.806e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
+# upper edge of the photon spectrum bins: above every photon (the beam's gamma stays below 2200)
+SPECTRUM_HI = 2500.0
+
+
+def window_label(start, steps):
+    return f"{WORKLOAD}; timed window: steps {start}-{start + steps}" + (
+        " (the collision: beam and pulse centres meet at the focus at step 1500)"
+        if start < STEPS_FULL // 2 < start + steps else "")
 
 
 def beam(n, seed, steps=STEPS_FULL):
@@ -76,7 +87,7 @@ def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64
     pho.set_pair(ele, pos)
     fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
     sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form,
-                       items=massive[0], min_blocks=massive[1], p_stages=photon[0], p_min_blocks=photon[1],
+                       m_stages=massive[0], min_blocks=massive[1], p_stages=photon[0], p_min_blocks=photon[1],
                        graph_chunk=graph_chunk, engine=engine)
     return sim
 
@@ -159,7 +170,7 @@ def run_c4(args):
     for j, k in enumerate(("massive", "photon")):
         gbs = alg[k] / (k_ms[j] * 1e-3) / 1e9 if k_ms[j] > 0 else 0.0
         per_kernel[k] = {"avg_ms": k_ms[j], "alg_bytes_per_launch": alg[k], "achieved_gbs": gbs, "frac": gbs / peak}
-    per_kernel["pairs"] = {"avg_ms": k_ms[2]}
+    per_kernel["appends"] = {"avg_ms": k_ms[2]}
     dominant = max(("massive", "photon"), key=lambda k: per_kernel[k]["avg_ms"])
     dk = per_kernel[dominant]
     ens.finish()
@@ -358,7 +369,7 @@ def run_c5(args):
                     "achieved_gbs": alg_m / (k_ms[0] * 1e-3) / 1e9 if k_ms[0] else 0.0},
         "photon": {"avg_ms": k_ms[1], "alg_bytes_per_launch": alg_p,
                    "achieved_gbs": alg_p / (k_ms[1] * 1e-3) / 1e9 if k_ms[1] else 0.0},
-        "pairs": {"avg_ms": k_ms[2]}}
+        "appends": {"avg_ms": k_ms[2]}}
     dominant = max(("massive", "photon"), key=lambda k: per_kernel[k]["avg_ms"])
     dk = per_kernel[dominant]
     line = {"metric": "particle-steps/s", "value": ps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
@@ -428,10 +439,13 @@ def make_oracle_sim(n, seed):
     return orc.OracleSim([ele, pos, pho], DT, terms, ("rs", iA, dA), seed=seed, z_max=zmax)
 
 
-def cpu_sample(n_e, max_steps, budget_s, warmup):
-    """Oracle port (C, OpenMP, all host threads) on a bounded sample."""
+def cpu_sample(n_e, start, max_steps, budget_s):
+    """Oracle port (C, OpenMP, all host threads) on a bounded sample of the
+    same window: `n_e` electrons of the same beam advanced untimed to step
+    `start`, then up to `max_steps` steps timed (fewer if `budget_s` runs
+    out).  Returns (rate, steps timed, particle-steps, seconds)."""
     sim = make_oracle_sim(n_e, 12345)
-    sim.run(warmup)
+    sim.run(max(start, 1))  # untimed: the approach (and one step of warm-up)
     ps0 = sim.particle_steps
     t0 = time.perf_counter()
     steps = 0
@@ -441,6 +455,19 @@ def cpu_sample(n_e, max_steps, budget_s, warmup):
     dt = time.perf_counter() - t0
     ps = sim.particle_steps - ps0
     return ps / dt, steps, ps, dt
+
+
+def window_start(args):
+    """First step of the timed window.  `--start-step` if given; else, when
+    the window is shorter than the 3000-step run, the steps centred on the
+    collision (the beam and pulse centres meet at the focus at step 1500), so
+    the window times the cascade -- photon emission and pair creation --
+    rather than the approach; else step 0."""
+    if args.start_step is not None and args.start_step >= 0:
+        return min(args.start_step, STEPS_FULL)
+    if args.steps >= STEPS_FULL:
+        return 0
+    return max(0, STEPS_FULL // 2 - args.steps // 2)
 
 
 def omp_threads():
@@ -511,20 +538,47 @@ def run_ours(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     seed = 1000 + rank
+    S0 = window_start(args)
     # warm-up: compile / load the module, W steps of a small instance, then a fresh timed instance
     wsim = make_sim(max(1000, args.electrons // 1000), seed, args.form)
     wsim.run_on_device(args.warmup)
     wsim.finish()
     del wsim
-    sim = make_sim(args.electrons, seed, args.form, (args.items, args.min_blocks), (args.p_stages, args.p_min_blocks),
+    sim = make_sim(args.electrons, seed, args.form, (args.m_stages, args.min_blocks), (args.p_stages, args.p_min_blocks),
                    graph_chunk=0 if args.no_graphs else 64)
     sim._begin()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    phases = {}  # device ms and particle-steps of the timed phases of the 3000-step run
+
+    def timed(name, n):
+        ps_a = sim.particle_steps
+        torch.cuda.synchronize()
+        e0.record()
+        sim.run_on_device(n)
+        e1.record()
+        torch.cuda.synchronize()
+        phases[name] = (e0.elapsed_time(e1), sim.particle_steps - ps_a, n)
+
+    # the approach, untimed for the headline: up to the variant search, which
+    # measures the kernel variants on the state the window starts from
+    from sfparticles_b200 import autotune
+    nvar = sum(len(v) for v in autotune.VARIANTS[(args.form, "rs")]) * 2
+    tune = not args.no_variants and S0 >= nvar
+    tm, tp = {}, {}
+    if S0 - (nvar if tune else 0) > 0:
+        timed("approach", S0 - (nvar if tune else 0))
+    if tune:
+        tm, tp = autotune.measure(sim, steps=2)
+        sim.set_kernel(massive=min(tm, key=tm.get), photon=min(tp, key=tp.get))
+    assert sim.step == S0, (sim.step, S0)
+    sim.reserve(args.steps)  # room for the window at twice the rate seen, so no growth inside it
+    start_counts = {p.name: p.N_buffered for p in sim.all_particles}
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     launches0 = sim.kernel_launches
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    ps0 = sim.particle_steps
     with ClockSampler(dev.index) as clk:
         e0.record()
         sim.run_on_device(args.steps)
@@ -532,14 +586,14 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = sim.kernel_launches - launches0
-    ps = sim.particle_steps
+    ps = sim.particle_steps - ps0
+    phases["window"] = (ms, ps, args.steps)
     counts = {p.name: p.N_buffered for p in sim.all_particles}
-    # roofline of each step kernel at the final state: CUDA events around every launch
-    from sfparticles_b200 import autotune
-    tm, tp = {}, {}
-    if not args.no_variants:
-        tm, tp = autotune.measure(sim, steps=2)
-        sim.set_kernel(massive=min(tm, key=tm.get), photon=min(tp, key=tp.get))
+    spectrum = None
+    if not args.no_compare:
+        from sfparticles_b200 import diagnostics as D
+        spectrum = D.photon_spectrum_device(sim.all_particles[2], 64, 2.0, SPECTRUM_HI)
+    # roofline of each step kernel at the window's end state: CUDA events around every launch
     alive = {p.name: p.Npart for p in sim.all_particles}
     buffered = {p.name: p.N_buffered for p in sim.all_particles}
     torch.cuda.nvtx.range_push("roofline")  # profilers select these launches by this range
@@ -550,34 +604,60 @@ def run_ours(args, rank, world):
     n_pairs = (after[1] - before[1]) / args.roofline_steps    # pairs per step
     n_epm = alive["electron"] + alive["positron"]
     dead_m = buffered["electron"] + buffered["positron"] - n_epm
+    # algorithmic bytes of each launch: the massive kernel streams every e+- (state read, a
+    # non-emitter's written back, an emitter's delta and mark written), the appends kernel reads
+    # each emitter / converted photon again and writes the children and the emitter's new state
+    n_emit = n_ph_app
     alg = {
-        "massive": n_epm * BYTES_EPM + dead_m * BYTES_DEAD + n_ph_app * BYTES_APPEND,
-        "photon": alive["photon"] * BYTES_PHOTON + (buffered["photon"] - alive["photon"]) * BYTES_DEAD
-        + 2 * n_pairs * BYTES_APPEND,
-        "pairs": n_pairs * BYTES_PAIR + math.ceil(buffered["photon"] / 1024) * BYTES_PTILE,
+        "massive": n_epm * (BYTES_EPM - 48) + (n_epm - n_emit) * 48 + n_emit * BYTES_EMIT_MARK
+        + dead_m * BYTES_DEAD,
+        "photon": alive["photon"] * BYTES_PHOTON + (buffered["photon"] - alive["photon"]) * BYTES_DEAD,
+        "appends": n_emit * BYTES_EMIT + n_pairs * BYTES_PAIR,
     }
     names = {
-        "massive": f"sfp_massive_{args.form}_rs_i{sim.items}_b{sim.min_blocks}",
+        "massive": f"sfp_massive_{args.form}_rs_s{sim.m_stages}_b{sim.min_blocks}",
         "photon": f"sfp_photon_{args.form}_rs_s{sim.p_stages}_b{sim.p_min_blocks}",
-        "pairs": f"sfp_pair_scan_kernel+sfp_pairs_{args.form}",
+        "appends": f"sfp_scan_kernel+sfp_appends_{args.form}",
     }
     per_kernel = {}
-    for j, k in enumerate(("massive", "photon", "pairs")):
+    for j, k in enumerate(("massive", "photon", "appends")):
         gbs = alg[k] / (k_ms[j] * 1e-3) / 1e9 if k_ms[j] > 0 else 0.0
         per_kernel[k] = {"kernel": names[k], "avg_ms": k_ms[j], "alg_bytes_per_launch": alg[k],
                          "achieved_gbs": gbs}
     dominant = max(per_kernel, key=lambda k: per_kernel[k]["avg_ms"])
+    # the e+- push as SURVEY-style work: 97 B per e+- and 49 B per appended photon over the two
+    # launches that do it (the appends time also covers the step's pairs)
+    push_alg = n_epm * BYTES_EPM + dead_m * BYTES_DEAD + n_ph_app * BYTES_APPEND
+    push_ms = k_ms[0] + k_ms[2]
+    per_kernel["push_path"] = {"kernel": "massive + appends", "avg_ms": push_ms, "alg_bytes_per_launch": push_alg,
+                               "achieved_gbs": push_alg / (push_ms * 1e-3) / 1e9 if push_ms > 0 else 0.0}
     step_units = {"electrons+positrons_alive": n_epm, "photons_alive": alive["photon"],
                   "photons_appended_per_step": n_ph_app, "pairs_per_step": n_pairs}
-    sim.finish()
+    # the rest of the 3000-step run, for the whole-run rate (second field)
+    whole = None
+    if not args.no_whole_run and sim.step < STEPS_FULL:
+        timed("rest", STEPS_FULL - sim.step)
+    if "approach" in phases or "rest" in phases:
+        wms = sum(v[0] for v in phases.values())
+        wps = sum(v[1] for v in phases.values())
+        wst = sum(v[2] for v in phases.values())
+        whole = {"value": wps / (wms * 1e-3), "unit": "particle-steps/s", "steps_timed": wst, "ms": wms,
+                 "particle_steps": wps, "final_step": sim.step,
+                 "final_counts": {p.name: p.N_buffered for p in sim.all_particles},
+                 "note": f"steps 0-{sim.step} timed in phases; the {sim.step - wst} variant-search and roofline "
+                         "steps are excluded from both time and work"}
+    sim._end()
     del sim
-    torch.cuda.empty_cache()
+    _release()
 
-    # end to end through the public API from host arrays
+    # end to end through the public API from host arrays: the same window
     e2e = None
     if not args.no_e2e:
         sim2 = make_sim(args.electrons, seed, args.form)
+        if S0 > 0:
+            sim2.start(S0)  # untimed: the approach, ending in host arrays
         h2d = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
+        ps_a = sim2.particle_steps
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e0.record()
@@ -589,71 +669,50 @@ def run_ours(args, rank, world):
         d2h = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
         # whole job: the slowest rank's time, every rank's work and copies
         from sfparticles_b200.shard import reduce_job, sum_over_ranks
-        ms2, ps2 = reduce_job(max(ms2, wall * 1e3), sim2.particle_steps, device=dev)
+        ms2, ps2 = reduce_job(max(ms2, wall * 1e3), sim2.particle_steps - ps_a, device=dev)
         h2d, d2h = sum_over_ranks([h2d, d2h], device=dev)
         e2e = dict(value=ps2 / (ms2 * 1e-3), unit="particle-steps/s",
                    h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
-                   wall_s=wall)
+                   wall_s=wall, window=f"steps {S0}-{S0 + args.steps}: Simulation.start({args.steps}) from host "
+                                       f"arrays after an untimed start({S0})")
         del sim2
+        _release()
 
-    # chosen form vs the plain float64 form, same seed, on a tenth of the beam
+    # the chosen form vs the plain float64 form: same beam, seed and window
     compare = None
-    if not args.no_compare:
+    if not args.no_compare and args.form != "fp64":
         from sfparticles_b200 import diagnostics as D
-        res = {}
-        for form in ("fp64", args.form):
-            if form in res:
-                continue
-            s = make_sim(args.compare_electrons, seed + 7, form)
-            s._begin()
-            torch.cuda.synchronize()
-            e0.record()
-            s.run_on_device(args.steps)
-            e1.record()
-            torch.cuda.synchronize()
-            cms = e0.elapsed_time(e1)
-            cps = s.particle_steps
-            s.finish()
-            ele, pos, pho = s.all_particles
-            res[form] = dict(value=cps / (cms * 1e-3), energies=D.photon_energies(pho), pairs=pos.N_buffered,
-                             photons=pho.N_buffered)
-            del s
-        if not args.no_ops:
-            # the reference's own step loop over the one-for-one float64 kernels (engine 'ops')
-            s = make_sim(args.compare_electrons, seed + 7, "fp64", engine="ops")
-            for p in s.all_particles:
-                p._to_gpu()
-            torch.cuda.synchronize()
-            e0.record()
-            s._loop_ops(args.steps, None)
-            e1.record()
-            torch.cuda.synchronize()
-            cms = e0.elapsed_time(e1)
-            cps = s.particle_steps
-            for p in s.all_particles:
-                p._prune()
-                p._to_host()
-            ele, pos, pho = s.all_particles
-            res["ops"] = dict(value=cps / (cms * 1e-3), energies=D.photon_energies(pho), pairs=pos.N_buffered,
-                              photons=pho.N_buffered)
-            del s
-        a, b = res[args.form], res["fp64"]
-        hi = max(a["energies"].max(initial=2.0), b["energies"].max(initial=2.0))
-        ha, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=a["energies"])
-        hb, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=b["energies"])
-        compare = {"electrons": args.compare_electrons, "steps": args.steps, "fp64_value": b["value"],
-                   "form_value": a["value"], "speedup_vs_fp64": a["value"] / b["value"],
-                   "spectrum_rel_l1": D.spectrum_rel_l1(ha, hb), "spectrum_bins": 64,
-                   "pair_yield_rel": D.rel_diff(a["pairs"], b["pairs"]), "pairs_fp64": b["pairs"],
-                   "pairs_form": a["pairs"], "photons_fp64": b["photons"], "photons_form": a["photons"]}
-        if "ops" in res:
-            o = res["ops"]
-            ho, _ = D.photon_spectrum(None, 64, 2.0, hi, energies=o["energies"])
-            compare.update({"ops_fp64_value": o["value"], "speedup_vs_ops_fp64": a["value"] / o["value"],
-                            "spectrum_rel_l1_vs_ops": D.spectrum_rel_l1(ha, ho),
-                            "pair_yield_rel_vs_ops": D.rel_diff(a["pairs"], o["pairs"]), "pairs_ops": o["pairs"],
-                            "photons_ops": o["photons"]})
-        torch.cuda.empty_cache()
+        s = make_sim(args.electrons, seed, "fp64")
+        s._begin()
+        if S0 > 0:
+            s.run_on_device(S0)
+        s.reserve(args.steps)
+        torch.cuda.synchronize()
+        ps_a = s.particle_steps
+        e0.record()
+        s.run_on_device(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        fms = e0.elapsed_time(e1)
+        fps = s.particle_steps - ps_a
+        spec64 = D.photon_spectrum_device(s.all_particles[2], 64, 2.0, SPECTRUM_HI)
+        c64 = {p.name: p.N_buffered for p in s.all_particles}
+        s._end()
+        del s
+        _release()
+        pairs_form = counts["positron"] - start_counts["positron"]
+        pairs_64 = c64["positron"] - start_counts["positron"]
+        v64 = fps / (fms * 1e-3)
+        compare = {"electrons": args.electrons, "window": f"steps {S0}-{S0 + args.steps}", "fp64_value": v64,
+                   "form_value": ps / (ms * 1e-3), "speedup_vs_fp64": (ps / ms) / (fps / fms),
+                   "spectrum_rel_l1": D.spectrum_rel_l1(spectrum, spec64), "spectrum_bins": 64,
+                   "spectrum_range": [2.0, SPECTRUM_HI], "photons_in_spectrum": float(spec64.sum()),
+                   "pair_yield_rel": D.rel_diff(counts["positron"], c64["positron"]),
+                   "pairs_fp64": c64["positron"], "pairs_form": counts["positron"],
+                   "pairs_created_in_window_fp64": pairs_64, "pairs_created_in_window_form": pairs_form,
+                   "photons_fp64": c64["photon"], "photons_form": counts["photon"],
+                   "note": "fused float64 step (the reference arithmetic) over the same window after the same "
+                           "approach; spectrum of all photons alive at the window's end"}
 
     # max over ranks of the device time; sum of work
     from sfparticles_b200.shard import reduce_job
@@ -670,10 +729,15 @@ def run_ours(args, rank, world):
                           "traffic_note": "ncu DRAM bytes of a 1e6-electron capture scaled by units processed",
                           "kernel": dk["kernel"], "kernel_avg_ms": dk["avg_ms"],
                           "alg_bytes_per_launch": dk["alg_bytes_per_launch"], "launches_timed": args.roofline_steps,
-                          "units_at_final_state": step_units, "per_kernel": per_kernel,
-                          "variants_ms": {**{f"massive_i{a}_b{b}": v for (a, b), v in tm.items()},
+                          "units_at_window_end": step_units, "per_kernel": per_kernel,
+                          "variants_ms": {**{f"massive_s{a}_b{b}": v for (a, b), v in tm.items()},
                                           **{f"photon_s{a}_b{b}": v for (a, b), v in tp.items()}}},
-                e2e=e2e, compare=compare)
+                e2e=e2e, compare=compare, start_step=S0, start_counts=start_counts, whole=whole)
+
+
+def _release():
+    import torch
+    torch.cuda.empty_cache()
 
 
 def main():
@@ -691,11 +755,13 @@ def main():
     ap.add_argument("--particle-cap", type=int, default=1_000_000_000, help="c5: stop at this many particles")
     ap.add_argument("--electrons", type=int, default=10_000_000)
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
-    ap.add_argument("--compare-electrons", type=int, default=1_000_000)
-    ap.add_argument("--no-compare", action="store_true")
-    ap.add_argument("--no-ops", action="store_true", help="skip the per-op float64 engine in the comparison")
+    ap.add_argument("--start-step", type=int, default=None,
+                    help="c2: first step of the timed window (default: centred on the collision at step 1500 "
+                         "when --steps < 3000, else 0); the steps before it run untimed")
+    ap.add_argument("--no-whole-run", action="store_true", help="c2: skip the rest of the 3000-step run")
+    ap.add_argument("--no-compare", action="store_true", help="c2: skip the float64 run over the same window")
     ap.add_argument("--no-variants", action="store_true")
-    ap.add_argument("--items", type=int, default=0)
+    ap.add_argument("--m-stages", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--p-stages", type=int, default=0)
     ap.add_argument("--p-min-blocks", type=int, default=0)
@@ -751,13 +817,19 @@ def main():
         # the reference's CPU algorithm (oracle port) on the host cores; rank 0 only
         if rank != 0:
             return
-        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, args.steps, args.cpu_budget * 3, args.warmup)
+        S0 = window_start(args)
+        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, max(S0, args.warmup), args.steps, args.cpu_budget * 3)
+        S0 = max(S0, args.warmup, 1)
         cores = omp_threads()
-        sample = f"{args.cpu_electrons} e- of the same cascade, {steps} steps after {args.warmup} warm-up"
+        sample = (f"{args.cpu_electrons} e- of the same beam (1/{args.electrons // args.cpu_electrons} of it), "
+                  f"advanced untimed to step {S0}, then steps {S0}-{S0 + steps} timed: {ps:.3g} particle-steps "
+                  f"in {dt:.2f}s")
         line = {"impl": "reference", "metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
                 "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(steps, 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": WORKLOAD, "sample_electrons": args.cpu_electrons},
+                "data": "synthetic",
+                "config": {"workload": window_label(S0, steps), "sample_electrons": args.cpu_electrons,
+                           "start_step": S0, "steps_timed": steps},
                 "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                                  "sample": sample},
                 "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -773,12 +845,14 @@ def main():
 
     # CPU baseline first (rank 0, N=1), before any CUDA context exists
     cpu = None
+    S0 = window_start(args)
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, STEPS_FULL, args.cpu_budget, 1)
+        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, S0, args.steps, args.cpu_budget)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": omp_threads(), "kind": "port",
-               "sample": f"{args.cpu_electrons} e- of the same cascade (1/{args.electrons // args.cpu_electrons} of "
-                         f"the beam), first {steps} steps, "
-                         f"{ps:.3g} particle-steps in {dt:.1f}s"}
+               "sample": f"{args.cpu_electrons} e- of the same beam (1/{args.electrons // args.cpu_electrons} of "
+                         f"it), advanced untimed to step {max(S0, 1)}, then steps {max(S0, 1)}-{max(S0, 1) + steps} "
+                         f"timed: {ps:.3g} particle-steps in {dt:.2f}s",
+               "start_step": max(S0, 1), "steps_timed": steps}
 
     r = run_ours(args, rank, world)
     if rank == 0:
@@ -787,11 +861,13 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "electrons_per_gpu": args.electrons, "form": args.form,
+                "config": {"workload": window_label(r["start_step"], args.steps), "electrons_per_gpu": args.electrons,
+                           "form": args.form, "start_step": r["start_step"], "steps_timed": args.steps,
                            "l2": "state > 1 GB per step, larger than L2 (no flush needed)",
-                           "final_counts": r["counts"]},
+                           "counts_at_window_start": r["start_counts"], "counts_at_window_end": r["counts"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
-                "clocks": r["clocks"], "particle_steps": r["particle_steps"], "vs_fp64": r["compare"]}
+                "clocks": r["clocks"], "particle_steps": r["particle_steps"], "whole_run": r["whole"],
+                "vs_fp64": r["compare"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

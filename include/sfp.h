@@ -151,7 +151,7 @@ typedef struct sfp_run_config {
     int64_t step0;           /* steps already taken (Philox step key)     */
     int32_t qed;             /* SFP_QED_*                                  */
     int32_t form;            /* SFP_FORM_*                                 */
-    int32_t items;           /* massive kernel: particles per thread per tile (0 = default) */
+    int32_t m_stages;        /* massive kernel: depth of the copy ring, 2..4 (0 = default)  */
     int32_t min_blocks;      /* massive kernel: min resident blocks per SM (0 = default)    */
     int32_t p_stages;        /* photon kernel: depth of the copy ring, 2..4 (0 = default)   */
     int32_t p_min_blocks;    /* photon kernel: min resident blocks per SM (0 = default)     */
@@ -169,28 +169,27 @@ int sfp_run_create(sfp_module *m, const sfp_run_config *cfg, int n_inst, const s
 int sfp_run_update(sfp_run *r, int n_seg, const sfp_segment *seg, const int64_t *n_buffered);
 /* advance up to nsteps steps; graph_chunk > 0 replays CUDA graphs of that
  * many steps.  Asynchronous on `stream`.  The run stops early with halted=1
- * (a) before a step when a photon destination lacks room for every emitter
- * emitting -- grow it (the reference's _extend rule), sfp_run_update,
- * sfp_run_clear_halt -- or (b) inside a step, after its pair events are
- * counted, when an e-/e+ destination lacks room for them (pairs_pending=1):
- * grow every segment to sfp_run_pending_need, sfp_run_update with NULL
- * counts, then sfp_run_resume to finish that step. */
+ * inside a step, once its photon and pair events are counted, when a
+ * destination lacks room for that step's children (appends_pending=1): grow
+ * every segment to sfp_run_pending_need (the reference's _extend rule),
+ * sfp_run_update with NULL counts, then sfp_run_resume to finish that step.
+ * The steps queued behind it do nothing. */
 int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
-/* like sfp_run_steps without graphs, with CUDA events recorded around each
- * of the three kernels of every step on the run's stream; synchronous.
+/* like sfp_run_steps without graphs, with CUDA events recorded around the
+ * kernels of every step on the run's stream; synchronous.
  * kernel_ms[3*i + k] is the duration of step i's massive (k=0) and photon
- * (k=1) kernels and of its pair scan + pairs kernels (k=2); 0 for kernels
- * the run does not launch (3*nsteps entries). */
+ * (k=1) kernels and of its scan + appends kernels (k=2); 0 for kernels the
+ * run does not launch (3*nsteps entries). */
 int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stream);
 /* synchronous: state and per-segment buffered counts (n_seg entries) */
 int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);
-/* clear the halted flag after the caller made room */
+/* clear a halted flag that no stopped step holds */
 int sfp_run_clear_halt(sfp_run *r, void *stream);
-/* synchronous: while pairs_pending, the buffer size each segment needs to
+/* synchronous: while appends_pending, the buffer size each segment needs to
  * finish the stopped step (n_seg entries); otherwise its buffered count */
 int sfp_run_pending_need(sfp_run *r, int64_t *need);
-/* finish a step stopped with pairs_pending: write and push its pairs, fold
- * its appends and advance t / step.  Asynchronous on the run's stream. */
+/* finish a step stopped with appends_pending: write and push its children,
+ * fold its appends and advance t / step.  Asynchronous on the run's stream. */
 int sfp_run_resume(sfp_run *r, void *stream);
 int sfp_run_destroy(sfp_run *r);
 

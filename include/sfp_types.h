@@ -53,8 +53,9 @@ typedef struct sfp_segment {
     double *x, *y, *z, *ux, *uy, *uz;
     double *sx, *sy, *sz; /* NULL unless spin (SpinParticles)              */
     double *tau;          /* NULL unless the optical-depth method is used  */
-    double *delta;        /* pair-creating photons: pair_delta, the delta of
-                             this step's pair events (NULL otherwise)       */
+    double *delta;        /* the delta of this step's events: photon_delta
+                             of a radiating species, pair_delta of a
+                             pair-creating one (NULL otherwise)             */
     sfp_u8 *pruned;       /* _to_be_pruned                                 */
     sfp_i64 capacity;     /* buffer_size                                   */
     double q;             /* charge [C]                                    */
@@ -111,7 +112,8 @@ typedef struct sfp_run_state {
     sfp_i32 halted;         /* 1: the run stopped for lack of capacity      */
     sfp_i32 error;          /* device error code (0 = none)                 */
     sfp_i64 particle_steps; /* sum over executed steps of all N_buffered    */
-    sfp_i32 pairs_pending;  /* 1: a step stopped before writing its pairs:
+    sfp_i32 appends_pending; /* 1: a step stopped before writing its
+                               children (photons or pairs) for lack of room:
                                grow to sfp_run_pending_need, then
                                sfp_run_resume                               */
     sfp_i32 pad;
@@ -121,7 +123,6 @@ typedef struct sfp_run_state {
 
 /* device error codes */
 #define SFP_DEV_OK 0
-#define SFP_DEV_LOOKBACK_TIMEOUT 1
-#define SFP_DEV_CAPACITY 2
+#define SFP_DEV_CAPACITY 2 /* more tiles than the run's counters hold */
 
 #endif

@@ -53,12 +53,12 @@ class RSTable(ctypes.Structure):
 
 class RunState(ctypes.Structure):
     _fields_ = [("t", c_d), ("step", c_i64), ("halted", c_i32), ("error", c_i32), ("particle_steps", c_i64),
-                ("pairs_pending", c_i32), ("pad", c_i32)]
+                ("appends_pending", c_i32), ("pad", c_i32)]
 
 
 class RunConfig(ctypes.Structure):
     _fields_ = [("dt", c_d), ("photon_threshold", c_d), ("t0", c_d), ("step0", c_i64), ("qed", c_i32), ("form", c_i32),
-                ("items", c_i32), ("min_blocks", c_i32), ("p_stages", c_i32), ("p_min_blocks", c_i32), ("mlp_params", P),
+                ("m_stages", c_i32), ("min_blocks", c_i32), ("p_stages", c_i32), ("p_min_blocks", c_i32), ("mlp_params", P),
                 ("rs", RSTable), ("od_photon", ODTable),
                 ("od_pair", ODTable)]
 
@@ -66,7 +66,7 @@ class RunConfig(ctypes.Structure):
 SFP_QED_REJECTION, SFP_QED_OPTICAL_DEPTH = 0, 1
 SFP_FORM_FP64, SFP_FORM_FP32 = 0, 1
 SFP_FIELD_PARAMS = 16
-DEV_ERRORS = {1: "look-back wait timed out", 2: "tile table too small"}
+DEV_ERRORS = {2: "tile table too small"}
 
 _SIGS = {
     "sfp_version": ([], ctypes.c_char_p),

@@ -1,12 +1,11 @@
 """Autotuner of the step kernels.
 
 Every NVRTC step module holds several variants of the two persistent step
-kernels:
+kernels, both over warp tiles of 1024 particles streamed through a
+``stages``-deep ring of asynchronous copies:
 
-* ``sfp_massive_<form>_<qed>_i<items>_b<blocks>`` -- e+- tiles of
-  256 * ``items`` particles (``items`` particles per thread);
-* ``sfp_photon_<form>_<qed>_s<stages>_b<blocks>`` -- warp tiles of 1024
-  photons streamed through a ``stages``-deep ring of asynchronous copies;
+* ``sfp_massive_<form>_<qed>_s<stages>_b<blocks>`` -- e+- tiles;
+* ``sfp_photon_<form>_<qed>_s<stages>_b<blocks>`` -- photon tiles;
 
 ``blocks`` is the register budget: at least that many blocks of 256 threads
 stay resident per SM.  Which variant is fastest depends on the particle mix,
@@ -30,19 +29,19 @@ import numpy as np
 
 from . import program
 
-# (massive variants (items, blocks), photon variants (stages, blocks)); the
+# (massive variants (stages, blocks), photon variants (stages, blocks)); the
 # NVRTC step module compiles exactly these
 VARIANTS = {
-    ("fp64", "rs"): ([(1, 2), (2, 2)], [(3, 3), (2, 3), (3, 2)]),
-    ("fp64", "od"): ([(1, 2), (2, 2)], [(3, 3), (2, 3)]),
-    ("fp32", "rs"): ([(1, 3), (1, 4), (2, 2), (2, 3)], [(3, 4), (2, 4), (3, 3), (4, 3)]),
-    ("fp32", "od"): ([(1, 3), (2, 2)], [(3, 4), (3, 3)]),
+    ("fp64", "rs"): ([(2, 2), (3, 2)], [(3, 3), (2, 3), (3, 2)]),
+    ("fp64", "od"): ([(2, 2), (3, 2)], [(3, 3), (2, 3)]),
+    ("fp32", "rs"): ([(2, 3), (3, 3), (3, 2), (4, 2)], [(3, 4), (2, 4), (3, 3), (4, 3)]),
+    ("fp32", "od"): ([(2, 3), (3, 2)], [(3, 4), (3, 3)]),
 }
 DEFAULT = {
-    ("fp64", "rs"): ((1, 2), (3, 3)),
-    ("fp64", "od"): ((1, 2), (3, 3)),
-    ("fp32", "rs"): ((2, 3), (3, 4)),
-    ("fp32", "od"): ((2, 2), (3, 3)),
+    ("fp64", "rs"): ((2, 2), (3, 3)),
+    ("fp64", "od"): ((2, 2), (3, 3)),
+    ("fp32", "rs"): ((3, 3), (3, 4)),
+    ("fp32", "od"): ((2, 3), (3, 3)),
 }
 
 _lock = threading.Lock()
@@ -117,7 +116,7 @@ def measure(sim, variants=None, steps: int = 3):
     (len(massive) + len(photon)) * steps steps."""
     mv, pv = variants or VARIANTS[(sim.form, sim.qed_method)]
     tm, tp = {}, {}
-    m0, p0 = (sim.items, sim.min_blocks), (sim.p_stages, sim.p_min_blocks)
+    m0, p0 = (sim.m_stages, sim.min_blocks), (sim.p_stages, sim.p_min_blocks)
     for v in mv:
         sim.set_kernel(massive=v, photon=p0)
         ms, _, _ = sim.time_step_kernel(steps)
@@ -132,7 +131,7 @@ def measure(sim, variants=None, steps: int = 3):
 def tune(sim, sample: int = 2_000_000, steps: int = 3, use_cache: bool = True):
     """Select the fastest massive- and photon-kernel variants for `sim` (see
     the module doc).  Returns ((massive, photon), times), times a dict
-    'm<items>_b<blocks>' / 'p<stages>_b<blocks>' -> ms."""
+    'm<stages>_b<blocks>' / 'p<stages>_b<blocks>' -> ms."""
     key = cache_key(sim)
     with _lock:
         cache = _load() if use_cache else {}
@@ -146,7 +145,7 @@ def tune(sim, sample: int = 2_000_000, steps: int = 3, use_cache: bool = True):
     finally:
         s.finish()
     # a kernel with no work (0 ms everywhere) keeps the default
-    m = min(tm, key=tm.get) if any(tm.values()) else (sim.items, sim.min_blocks)
+    m = min(tm, key=tm.get) if any(tm.values()) else (sim.m_stages, sim.min_blocks)
     p = min(tp, key=tp.get) if any(tp.values()) else (sim.p_stages, sim.p_min_blocks)
     sim.set_kernel(massive=m, photon=p)
     times = {**{f"m{a}_b{b}": v for (a, b), v in tm.items()}, **{f"p{a}_b{b}": v for (a, b), v in tp.items()}}

@@ -4,10 +4,10 @@
 //     (the plugin boundary, sfparticles/particles.py:14-25);
 //   * NVRTC compilation / loading of field-specialised step modules;
 //   * step runs: device bookkeeping, persistent launches of the massive /
-//     photon / pair-children kernels, CUDA graphs.
+//     photon / scan / appends kernels, CUDA graphs.
 //
 // Device memory of particle buffers belongs to the caller; a run allocates
-// only its own bookkeeping (segment tables, tile look-back flags, counters).
+// only its own bookkeeping (segment tables, tile maps, event counters).
 #include <cuda_runtime.h>
 #include <nvrtc.h>
 
@@ -718,20 +718,26 @@ int sfp_inv_gamma(const double* ux, const double* uy, const double* uz, double* 
 
 // ================================ runs =======================================
 //
-// One step = book(prepare) + massive + photon [+ pair scan + pairs] launches
-// on the run's stream.  The massive and photon kernels are persistent grids
-// that take tiles by ticket; the pair scan is one block; the pairs kernel is
-// a grid over the photon-tile counters.
+// One step = book(prepare) + massive + photon [+ scan + appends] launches on
+// the run's stream.  The massive and photon kernels are persistent grids that
+// take warp tiles by ticket; the scan is one block; the appends kernel is a
+// grid over both groups' tile counters.
 
-// photon (warp) tile: SFP_PHOTON_WSUB_HOST sub-steps of 32 photons; the NVRTC
-// modules are built with SFP_PHOTON_WSUB equal to it
-#define SFP_PHOTON_WSUB_HOST 32
+// warp tile of both groups: SFP_WSUB_HOST sub-steps of 32 particles; the
+// NVRTC modules are built with SFP_WSUB equal to it
+#define SFP_WSUB_HOST 32
 #define SFP_SUPER_TILE_HOST 64
+
+struct sfp_group_host {
+    std::vector<int> seg;
+    int* d_seg = nullptr;
+    long long* d_start = nullptr;
+};
 
 struct sfp_run {
     sfp_module* mod = nullptr;
-    cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_pairs = nullptr, k_book = nullptr;
-    int grid_m = 0, grid_p = 0, grid_c = 0;
+    cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_appends = nullptr, k_book = nullptr;
+    int grid_m = 0, grid_p = 0, grid_a = 0;
     size_t smem_m = 0, smem_p = 0;
     cudaStream_t s = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -741,69 +747,55 @@ struct sfp_run {
     std::map<int, cudaGraphExec_t> graphs;
     std::vector<sfp_segment> segs;
     std::vector<sfp_instance> insts;
-    std::vector<int> mseg, pseg, cseg;
+    sfp_group_host mg, pg;
+    std::vector<int> dseg;
 };
 
-// massive tiles (look-back flags) and photon tiles (event counters) at full
-// capacity, plus slack; photon segments start at multiples of a super-tile
-static long long mtiles_for(const sfp_run* r) {
+// tiles of a group at full capacity: each segment's tiles plus the padding
+// up to the next multiple of a super-tile
+static long long tiles_for(const sfp_run* r, const std::vector<int>& segs) {
     long long t = 0;
-    for (int s : r->mseg) t += (r->segs[s].capacity + r->h.mtile - 1) / r->h.mtile;
-    return t + (long long)r->segs.size() + 1;
-}
-static long long ptiles_for(const sfp_run* r) {
-    long long t = 0;
-    for (int s : r->pseg) t += (r->segs[s].capacity + r->h.ptile - 1) / r->h.ptile + SFP_SUPER_TILE_HOST;
+    for (int s : segs) t += (r->segs[s].capacity + r->h.tile - 1) / r->h.tile + SFP_SUPER_TILE_HOST;
     return t + 1;
 }
 
-static int run_alloc_tiles(sfp_run* r) {
-    const long long need_m = mtiles_for(r), need_p = ptiles_for(r);
-    if (need_m > r->h.max_tiles) {
-        const long long n = need_m + need_m / 4 + 64;
-        if (r->h.tile_flag) cudaFree(r->h.tile_flag);
-        if (r->h.tile_agg) cudaFree(r->h.tile_agg);
-        if (r->h.tile_incl) cudaFree(r->h.tile_incl);
-        r->h.tile_flag = nullptr;
-        r->h.tile_agg = r->h.tile_incl = nullptr;
-        r->h.max_tiles = 0;
-        SFP_CUDA(cudaMalloc(&r->h.tile_flag, n * sizeof(unsigned int)));
-        SFP_CUDA(cudaMalloc(&r->h.tile_agg, n * sizeof(uint4)));
-        SFP_CUDA(cudaMalloc(&r->h.tile_incl, n * sizeof(uint4)));
-        SFP_CUDA(cudaMemsetAsync(r->h.tile_flag, 0, n * sizeof(unsigned int), r->s));
-        r->h.max_tiles = n;
+// (re)allocate a group's tile counters for the current capacities; a step
+// stopped for room keeps its counters through a reallocation
+static int group_alloc(sfp_run* r, sfp_group_dev& G, long long need) {
+    if (need <= G.max_tiles) return SFP_OK;
+    const long long n = need + need / 4 + 64;
+    const long long ns = n / SFP_SUPER_TILE_HOST + 2;
+    const long long n_old = G.max_tiles, ns_old = n_old ? n_old / SFP_SUPER_TILE_HOST + 2 : 0;
+    unsigned int *cnt = nullptr, *scnt = nullptr;
+    long long* spre = nullptr;
+    if (cudaMalloc(&cnt, n * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc(&scnt, ns * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc(&spre, ns * sizeof(long long)) != cudaSuccess) {
+        cudaFree(cnt);
+        cudaFree(scnt);
+        cudaFree(spre);
+        return fail(SFP_ENOMEM, "cudaMalloc of the tile counters");
     }
-    if (need_p > r->h.max_ptiles) {
-        // grown between steps, or while a stopped step waits for its pairs:
-        // the counters of that step are carried over
-        const long long n = need_p + need_p / 4 + 64;
-        const long long ns = n / SFP_SUPER_TILE_HOST + 2;
-        const long long n_old = r->h.max_ptiles, ns_old = n_old ? n_old / SFP_SUPER_TILE_HOST + 2 : 0;
-        unsigned int *cnt = nullptr, *scnt = nullptr;
-        long long* spre = nullptr;
-        if (cudaMalloc(&cnt, n * sizeof(unsigned int)) != cudaSuccess ||
-            cudaMalloc(&scnt, ns * sizeof(unsigned int)) != cudaSuccess ||
-            cudaMalloc(&spre, ns * sizeof(long long)) != cudaSuccess) {
-            cudaFree(cnt);
-            cudaFree(scnt);
-            cudaFree(spre);
-            return fail(SFP_ENOMEM, "cudaMalloc of the photon-tile counters");
-        }
-        if (n_old) {
-            SFP_CUDA(cudaMemcpyAsync(cnt, r->h.ptile_cnt, n_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
-            SFP_CUDA(cudaMemcpyAsync(scnt, r->h.psuper_cnt, ns_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
-            SFP_CUDA(cudaMemcpyAsync(spre, r->h.psuper_pre, ns_old * sizeof(long long), cudaMemcpyDeviceToDevice, r->s));
-            SFP_CUDA(cudaStreamSynchronize(r->s));
-        }
-        cudaFree(r->h.ptile_cnt);
-        cudaFree(r->h.psuper_cnt);
-        cudaFree(r->h.psuper_pre);
-        r->h.ptile_cnt = cnt;
-        r->h.psuper_cnt = scnt;
-        r->h.psuper_pre = spre;
-        r->h.max_ptiles = n;
+    if (n_old) {
+        SFP_CUDA(cudaMemcpyAsync(cnt, G.tile_cnt, n_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
+        SFP_CUDA(cudaMemcpyAsync(scnt, G.super_cnt, ns_old * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
+        SFP_CUDA(cudaMemcpyAsync(spre, G.super_pre, ns_old * sizeof(long long), cudaMemcpyDeviceToDevice, r->s));
+        SFP_CUDA(cudaStreamSynchronize(r->s));
     }
+    cudaFree(G.tile_cnt);
+    cudaFree(G.super_cnt);
+    cudaFree(G.super_pre);
+    G.tile_cnt = cnt;
+    G.super_cnt = scnt;
+    G.super_pre = spre;
+    G.max_tiles = n;
     return SFP_OK;
+}
+
+static int run_alloc_tiles(sfp_run* r) {
+    int rc = group_alloc(r, r->h.mg, tiles_for(r, r->mg.seg));
+    if (rc) return rc;
+    return group_alloc(r, r->h.pg, tiles_for(r, r->pg.seg));
 }
 
 static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, const sfp_segment* seg) {
@@ -818,25 +810,27 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
     if (expect != n_seg) return fail(SFP_EINVAL, "instances do not cover all segments");
     for (int s = 0; s < n_seg; ++s) {
         const sfp_segment& S = seg[s];
-        if (S.capacity < 0) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": negative capacity");
+        const std::string name = "segment " + std::to_string(s);
+        if (S.capacity < 0) return fail(SFP_EINVAL, name + ": negative capacity");
         // an empty buffer (capacity 0) may have NULL arrays: nothing reads or writes it
         if (S.capacity > 0 && (!S.x || !S.y || !S.z || !S.ux || !S.uy || !S.uz || !S.pruned))
-            return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": NULL state pointer");
+            return fail(SFP_EINVAL, name + ": NULL state pointer");
         if (S.capacity > 0 && S.spin && (!S.sx || !S.sy || !S.sz))
             return fail(SFP_EINVAL, "spin segment without spin arrays");
         if (S.channel < 0 || S.channel >= SFP_MAX_CHANNELS) return fail(SFP_EINVAL, "append channel out of range");
-        // the photon kernel streams photon state with 16-byte asynchronous copies
-        if (S.massless && S.capacity > 0) {
-            const void* a[] = {S.x, S.y, S.z, S.ux, S.uy, S.uz, S.pruned, S.tau};
+        // both group kernels stream the state with 16-byte asynchronous copies,
+        // and the appends kernel reads the flags 16 at a time
+        if (S.capacity > 0) {
+            const void* a[] = {S.x, S.y, S.z, S.ux, S.uy, S.uz, S.pruned, S.tau, S.sx, S.sy, S.sz};
             for (const void* p : a)
                 if (p && (reinterpret_cast<uintptr_t>(p) & 15u))
-                    return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": photon arrays must be 16-byte aligned");
-            if (S.bw && !S.delta)
-                return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": pair-creating photons need a delta array");
+                    return fail(SFP_EINVAL, name + ": state arrays must be 16-byte aligned");
+            if ((S.bw || S.radiating) && !S.delta)
+                return fail(SFP_EINVAL, name + ": a segment with events needs a delta array");
         }
         // the massive kernel handles emission, the photon kernel pair creation
-        if (S.massless && S.radiating) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": a photon cannot radiate");
-        if (!S.massless && S.bw) return fail(SFP_EINVAL, "segment " + std::to_string(s) + ": only photons create pairs");
+        if (S.massless && S.radiating) return fail(SFP_EINVAL, name + ": a photon cannot radiate");
+        if (!S.massless && S.bw) return fail(SFP_EINVAL, name + ": only photons create pairs");
         const sfp_instance& I = inst[S.instance];
         auto in_inst = [&](int d) { return d >= I.first_seg && d < I.first_seg + I.n_seg; };
         if (S.radiating && (!in_inst(S.photon_dest) || !seg[S.photon_dest].massless))
@@ -860,7 +854,6 @@ static int run_upload(sfp_run* r, const sfp_instance* inst, const int64_t* n_buf
     return SFP_OK;
 }
 
-// persistent grid of one kernel: resident blocks per SM x SMs
 // the kernel's dynamic shared memory limit, raised to at least `need` bytes
 static cudaError_t raise_dynamic_smem(const void* k, size_t need) {
     cudaFuncAttributes fa;
@@ -870,6 +863,7 @@ static cudaError_t raise_dynamic_smem(const void* k, size_t need) {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
 }
 
+// persistent grid of one kernel: resident blocks per SM x SMs
 static int persistent_grid(cudaKernel_t k, size_t smem, int fallback_per_sm) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, SFP_TILE_HOST, smem) != cudaSuccess ||
@@ -893,11 +887,11 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if (cfg->mlp_params && cfg->qed != SFP_QED_OPTICAL_DEPTH)
         return fail(SFP_EINVAL, "the learned photon-energy sampler serves the optical-depth method only");
     const bool f64 = cfg->form == SFP_FORM_FP64;
-    const int items = cfg->items > 0 ? cfg->items : (f64 ? 1 : 1);
+    const int mstages = cfg->m_stages > 0 ? cfg->m_stages : (f64 ? 2 : 3);
     const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : (f64 ? 2 : 3);
     const int stages = cfg->p_stages > 0 ? cfg->p_stages : 3;
     const int pminb = cfg->p_min_blocks > 0 ? cfg->p_min_blocks : (f64 ? 3 : 4);
-    if (items < 1 || items > 4 || minb < 1 || minb > 8 || stages < 2 || stages > 4 || pminb < 1 || pminb > 8)
+    if (mstages < 2 || mstages > 4 || minb < 1 || minb > 8 || stages < 2 || stages > 4 || pminb < 1 || pminb > 8)
         return fail(SFP_EINVAL, "kernel variant out of range");
     auto* r = new sfp_run();
     r->mod = m;
@@ -905,20 +899,24 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     r->n_inst = n_inst;
     r->segs.assign(seg, seg + n_seg);
     r->insts.assign(inst, inst + n_inst);
+    bool any_spin = false;
     for (int s = 0; s < n_seg; ++s) {
-        (seg[s].massless ? r->pseg : r->mseg).push_back(s);
+        (seg[s].massless ? r->pg.seg : r->mg.seg).push_back(s);
+        if (!seg[s].massless && seg[s].spin) any_spin = true;
         bool dest = false;
         for (int q = 0; q < n_seg; ++q)
-            if (seg[q].bw && (seg[q].ele_dest == s || seg[q].pos_dest == s)) dest = true;
-        if (dest) r->cseg.push_back(s);
+            if ((seg[q].bw && (seg[q].ele_dest == s || seg[q].pos_dest == s)) ||
+                (seg[q].radiating && seg[q].photon_dest == s))
+                dest = true;
+        if (dest) r->dseg.push_back(s);
     }
     const std::string fq = std::string(f64 ? "fp64_" : "fp32_") + (cfg->qed == SFP_QED_REJECTION ? "rs" : "od");
-    const std::string km = "sfp_massive_" + fq + "_i" + std::to_string(items) + "_b" + std::to_string(minb);
+    const std::string km = "sfp_massive_" + fq + "_s" + std::to_string(mstages) + "_b" + std::to_string(minb);
     const std::string kp = "sfp_photon_" + fq + "_s" + std::to_string(stages) + "_b" + std::to_string(pminb);
-    const std::string kc = f64 ? "sfp_pairs_fp64" : "sfp_pairs_fp32";
+    const std::string ka = f64 ? "sfp_appends_fp64" : "sfp_appends_fp32";
     if ((rc = module_kernel(m, km.c_str(), &r->k_massive)) || (rc = module_kernel(m, kp.c_str(), &r->k_photon)) ||
-        (rc = module_kernel(m, kc.c_str(), &r->k_pairs)) ||
-        (rc = module_kernel(m, "sfp_pair_scan_kernel", &r->k_scan)) ||
+        (rc = module_kernel(m, ka.c_str(), &r->k_appends)) ||
+        (rc = module_kernel(m, "sfp_scan_kernel", &r->k_scan)) ||
         (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
         delete r;
         return rc;
@@ -937,13 +935,15 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     h.dt = cfg->dt;
     h.photon_threshold = cfg->photon_threshold;
     h.qed = cfg->qed;
-    h.mtile = SFP_TILE_HOST * items;
-    h.ptile = 32 * SFP_PHOTON_WSUB_HOST;
-    h.any_appends = 0;
-    for (int s = 0; s < n_seg; ++s) h.any_appends |= seg[s].radiating ? 1 : 0;
-    h.n_mseg = (int)r->mseg.size();
-    h.n_pseg = (int)r->pseg.size();
-    h.n_cseg = (int)r->cseg.size();
+    h.tile = 32 * SFP_WSUB_HOST;
+    h.any_rad = h.any_bw = 0;
+    for (int s = 0; s < n_seg; ++s) {
+        h.any_rad |= seg[s].radiating ? 1 : 0;
+        h.any_bw |= seg[s].bw ? 1 : 0;
+    }
+    h.n_dseg = (int)r->dseg.size();
+    h.mg.n_seg = (int)r->mg.seg.size();
+    h.pg.n_seg = (int)r->pg.seg.size();
     h.rs = cfg->rs;
     h.od_photon = cfg->od_photon;
     h.od_pair = cfg->od_pair;
@@ -951,34 +951,36 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) return cleanup(fail(SFP_ENOMEM, "cudaMalloc " #ptr))
     sfp_segment* dseg;
     sfp_instance* dinst;
-    int *dm, *dp, *dc;
+    int* dd;
     ALLOC(dseg, n_seg * sizeof(sfp_segment));
     ALLOC(dinst, n_inst * sizeof(sfp_instance));
     h.seg = dseg;
     h.inst = dinst;
-    ALLOC(dm, (r->mseg.size() + 1) * sizeof(int));
-    ALLOC(dp, (r->pseg.size() + 1) * sizeof(int));
-    ALLOC(dc, (r->cseg.size() + 1) * sizeof(int));
-    h.mseg = dm;
-    h.pseg = dp;
-    h.cseg = dc;
+    ALLOC(r->mg.d_seg, (r->mg.seg.size() + 1) * sizeof(int));
+    ALLOC(r->pg.d_seg, (r->pg.seg.size() + 1) * sizeof(int));
+    ALLOC(dd, (r->dseg.size() + 1) * sizeof(int));
+    ALLOC(r->mg.d_start, (r->mg.seg.size() + 1) * sizeof(long long));
+    ALLOC(r->pg.d_start, (r->pg.seg.size() + 1) * sizeof(long long));
+    h.mg.seg = r->mg.d_seg;
+    h.pg.seg = r->pg.d_seg;
+    h.mg.tile_start = r->mg.d_start;
+    h.pg.tile_start = r->pg.d_start;
+    h.dseg = dd;
     ALLOC(h.n_buffered, n_seg * sizeof(long long));
     ALLOC(h.appended, n_seg * sizeof(unsigned long long));
     ALLOC(h.n_buf_step, n_seg * sizeof(long long));
-    ALLOC(h.mtile_start, (r->mseg.size() + 1) * sizeof(long long));
-    ALLOC(h.ptile_start, (r->pseg.size() + 1) * sizeof(long long));
-    ALLOC(h.chain_first, n_seg * sizeof(long long));
     ALLOC(h.st, sizeof(sfp_step_state));
     ALLOC(r->d, sizeof(sfp_run_dev));
 #undef ALLOC
-    if ((!r->mseg.empty() &&
-         cudaMemcpyAsync(dm, r->mseg.data(), r->mseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
-        (!r->pseg.empty() &&
-         cudaMemcpyAsync(dp, r->pseg.data(), r->pseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
-        (!r->cseg.empty() &&
-         cudaMemcpyAsync(dc, r->cseg.data(), r->cseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
-        cudaMemsetAsync(h.appended, 0, n_seg * sizeof(unsigned long long), r->s) != cudaSuccess ||
-        cudaMemsetAsync(h.chain_first, 0, n_seg * sizeof(long long), r->s) != cudaSuccess)
+    if ((!r->mg.seg.empty() && cudaMemcpyAsync(r->mg.d_seg, r->mg.seg.data(), r->mg.seg.size() * sizeof(int),
+                                               cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        (!r->pg.seg.empty() && cudaMemcpyAsync(r->pg.d_seg, r->pg.seg.data(), r->pg.seg.size() * sizeof(int),
+                                               cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        (!r->dseg.empty() &&
+         cudaMemcpyAsync(dd, r->dseg.data(), r->dseg.size() * sizeof(int), cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
+        cudaMemsetAsync(r->mg.d_start, 0, (r->mg.seg.size() + 1) * sizeof(long long), r->s) != cudaSuccess ||
+        cudaMemsetAsync(r->pg.d_start, 0, (r->pg.seg.size() + 1) * sizeof(long long), r->s) != cudaSuccess ||
+        cudaMemsetAsync(h.appended, 0, n_seg * sizeof(unsigned long long), r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "segment lists upload"));
     sfp_step_state st0{};
     st0.t = cfg->t0;
@@ -986,32 +988,38 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     st0.skip = 1;
     if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "state upload"));
-    // shared memory: the QED tables (both kernels), then the photon kernel's
-    // copy ring of `stages` stages per warp (photon state + flags)
+    // shared memory: the QED tables (both kernels); the massive kernel then
+    // the learned sampler's weights (when used) and its copy ring, the photon
+    // kernel its copy ring; rings of `stages` stages per warp
     size_t tab;
     if (cfg->qed == SFP_QED_REJECTION)
         tab = 2 * (size_t)cfg->rs.z_N * (f64 ? sizeof(double) : sizeof(float));
     else
         tab = ((size_t)cfg->od_photon.chi_N + (size_t)cfg->od_pair.chi_N) * sizeof(double);
-    const size_t nc = cfg->qed == SFP_QED_OPTICAL_DEPTH ? 7 : 6;
+    const int od = cfg->qed == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    const size_t warps = SFP_TILE_HOST / 32;
     h.mlp_params = cfg->mlp_params;
     h.mlp_off = (int)((tab + 127) / 128 * 128);
-    r->smem_m = cfg->mlp_params ? (size_t)h.mlp_off + sizeof(sfp_mlp::Smem) : tab;
+    const size_t m_head = cfg->mlp_params ? (size_t)h.mlp_off + sizeof(sfp_mlp::Smem) : tab;
+    h.m_stage_bytes = (6 + od + (any_spin ? 3 : 0)) * 256 + 32;
+    h.m_ring_off = (int)((m_head + 127) / 128 * 128);
+    r->smem_m = (size_t)h.m_ring_off + warps * mstages * (size_t)h.m_stage_bytes;
     h.ring_off = (int)((tab + 127) / 128 * 128);
-    r->smem_p = (size_t)h.ring_off + (size_t)(SFP_TILE_HOST / 32) * stages * (nc * 32 * 8 + 32);
+    r->smem_p = (size_t)h.ring_off + warps * stages * ((6 + od) * 256 + 32);
     if ((rc = run_alloc_tiles(r))) return cleanup(rc);
     if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
     const size_t cap = 200 * 1024;
-    if (r->smem_m > cap || r->smem_p > cap) return cleanup(fail(SFP_EINVAL, "QED tables too large for shared memory"));
+    if (r->smem_m > cap || r->smem_p > cap)
+        return cleanup(fail(SFP_EINVAL, "QED tables and copy rings too large for shared memory"));
     // always raised, never lowered: the kernels' static shared memory counts
     // toward the 48 KB a launch gets without it, and runs that share a module
-    // (with and without the learned sampler) need different amounts
+    // need different amounts
     if (raise_dynamic_smem((const void*)r->k_massive, r->smem_m) != cudaSuccess ||
         raise_dynamic_smem((const void*)r->k_photon, r->smem_p) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory"));
     r->grid_m = persistent_grid(r->k_massive, r->smem_m, minb);
     r->grid_p = persistent_grid(r->k_photon, r->smem_p, pminb);
-    r->grid_c = persistent_grid(r->k_pairs, 0, 2);
+    r->grid_a = persistent_grid(r->k_appends, 0, 2);
     *out = r;
     return SFP_OK;
 }
@@ -1022,7 +1030,8 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
     for (int s = 0; s < n_seg; ++s)
         if (seg[s].massless != r->segs[s].massless || seg[s].radiating != r->segs[s].radiating ||
             seg[s].bw != r->segs[s].bw || seg[s].ele_dest != r->segs[s].ele_dest ||
-            seg[s].pos_dest != r->segs[s].pos_dest)
+            seg[s].pos_dest != r->segs[s].pos_dest || seg[s].photon_dest != r->segs[s].photon_dest ||
+            (!seg[s].massless && seg[s].spin != r->segs[s].spin))
             return fail(SFP_EINVAL, "sfp_run_update: segment roles changed");
     int rc = validate_segments(r->n_inst, r->insts.data(), n_seg, seg);
     if (rc) return rc;
@@ -1032,25 +1041,25 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
     return run_upload(r, nullptr, n_buffered);
 }
 
-// one step: book(prepare), massive, photon, pair scan + pairs; ev (6
-// events) brackets the massive, the photon and the two pair kernels when given
+// one step: book(prepare), massive, photon, scan + appends; ev (6 events)
+// brackets the massive, the photon and the scan + appends kernels when given
 static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev) {
     int prep = 1;
     void* a_book[] = {&r->d, &prep};
     void* a[] = {&r->d};
     SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[0], s));
-    if (!r->mseg.empty())
+    if (!r->mg.seg.empty())
         SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem_m, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[1], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[2], s));
-    if (!r->pseg.empty())
+    if (!r->pg.seg.empty())
         SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem_p, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[3], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[4], s));
-    if (!r->cseg.empty()) {
+    if (!r->dseg.empty()) {
         SFP_CUDA(cudaLaunchKernel((const void*)r->k_scan, dim3(1), dim3(1024), a, 0, s));
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_pairs, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, s));
+        SFP_CUDA(cudaLaunchKernel((const void*)r->k_appends, dim3(r->grid_a), dim3(SFP_TILE_HOST), a, 0, s));
     }
     if (ev) SFP_CUDA(cudaEventRecord(ev[5], s));
     return SFP_OK;
@@ -1112,7 +1121,7 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, &ev[6 * k]);
     if (rc == SFP_OK) rc = launch_fold(r);
     if (rc == SFP_OK && cudaStreamSynchronize(r->s) != cudaSuccess) rc = fail(SFP_ECUDA, "synchronize");
-    const bool has[3] = {!r->mseg.empty(), !r->pseg.empty(), !r->cseg.empty()};
+    const bool has[3] = {!r->mg.seg.empty(), !r->pg.seg.empty(), !r->dseg.empty()};
     for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k)
         for (int j = 0; j < 3 && rc == SFP_OK; ++j) {
             kernel_ms[3 * k + j] = 0.0f;
@@ -1141,7 +1150,7 @@ int sfp_run_read_state(sfp_run* r, sfp_run_state* state, int64_t* n_buffered, vo
     state->halted = st.halted;
     state->error = st.error;
     state->particle_steps = st.particle_steps;
-    state->pairs_pending = st.pair_wait;
+    state->appends_pending = st.append_wait;
     state->pad = 0;
     return SFP_OK;
 }
@@ -1152,8 +1161,9 @@ int sfp_run_clear_halt(sfp_run* r, void* stream) {
     sfp_step_state st;
     SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
-    if (st.pair_wait)
-        return fail(SFP_EINVAL, "sfp_run_clear_halt: a step waits for its pairs; finish it with sfp_run_resume");
+    if (st.append_wait)
+        return fail(SFP_EINVAL, "sfp_run_clear_halt: a step waits for room for its children; finish it with "
+                                "sfp_run_resume");
     st.halted = 0;
     st.skip = 1;
     SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
@@ -1172,7 +1182,7 @@ int sfp_run_pending_need(sfp_run* r, int64_t* need) {
     SFP_CUDA(cudaMemcpyAsync(ap.data(), r->h.appended, r->n_seg * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
-    for (int s = 0; s < r->n_seg; ++s) need[s] = st.pair_wait ? ns[s] + (long long)ap[s] : nb[s];
+    for (int s = 0; s < r->n_seg; ++s) need[s] = st.append_wait ? ns[s] + (long long)ap[s] : nb[s];
     return SFP_OK;
 }
 
@@ -1186,13 +1196,13 @@ int sfp_run_resume(sfp_run* r, void* stream) {
     SFP_CUDA(cudaMemcpyAsync(ap.data(), r->h.appended, r->n_seg * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
-    if (!st.pair_wait) return SFP_OK;
-    // the pairs kernel runs only when every destination holds its pairs
-    for (int c : r->cseg)
+    if (!st.append_wait) return SFP_OK;
+    // the appends kernel runs only when every destination holds its children
+    for (int c : r->dseg)
         if (ns[c] + (long long)ap[c] > r->segs[c].capacity)
             return fail(SFP_EINVAL, "sfp_run_resume: segment " + std::to_string(c) +
-                                        " still lacks room for the pairs of the stopped step");
-    st.pair_wait = 0;
+                                        " still lacks room for the children of the stopped step");
+    st.append_wait = 0;
     st.halted = 0;
     st.skip = 0;
     cudaStream_t cs = as_stream(stream);
@@ -1201,7 +1211,7 @@ int sfp_run_resume(sfp_run* r, void* stream) {
     SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
     void* a[] = {&r->d};
-    SFP_CUDA(cudaLaunchKernel((const void*)r->k_pairs, dim3(r->grid_c), dim3(SFP_TILE_HOST), a, 0, r->s));
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_appends, dim3(r->grid_a), dim3(SFP_TILE_HOST), a, 0, r->s));
     const int rc = launch_fold(r);
     if (rc) return rc;
     SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
@@ -1215,21 +1225,19 @@ int sfp_run_destroy(sfp_run* r) {
     for (auto& kv : r->graphs) cudaGraphExecDestroy(kv.second);
     cudaFree((void*)r->h.seg);
     cudaFree((void*)r->h.inst);
-    cudaFree((void*)r->h.mseg);
-    cudaFree((void*)r->h.pseg);
-    cudaFree((void*)r->h.cseg);
+    cudaFree(r->mg.d_seg);
+    cudaFree(r->pg.d_seg);
+    cudaFree(r->mg.d_start);
+    cudaFree(r->pg.d_start);
+    cudaFree((void*)r->h.dseg);
     cudaFree(r->h.n_buffered);
     cudaFree(r->h.appended);
     cudaFree(r->h.n_buf_step);
-    cudaFree(r->h.mtile_start);
-    cudaFree(r->h.ptile_start);
-    cudaFree(r->h.chain_first);
-    cudaFree(r->h.tile_flag);
-    cudaFree(r->h.tile_agg);
-    cudaFree(r->h.tile_incl);
-    cudaFree(r->h.ptile_cnt);
-    cudaFree(r->h.psuper_cnt);
-    cudaFree(r->h.psuper_pre);
+    for (sfp_group_dev* G : {&r->h.mg, &r->h.pg}) {
+        cudaFree(G->tile_cnt);
+        cudaFree(G->super_cnt);
+        cudaFree(G->super_pre);
+    }
     cudaFree(r->h.st);
     cudaFree(r->d);
     if (r->ev_in) cudaEventDestroy(r->ev_in);

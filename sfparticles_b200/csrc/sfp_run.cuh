@@ -2,16 +2,24 @@
 // C-ABI (nvcc) and the NVRTC-compiled step modules.
 //
 // A step runs four kernels after the bookkeeping kernel:
-//   massive   -- block tiles over the e+- (massive) segments: QED photon
-//                emission, recoil, Boris push, photon children (ordered by
-//                a decoupled look-back over the tiles);
-//   photon    -- warp tiles over the photon segments: pair creation (the
-//                converted photon is marked and its delta stored), photon
-//                push; per-tile event counts, summed per super-tile of 64;
-//   pair scan -- one block: exclusive scan of the super-tile counts;
-//   pairs     -- e-/e+ children of the marked photons, in index order, pushed.
-// Photon-segment tile ranges start at multiples of 64 tiles, so a
-// super-tile never spans two segments.
+//   massive -- warp tiles over the e+- (massive) segments, streamed through
+//              a ring of asynchronous copies: QED photon emission at t; an
+//              emitter is marked (pruned = 2) with its delta stored and is
+//              left unpushed, every other particle is pushed to t+dt;
+//              per-tile emission counts, summed per super-tile of 64;
+//   photon  -- warp tiles over the photon segments: pair creation (the
+//              converted photon is marked and its delta stored), photon
+//              push; per-tile event counts, summed per super-tile;
+//   scan    -- one block: exclusive scans of both groups' super-tile counts
+//              (segmented by instance, per append channel), the step's
+//              append counts, and the exact room check of every destination;
+//   appends -- photon children of the marked emitters (then their recoil
+//              and push) and e-/e+ children of the marked photons (pushed),
+//              each written at the slot the reference's find_event_index +
+//              create_* gives it.
+// Both groups' segments start at multiples of 64 tiles, so a super-tile
+// never spans two segments.  No kernel waits on another block: there is no
+// spin-wait anywhere in a step.
 #pragma once
 #include "sfp_types.h"
 
@@ -23,12 +31,25 @@ struct sfp_step_state {
     int mticket;                // next massive tile to hand out
     int pticket;                // next photon tile to hand out
     int skip;                   // 1: the prepared step must not run
-    int halted;                 // sticky: capacity guard tripped (host regrows, resets)
+    int halted;                 // sticky: a destination lacked room (host regrows, resumes)
     int error;                  // sticky device error (SFP_DEV_*)
-    unsigned int epoch;         // look-back flag epoch of the prepared step
+    int pad0;
     int pending;                // a prepared step awaits folding
-    int pair_wait;              // the prepared step stopped before writing its pairs (no room)
+    int append_wait;            // the prepared step stopped before writing its children (no room)
     long long particle_steps;   // sum over executed steps of all N_buffered
+};
+
+// one group of tiles (massive or photon): the tile map of its segments and
+// its per-tile / per-super-tile event counts
+struct sfp_group_dev {
+    const int* seg;             // [n_seg] segment indices, in segment order
+    long long* tile_start;      // [n_seg + 1] first tile of each segment (multiples of 64)
+    unsigned int* tile_cnt;     // [max_tiles] events per tile
+    unsigned int* super_cnt;    // [max_tiles / 64 + 2] events per super-tile
+    long long* super_pre;       // [max_tiles / 64 + 2] exclusive prefix in its instance, per channel
+    long long max_tiles;
+    int n_seg;
+    int pad;
 };
 
 struct sfp_run_dev {
@@ -39,35 +60,24 @@ struct sfp_run_dev {
     double dt;
     double photon_threshold;
     int qed;                    // SFP_QED_*
-    int mtile;                  // particles per massive tile (256 * items)
-    int ptile;                  // photons per photon (warp) tile
-    int any_appends;            // some massive segment radiates (the massive look-back runs)
-    int n_mseg;                 // massive segments (instance order)
-    int n_pseg;                 // photon segments
-    int n_cseg;                 // segments receiving pair children
-    int pad;
-    const int* mseg;            // [n_mseg] segment indices
-    const int* pseg;            // [n_pseg]
-    const int* cseg;            // [n_cseg]
+    int tile;                   // particles per (warp) tile, both groups
+    int any_rad;                // some massive segment radiates
+    int any_bw;                 // some photon segment creates pairs
+    int n_dseg;                 // segments receiving children (photons or pairs)
+    int m_ring_off;             // massive kernel: byte offset of its copy ring in dynamic smem
+    int m_stage_bytes;          // massive kernel: bytes per ring stage (the run's widest segment layout)
+    int ring_off;               // photon kernel: byte offset of its copy ring in dynamic smem
+    int mlp_off;                // massive kernel: byte offset of the network weights in dynamic smem
+    int pad1;
+    const int* dseg;            // [n_dseg]
+    sfp_group_dev mg;           // massive group
+    sfp_group_dev pg;           // photon group
     sfp_rs_table rs;
     sfp_od_table od_photon;
     sfp_od_table od_pair;
     long long* n_buffered;        // [n_seg] authoritative buffered counts
     unsigned long long* appended; // [n_seg] children appended by the running step
     long long* n_buf_step;        // [n_seg] counts at the start of the running step
-    long long* mtile_start;       // [n_mseg + 1]
-    long long* ptile_start;       // [n_pseg + 1]
-    long long* chain_first;       // [n_seg] first massive tile of the segment's chain
-    long long max_ptiles;
-    unsigned int* ptile_cnt;      // [max_ptiles] pair events per photon tile
-    unsigned int* psuper_cnt;     // [max_ptiles / 64 + 1] pair events per super-tile
-    long long* psuper_pre;        // [max_ptiles / 64 + 1] exclusive prefix in its chain
-    int ring_off;                 // photon kernel: byte offset of the copy ring in dynamic smem
-    int mlp_off;                  // massive kernel: byte offset of the network weights in dynamic smem
     const float* mlp_params;      // learned photon-energy sampler (optical depth), or NULL: the table
-    long long max_tiles;
-    unsigned int* tile_flag;      // [max_tiles] (epoch << 2) | status
-    uint4* tile_agg;              // [max_tiles] per-channel tile counts
-    uint4* tile_incl;             // [max_tiles] per-channel inclusive prefixes
     sfp_step_state* st;
 };

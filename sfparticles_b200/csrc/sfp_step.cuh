@@ -1,5 +1,5 @@
-// sfp_step.cuh -- the fused particle step (one launch advances every species
-// of every instance by one step) plus its bookkeeping kernel.
+// sfp_step.cuh -- the fused particle step (one launch per kernel advances
+// every species of every instance by one step) plus its bookkeeping kernel.
 //
 // Compiled by NVRTC together with a generated field program that defines
 //     SFP_DEVICE_INLINE void sfp_field_program(double x, double y, double z,
@@ -14,15 +14,20 @@
 //   5. pairs appended, converted photons pruned,
 //   6. every pushed particle -- children included -- pushed from t to t+dt:
 //      half position, fields at t+dt/2, Boris / Boris-TBMT (+LL/CLL), half position.
-// After the bookkeeping kernel a step is: the massive kernel (e+- tiles:
-// 3, 4, recoil, 6), the photon kernel (photon tiles: 2, the marking of 5,
-// 6 for photons), the pair scan and the pairs kernel (5 and 6 for this
-// step's pairs).  The massive and photon kernels touch disjoint memory:
-// each writes past the start-of-step count of the other group's buffers.
-// Appends are ordered: a child gets the slot that the reference's
-// find_event_index + create_* would give it (photons: block scan plus a
-// decoupled look-back across the massive tiles; pairs: per-tile counts,
-// scanned), so Philox streams keyed by slot are reproducible.
+// After the bookkeeping kernel a step is:
+//   massive -- 3; a particle with an event is marked and left as it was at t
+//              (its delta stored), every other one takes 6;
+//   photon  -- 2; a converted photon is marked (its delta stored), every
+//              other one takes 6;
+//   scan    -- the children's slots: per-tile event counts scanned in the
+//              reference's order;
+//   appends -- 4 (child from the parent's state at t, then the parent's
+//              recoil and 6) and 5 (children pushed, 6), at those slots.
+// The massive and photon kernels touch disjoint memory: each writes only
+// below the start-of-step counts of its own group's buffers.  Appends are
+// ordered: a child gets the slot that the reference's find_event_index +
+// create_* would give it, so Philox streams keyed by slot are reproducible.
+// No kernel waits on another block.
 #pragma once
 #include "sfp_device.cuh"
 #include "sfp_device32.cuh"
@@ -32,39 +37,17 @@
 #ifndef SFP_TILE
 #define SFP_TILE 256
 #endif
-// photon (warp) tile: SFP_PHOTON_WSUB sub-steps of 32 photons
-#ifndef SFP_PHOTON_WSUB
-#define SFP_PHOTON_WSUB 32
+// warp tile of both groups: SFP_WSUB sub-steps of 32 particles
+#ifndef SFP_WSUB
+#define SFP_WSUB 32
 #endif
-// photon tiles per super-tile of the pair-event scan
+// tiles per super-tile of the event scan
 #define SFP_SUPER_TILE 64
-#define SFP_LOOKBACK_SPIN_LIMIT (1u << 24)
-
-#define SFP_FLAG_AGG 1u
-#define SFP_FLAG_INCL 2u
+// pruned-flag value of a particle whose event of this step awaits its children
+#define SFP_MARK 2
 
 namespace sfp {
 
-SFP_DEVICE_INLINE void st_release_u32(unsigned int* p, unsigned int v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-SFP_DEVICE_INLINE unsigned int ld_acquire_u32(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-SFP_DEVICE_INLINE uint4 ld_cg_u4(const uint4* p) {
-    uint4 v;
-    asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p)
-                 : "memory");
-    return v;
-}
-SFP_DEVICE_INLINE void st_cg_u4(uint4* p, uint4 v) {
-    asm volatile("st.global.cg.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
-                 : "memory");
-}
 SFP_DEVICE_INLINE unsigned int u4_get(const uint4& v, int c) {
     return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
 }
@@ -77,16 +60,6 @@ SFP_DEVICE_INLINE uint4 u4_one(int c, unsigned int n) {
     return v;
 }
 SFP_DEVICE_INLINE uint4 u4_add(uint4 a, uint4 b) { return uint4{a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
-SFP_DEVICE_INLINE uint4 warp_sum_u4(uint4 v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-        v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
-        v.w += __shfl_xor_sync(0xffffffffu, v.w, o);
-    }
-    return v;
-}
 
 // Asynchronous 16-byte global -> shared copies (cp.async, one per thread,
 // L2 only); `src_bytes` < 16 zero-fills the rest and reads only that many.
@@ -105,87 +78,31 @@ SFP_DEVICE_INLINE void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Decoupled look-back (Merrill & Garland, 2016) over the tiles of one
-// instance, run by warp 0.  A tile publishes its aggregate (AGG) as soon as
-// its events are known and its inclusive prefix (INCL) once the exclusive
-// prefix is known; look-backs sum predecessors' AGGs until an INCL.
-SFP_DEVICE_INLINE void publish(const sfp_run_dev* R, long long tile, uint4 v, unsigned int epoch, bool incl) {
-    if ((threadIdx.x & 31) == 0) {
-        st_cg_u4((incl ? R->tile_incl : R->tile_agg) + tile, v);
-        st_release_u32(R->tile_flag + tile, (epoch << 2) | (incl ? SFP_FLAG_INCL : SFP_FLAG_AGG));
+// inclusive / exclusive warp sums
+SFP_DEVICE_INLINE unsigned int warp_incl_scan(unsigned int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
     }
+    return v;
+}
+SFP_DEVICE_INLINE unsigned int warp_sum(unsigned int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
-// one window of 32 predecessors without waiting: true (and the exclusive
-// prefix) when an INCL is reached through ready tiles only
-SFP_DEVICE_INLINE bool lookback_try(const sfp_run_dev* R, long long tile, long long first_tile, unsigned int epoch,
-                                    uint4& excl) {
-    const int lane = threadIdx.x & 31;
-    const long long p = tile - 1 - lane;
-    const bool valid = p >= first_tile;
-    unsigned int status = 0;
-    if (valid) {
-        const unsigned int f = ld_acquire_u32(R->tile_flag + p);
-        if ((f >> 2) == epoch) status = f & 3u;
-    }
-    const unsigned int incl_mask = __ballot_sync(0xffffffffu, valid && status == SFP_FLAG_INCL);
-    const unsigned int ready_mask = __ballot_sync(0xffffffffu, valid && status != 0u);
-    if (!incl_mask) return false;
-    const int k = __ffs(incl_mask) - 1;
-    const unsigned int need = (k == 31) ? 0xffffffffu : ((1u << (k + 1)) - 1u);
-    if ((ready_mask & need) != need) return false;
-    uint4 v{0u, 0u, 0u, 0u};
-    if (lane < k) v = ld_cg_u4(R->tile_agg + p);
-    else if (lane == k) v = ld_cg_u4(R->tile_incl + p);
-    excl = warp_sum_u4(v);
-    return true;
-}
-
-// blocking look-back; every wait is bounded, and on timeout the run's error
-// word is set and the tile still publishes so that no successor waits on it
-SFP_DEVICE_INLINE uint4 lookback_wait(const sfp_run_dev* R, long long tile, long long first_tile, unsigned int epoch) {
-    const int lane = threadIdx.x & 31;
-    uint4 excl{0u, 0u, 0u, 0u};
-    long long base = tile - 1;
-    bool failed = false;
-    while (base >= first_tile) {
-        const long long p = base - lane;
-        const bool valid = p >= first_tile;
-        unsigned int status = 0;
-        if (valid) {
-            unsigned int spins = 0;
-            while (true) {
-                const unsigned int f = ld_acquire_u32(R->tile_flag + p);
-                if ((f >> 2) == epoch && (f & 3u) != 0u) {
-                    status = f & 3u;
-                    break;
-                }
-                if (++spins > SFP_LOOKBACK_SPIN_LIMIT ||
-                    ((spins & 255u) == 0u && *(volatile int*)&R->st->error != 0)) {
-                    failed = true;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        if (__any_sync(0xffffffffu, failed)) {
-            if (lane == 0) atomicExch(&R->st->error, SFP_DEV_LOOKBACK_TIMEOUT);
-            return uint4{0u, 0u, 0u, 0u};
-        }
-        const unsigned int incl_mask = __ballot_sync(0xffffffffu, valid && status == SFP_FLAG_INCL);
-        uint4 v{0u, 0u, 0u, 0u};
-        if (incl_mask) {
-            const int k = __ffs(incl_mask) - 1;
-            if (lane < k) v = ld_cg_u4(R->tile_agg + p);
-            else if (lane == k) v = ld_cg_u4(R->tile_incl + p);
-            excl = u4_add(excl, warp_sum_u4(v));
-            break;
-        }
-        if (valid) v = ld_cg_u4(R->tile_agg + p);
-        excl = u4_add(excl, warp_sum_u4(v));
-        base -= 32;
-    }
-    return excl;
+// bit b set where byte b of the 16 bytes v equals SFP_MARK
+SFP_DEVICE_INLINE unsigned int marks16(uint4 v) {
+    const unsigned int k = SFP_MARK * 0x01010101u;
+    const unsigned int w[4] = {__vcmpeq4(v.x, k), __vcmpeq4(v.y, k), __vcmpeq4(v.z, k), __vcmpeq4(v.w, k)};
+    unsigned int m = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        m |= (((w[q] >> 7) & 1u) | ((w[q] >> 14) & 2u) | ((w[q] >> 21) & 4u) | ((w[q] >> 28) & 8u)) << (4 * q);
+    return m;
 }
 
 // Push of one massive particle from t to t+dt (simulation.py:128-137 with
@@ -565,16 +482,26 @@ __device__ __forceinline__ int sfp_find_group_pos(const long long* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Bookkeeping: fold the appends of the step that ran, advance t; then
-// (prepare) the capacity guard, the tile maps of both groups, tickets, epoch.
+// (prepare) the tile maps of both groups, tickets, super-tile counts.
 // One block of 256 threads.
 // ---------------------------------------------------------------------------
+SFP_DEVICE_INLINE long long sfp_group_map(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G) {
+    long long acc = 0;
+    for (int j = 0; j < G.n_seg; ++j) {
+        acc = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE * SFP_SUPER_TILE;
+        G.tile_start[j] = acc;
+        acc += (R->n_buffered[G.seg[j]] + R->tile - 1) / R->tile;
+    }
+    G.tile_start[G.n_seg] = acc;
+    return acc;
+}
+
 extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_dev* __restrict__ R, int prepare) {
-    __shared__ int s_bad;
-    __shared__ long long s_nsuper;
+    __shared__ long long s_nsuper_m, s_nsuper_p;
     sfp_step_state* st = R->st;
     const int n = R->n_seg;
-    // a step that stopped before writing its pairs is folded only once resumed
-    if (st->pending && !st->pair_wait) {
+    // a step that stopped before writing its children is folded only once resumed
+    if (st->pending && !st->append_wait) {
         for (int s = threadIdx.x; s < n; s += blockDim.x) {
             R->n_buffered[s] += (long long)R->appended[s];
             R->appended[s] = 0ull;
@@ -588,296 +515,88 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
     }
     __syncthreads();
     if (!prepare) return;
-    if (threadIdx.x == 0) {
-        s_bad = 0;
-        s_nsuper = 0;
-    }
-    __syncthreads();
-    if (st->halted || st->error || st->pair_wait) {
+    if (st->halted || st->error || st->append_wait) {
         if (threadIdx.x == 0) st->skip = 1;
         return;
     }
-    // worst case photon appends per destination: every emitter emits.  (Pair
-    // destinations are checked against the exact pair count by the pair scan.)
-    for (int d = threadIdx.x; d < n; d += blockDim.x) {
-        long long need = 0;
-        const int inst = R->seg[d].instance;
-        const int f = R->inst[inst].first_seg, l = f + R->inst[inst].n_seg;
-        for (int s = f; s < l; ++s) {
-            const sfp_segment& S = R->seg[s];
-            if (S.radiating && S.photon_dest == d) need += R->n_buffered[s];
-        }
-        if (R->n_buffered[d] + need > R->seg[d].capacity) atomicExch(&s_bad, 1);
-    }
-    __syncthreads();
-    if (s_bad) {
-        if (threadIdx.x == 0) {
-            st->halted = 1;
-            st->skip = 1;
-        }
-        return;
-    }
     if (threadIdx.x == 0) {
+        s_nsuper_m = s_nsuper_p = 0;
         long long ps = 0;
         for (int s = 0; s < n; ++s) {
             R->n_buf_step[s] = R->n_buffered[s];
             ps += R->n_buffered[s];
         }
-        // massive group: tiles in segment order; each instance's tiles form one look-back chain
-        long long acc = 0;
-        int prev_inst = -1;
-        long long chain = 0;
-        for (int j = 0; j < R->n_mseg; ++j) {
-            const int s = R->mseg[j];
-            R->mtile_start[j] = acc;
-            if (R->seg[s].instance != prev_inst) {
-                prev_inst = R->seg[s].instance;
-                chain = acc;
-            }
-            R->chain_first[s] = chain;
-            acc += (R->n_buffered[s] + R->mtile - 1) / R->mtile;
-        }
-        R->mtile_start[R->n_mseg] = acc;
-        const long long m_tiles = acc;
-        // photon group: each segment starts at a multiple of SFP_SUPER_TILE tiles
-        acc = 0;
-        for (int j = 0; j < R->n_pseg; ++j) {
-            const int s = R->pseg[j];
-            acc = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE * SFP_SUPER_TILE;
-            R->ptile_start[j] = acc;
-            acc += (R->n_buffered[s] + R->ptile - 1) / R->ptile;
-        }
-        R->ptile_start[R->n_pseg] = acc;
-        if (m_tiles > R->max_tiles || acc > R->max_ptiles) {
+        // each segment's tiles start at a multiple of SFP_SUPER_TILE tiles
+        const long long m_tiles = sfp_group_map(R, R->mg);
+        const long long p_tiles = sfp_group_map(R, R->pg);
+        if (m_tiles > R->mg.max_tiles || p_tiles > R->pg.max_tiles) {
             st->error = SFP_DEV_CAPACITY;
             st->skip = 1;
         } else {
             st->n_mtiles = m_tiles;
-            st->n_ptiles = acc;
+            st->n_ptiles = p_tiles;
             st->mticket = 0;
             st->pticket = 0;
-            st->epoch = (unsigned int)((st->step + 1) & 0x3FFFFFFFll);
-            if (st->epoch == 0u) st->epoch = 1u;
             st->skip = 0;
             st->pending = 1;
             st->particle_steps += ps;
-            s_nsuper = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
+            s_nsuper_m = (m_tiles + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
+            s_nsuper_p = (p_tiles + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
         }
     }
     __syncthreads();
-    // the photon kernel adds into the super-tile counts: start them at zero
-    for (long long k = threadIdx.x; k < s_nsuper; k += blockDim.x) R->psuper_cnt[k] = 0u;
+    // the group kernels add into the super-tile counts: start them at zero
+    for (long long k = threadIdx.x; k < s_nsuper_m; k += blockDim.x) R->mg.super_cnt[k] = 0u;
+    for (long long k = threadIdx.x; k < s_nsuper_p; k += blockDim.x) R->pg.super_cnt[k] = 0u;
 }
 
 // ---------------------------------------------------------------------------
-// Massive group.  Tiles of 256 * ITEMS particles; item k of thread j is
-// particle k*256 + j of the tile (so the ordered append scans items
-// k-major).  Per tile: load -> photon events at t -> publish the count, try
-// the look-back -> recoil + push (registers) -> finish the look-back ->
-// photon children from the parents' stored (pre-push) state -> store.
+// The copy ring of both group kernels.  A warp streams its tile of
+// SFP_WSUB * 32 particles 32 at a time through STAGES shared-memory stages
+// filled with cp.async, so the state of the next sub-steps is in flight
+// while the current one computes.  The copies and the stores address the
+// tile through a per-warp descriptor in shared memory, written once per
+// tile: slots 0..NC-1 the staged float64 arrays (x, y, z, ux, uy, uz, then
+// tau under optical depth, then sx, sy, sz for spin), slot NC the pruned
+// flags, slot NC+1 the delta array; each offset to the tile's first
+// particle (NULL where the segment has no such array).
 // ---------------------------------------------------------------------------
-template <int FORM, int QED, int ITEMS>
-__device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__ R) {
-    using namespace sfp;
-    extern __shared__ __align__(16) double s_tab[];
-    __shared__ long long s_tile;
-    __shared__ int s_pos;
-    __shared__ unsigned int s_warp[ITEMS][SFP_TILE / 32];
-    __shared__ uint4 s_excl;
-    sfp_step_state* st = R->st;
-    if (st->skip || st->n_mtiles == 0) return;
-    const long long n_tiles = st->n_mtiles;
-    const double t = st->t;
-    const double dt = R->dt;
-    const unsigned int step = (unsigned int)st->step;
-    const unsigned int epoch = st->epoch;
-    const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
-    const bool any_appends = R->any_appends != 0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // learned photon-energy sampler: weights after the tables (staged before the first barrier)
-    sfp_mlp::Smem& M = *reinterpret_cast<sfp_mlp::Smem*>(reinterpret_cast<unsigned char*>(s_tab) + R->mlp_off);
-    if (QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) sfp_mlp::stage(M, R->mlp_params);
-
-    // thread 0 takes the next tile's ticket while the current tile computes
-    int next_tk = 0;
-    if (threadIdx.x == 0) next_tk = atomicAdd(&st->mticket, 1);
-    while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const long long tk = (long long)next_tk;
-            s_tile = tk;
-            s_pos = tk < n_tiles ? sfp_find_group_pos(R->mtile_start, R->n_mseg, tk) : 0;
-            if (tk < n_tiles) next_tk = atomicAdd(&st->mticket, 1);
-        }
-        __syncthreads();
-        const long long tile = s_tile;
-        if (tile >= n_tiles) break;
-        const int pos = s_pos;
-        const int si = R->mseg[pos];
-        const sfp_segment& S = R->seg[si];
-        const sfp_instance& I = R->inst[S.instance];
-        const double* __restrict__ P = I.field_params;
-        const long long N = R->n_buf_step[si];
-        const long long first_tile = R->chain_first[si];
-        const long long i0 = (tile - R->mtile_start[pos]) * (long long)(SFP_TILE * ITEMS) + threadIdx.x;
-
-        bool alive[ITEMS], ev[ITEMS];
-        double x[ITEMS], y[ITEMS], z[ITEMS], ux[ITEMS], uy[ITEMS], uz[ITEMS], tau[ITEMS], delta[ITEMS];
-        double hs[ITEMS], lchi[ITEMS];  // learned sampler only
-#pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            const long long i = i0 + (long long)k * SFP_TILE;
-            alive[k] = (i < N) && (S.pruned[i] == 0);
-            ev[k] = false;
-            delta[k] = hs[k] = lchi[k] = 0.0;
-            x[k] = y[k] = z[k] = ux[k] = uy[k] = uz[k] = tau[k] = 0.0;
-            if (alive[k]) {
-                x[k] = S.x[i]; y[k] = S.y[i]; z[k] = S.z[i];
-                ux[k] = S.ux[i]; uy[k] = S.uy[i]; uz[k] = S.uz[i];
-                if (QED == SFP_QED_OPTICAL_DEPTH && S.tau) tau[k] = S.tau[i];
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            if (alive[k] && S.radiating) {
-                const long long i = i0 + (long long)k * SFP_TILE;
-                ev[k] = sfp_photon_event<FORM, QED>(R, T, S, I, P, x[k], y[k], z[k], ux[k], uy[k], uz[k], t, step, i,
-                                                    tau[k], delta[k], hs[k], lchi[k]);
-            }
-        }
-        if (QED == SFP_QED_OPTICAL_DEPTH && R->mlp_params) sfp_mlp_events<FORM, ITEMS>(R, M, ev, delta, hs, lchi);
-        // tile count (k-major block scan); publish and try the look-back
-        unsigned int wpre[ITEMS];
-#pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            const unsigned int bal = __ballot_sync(0xffffffffu, ev[k]);
-            wpre[k] = __popc(bal & ((1u << lane) - 1u));
-            if (lane == 0) s_warp[k][warp] = __popc(bal);
-        }
-        __syncthreads();
-        uint4 agg{0u, 0u, 0u, 0u};
-        bool have_excl = true;
-        if (warp == 0 && any_appends) {
-            constexpr int NW = SFP_TILE / 32;
-            const unsigned int v = (lane < ITEMS * NW) ? s_warp[lane / NW][lane % NW] : 0u;
-            unsigned int inc = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int n2 = __shfl_up_sync(0xffffffffu, inc, o);
-                if (lane >= o) inc += n2;
-            }
-            const unsigned int total = __shfl_sync(0xffffffffu, inc, 31);
-            if (lane < ITEMS * NW) s_warp[lane / NW][lane % NW] = inc - v;
-            if (S.radiating) agg = u4_one(S.channel, total);
-            if (lane == 0 && total) atomicAdd(&R->appended[S.photon_dest], (unsigned long long)total);
-            uint4 ex{0u, 0u, 0u, 0u};
-            if (tile == first_tile) {
-                publish(R, tile, agg, epoch, true);
-            } else {
-                publish(R, tile, agg, epoch, false);
-                have_excl = lookback_try(R, tile, first_tile, epoch, ex);
-                if (have_excl) publish(R, tile, u4_add(ex, agg), epoch, true);
-            }
-            if (lane == 0) s_excl = ex;
-        }
-        // recoil and push, in registers
-        double sx[ITEMS], sy[ITEMS], sz[ITEMS];
-#pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            const long long i = i0 + (long long)k * SFP_TILE;
-            sx[k] = sy[k] = sz[k] = 0.0;
-            if (ev[k] && S.rr == SFP_RR_PHOTON) {  // recoil, cpu.py:76-87
-                const double f = 1.0 - delta[k];
-                ux[k] = ux[k] * f; uy[k] = uy[k] * f; uz[k] = uz[k] * f;
-            }
-            if (!(alive[k] && S.push)) continue;
-            if (S.spin) { sx[k] = S.sx[i]; sy[k] = S.sy[i]; sz[k] = S.sz[i]; }
-            if (FORM == SFP_FORM_FP64) push_massive(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
-            else push_massive32(x[k], y[k], z[k], ux[k], uy[k], uz[k], sx[k], sy[k], sz[k], S, P, t, dt);
-        }
-        if (warp == 0 && any_appends && !__all_sync(0xffffffffu, have_excl)) {
-            const uint4 ex = lookback_wait(R, tile, first_tile, epoch);
-            publish(R, tile, u4_add(ex, agg), epoch, true);
-            if (lane == 0) s_excl = ex;
-        }
-        __syncthreads();
-        const long long ch_base = any_appends ? (long long)u4_get(s_excl, S.channel) : 0ll;
-        // photon children (cpu.py:89-116) from the stored pre-push state, then the parents
-#pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            const long long i = i0 + (long long)k * SFP_TILE;
-            if (ev[k]) {
-                const sfp_segment& D = R->seg[S.photon_dest];
-                const long long slot = R->n_buf_step[S.photon_dest] + ch_base + s_warp[k][warp] + wpre[k];
-                double cx = S.x[i], cy = S.y[i], cz = S.z[i];
-                const double cux = delta[k] * S.ux[i], cuy = delta[k] * S.uy[i], cuz = delta[k] * S.uz[i];
-                if (D.push) {
-                    if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
-                    else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
-                }
-                D.x[slot] = cx; D.y[slot] = cy; D.z[slot] = cz;
-                D.ux[slot] = cux; D.uy[slot] = cuy; D.uz[slot] = cuz;
-                if (D.tau) D.tau[slot] = 0.0;
-                D.pruned[slot] = 0;
-            }
-            if (alive[k]) {
-                if (S.push) {
-                    S.x[i] = x[k]; S.y[i] = y[k]; S.z[i] = z[k];
-                    if (S.spin) { S.sx[i] = sx[k]; S.sy[i] = sy[k]; S.sz[i] = sz[k]; }
-                }
-                if (S.push || (ev[k] && S.rr == SFP_RR_PHOTON)) { S.ux[i] = ux[k]; S.uy[i] = uy[k]; S.uz[i] = uz[k]; }
-                if (QED == SFP_QED_OPTICAL_DEPTH && S.tau && S.radiating) S.tau[i] = tau[k];
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Photon group.  Each warp takes tiles of SFP_PHOTON_WSUB * 32 photons by
-// ticket and streams them 32 at a time through a ring of STAGES shared-
-// memory stages filled with cp.async, so the state of the next sub-steps is
-// in flight while the current one computes; after the QED tables are staged
-// no block barrier is taken.  The copies and the stores address the tile
-// through a per-warp descriptor of its arrays in shared memory, written once
-// per tile (sfp_desc_slot).  Per photon: the pair event at t; a converted
-// photon is marked (pruned = 2, not pushed) and its delta stored for the
-// pairs kernel; every other alive photon is pushed.  The warp's event count
-// goes to its tile's counter and is added to its super-tile's.
-// ---------------------------------------------------------------------------
-template <int QED>
-struct sfp_photon_ring {
-    static constexpr int NC = QED == SFP_QED_OPTICAL_DEPTH ? 7 : 6;  // staged doubles per photon
-    static constexpr int STAGE_BYTES = NC * 32 * 8 + 32;             // + the 32 pruned flags
+template <int NC>
+struct sfp_ring {
+    static constexpr int STAGE_BYTES = NC * 32 * 8 + 32;  // NC components + 32 flags
 };
 
-// A warp's tile descriptor in shared memory: each array of the tile's
-// segment, offset to the tile's first photon (NULL where the segment has no
-// such array).  Slots 0-5 x..uz, 6 tau, 7 the pruned flags, 8 pair delta.
-constexpr int SFP_DESC_TAU = 6, SFP_DESC_PRUNED = 7, SFP_DESC_DELTA = 8, SFP_DESC_N = 9;
-
+template <int QED, bool SPIN>
 SFP_DEVICE_INLINE char* sfp_desc_slot(const sfp_segment& S, int c, long long base) {
+    constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    constexpr int NC = 6 + OD + (SPIN ? 3 : 0);
+    double* p = nullptr;
     switch (c) {
-        case 0: return reinterpret_cast<char*>(S.x + base);
-        case 1: return reinterpret_cast<char*>(S.y + base);
-        case 2: return reinterpret_cast<char*>(S.z + base);
-        case 3: return reinterpret_cast<char*>(S.ux + base);
-        case 4: return reinterpret_cast<char*>(S.uy + base);
-        case 5: return reinterpret_cast<char*>(S.uz + base);
-        case SFP_DESC_TAU: return S.tau ? reinterpret_cast<char*>(S.tau + base) : nullptr;
-        case SFP_DESC_PRUNED: return reinterpret_cast<char*>(S.pruned + base);
-        default: return S.delta ? reinterpret_cast<char*>(S.delta + base) : nullptr;
+        case 0: p = S.x; break;
+        case 1: p = S.y; break;
+        case 2: p = S.z; break;
+        case 3: p = S.ux; break;
+        case 4: p = S.uy; break;
+        case 5: p = S.uz; break;
+        default: break;
     }
+    if (OD && c == 6) p = S.tau;
+    if (SPIN && c == 6 + OD) p = S.sx;
+    if (SPIN && c == 7 + OD) p = S.sy;
+    if (SPIN && c == 8 + OD) p = S.sz;
+    if (c == NC) return reinterpret_cast<char*>(S.pruned + base);
+    if (c == NC + 1) p = S.delta;
+    return p ? reinterpret_cast<char*>(p + base) : nullptr;
 }
 
-// copies of sub-step `sub` (tile photons 32 sub .. + 31) into one stage: copy
-// c is component c/16 of photons 2(c%16), +1 (c < 16 NC) or 16 pruned flags,
-// always to dst + 16 c, so components land at dst + 256 comp and the flags at
-// dst + 256 NC.  `left` = photons of the segment from the tile's first on;
-// entries past them are zero-filled and not read.  One commit group.
-template <int QED>
+// copies of sub-step `sub` (tile particles 32 sub .. + 31) into one stage:
+// copy c is component c/16 of particles 2(c%16), +1 (c < 16 NC) or 16
+// flags, always to dst + 16 c, so components land at dst + 256 comp and the
+// flags at dst + 256 NC.  `left` = particles of the segment from the tile's
+// first on; entries past them are zero-filled and not read.  One commit group.
+template <int NC>
 __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long long left, unsigned char* dst,
                                                int lane) {
-    constexpr int NC = sfp_photon_ring<QED>::NC;
     constexpr int NCOPY = NC * 16 + 2;
     const bool full = left >= (long long)(sub + 1) * 32;  // warp-uniform: no copy is short
 #pragma unroll
@@ -888,11 +607,11 @@ __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long lon
             const char* src = D[c >> 4];
             unsigned int nb = 16u;
             if (!full) nb = left - e >= 2 ? 16u : (left - e == 1 ? 8u : 0u);
-            if (!src) nb = 0u;  // no optical depth array on this segment
-            sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + (size_t)e * 8) : (const void*)D[0], nb);
+            if (!src) nb = 0u;  // the segment has no such array
+            sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + (size_t)e * 8) : (const void*)D[NC], nb);
         } else if (c < NCOPY) {
             const int e = sub * 32 + 16 * (c - NC * 16);
-            const char* src = D[SFP_DESC_PRUNED];
+            const char* src = D[NC];
             unsigned int nb = 16u;
             if (!full) nb = left - e >= 16 ? 16u : (left - e > 0 ? (unsigned int)(left - e) : 0u);
             sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + e) : (const void*)src, nb);
@@ -901,13 +620,156 @@ __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long lon
     sfp::cp_async_commit();
 }
 
+// ---------------------------------------------------------------------------
+// Massive group.  Each warp takes tiles of SFP_WSUB * 32 particles by ticket
+// (the next ticket in flight while the tile computes) and streams them
+// through the copy ring; after the tables are staged no block barrier is
+// taken.  Per particle: the photon event at t (rejection sampling or optical
+// depth, hard-photon cut); an emitter is marked (pruned = SFP_MARK) with its
+// delta stored and keeps its state at t for the appends kernel; every other
+// alive particle is pushed to t+dt (Boris / Boris-TBMT, LL/CLL) and stored.
+// The warp's event count goes to its tile's counter and its super-tile's.
+// ---------------------------------------------------------------------------
+template <int FORM, int QED, int STAGES, bool SPIN>
+__device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
+                                                         const sfp_mlp::Smem& M, const sfp_segment& S, char** desc,
+                                                         unsigned char* ring, int SB, long long base, long long left,
+                                                         double t, double dt, unsigned int step) {
+    using namespace sfp;
+    constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    constexpr int NC = 6 + OD + (SPIN ? 3 : 0);
+    const int lane = threadIdx.x & 31;
+    const sfp_instance& I = R->inst[S.instance];
+    const double* __restrict__ P = I.field_params;
+    const bool rad = S.radiating != 0, push = S.push != 0;
+    __syncwarp();  // the previous tile's lanes are done with the descriptor and the stages
+    if (lane < NC + 2) desc[lane] = sfp_desc_slot<QED, SPIN>(S, lane, base);
+    __syncwarp();
+    char* const* D = desc;
+    unsigned int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<NC>(D, k, left, ring + k * SB, lane);
+#pragma unroll 1
+    for (int sub = 0; sub < SFP_WSUB; ++sub) {
+        __syncwarp();  // every lane has read the stage about to be refilled
+        const int nsub = sub + STAGES - 1;
+        if (nsub < SFP_WSUB) sfp_ring_issue<NC>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
+        else cp_async_commit();
+        cp_async_wait<STAGES - 1>();
+        __syncwarp();  // the stage of `sub` is complete for the whole warp
+        const unsigned char* stg = ring + (sub % STAGES) * SB;
+        const double* sd = reinterpret_cast<const double*>(stg);
+        const int e = sub * 32 + lane;  // particle index from the tile's first
+        const long long i = base + e;
+        const bool alive = e < left && stg[NC * 256 + lane] == 0;
+        double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
+        double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
+        double tau = OD ? sd[192 + lane] : 0.0;
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        if (SPIN) {
+            sx = sd[(6 + OD) * 32 + lane];
+            sy = sd[(7 + OD) * 32 + lane];
+            sz = sd[(8 + OD) * 32 + lane];
+        }
+        bool ev = false;
+        double delta = 0.0, hs = 0.0, lchi = 0.0;
+        if (alive && rad)
+            ev = sfp_photon_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta, hs, lchi);
+        if (OD && R->mlp_params) {  // warp-uniform: the learned sampler draws the events' energies
+            bool e1[1] = {ev};
+            double d1[1] = {delta};
+            const double h1[1] = {hs}, l1[1] = {lchi};
+            sfp_mlp_events<FORM, 1>(R, M, e1, d1, h1, l1);
+            ev = e1[0];
+            delta = d1[0];
+        }
+        if (ev) {
+            // the appends kernel writes the photon and pushes the parent
+            reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
+            reinterpret_cast<double*>(D[NC + 1])[e] = delta;
+        } else if (alive && push) {
+            if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            reinterpret_cast<double*>(D[0])[e] = x;
+            reinterpret_cast<double*>(D[1])[e] = y;
+            reinterpret_cast<double*>(D[2])[e] = z;
+            reinterpret_cast<double*>(D[3])[e] = ux;
+            reinterpret_cast<double*>(D[4])[e] = uy;
+            reinterpret_cast<double*>(D[5])[e] = uz;
+            if (SPIN) {
+                reinterpret_cast<double*>(D[6 + OD])[e] = sx;
+                reinterpret_cast<double*>(D[7 + OD])[e] = sy;
+                reinterpret_cast<double*>(D[8 + OD])[e] = sz;
+            }
+        }
+        if (OD && alive && rad && D[6]) reinterpret_cast<double*>(D[6])[e] = tau;
+        cnt += __popc(__ballot_sync(0xffffffffu, ev));
+    }
+    return cnt;
+}
+
+template <int FORM, int QED, int STAGES>
+__device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__ R) {
+    using namespace sfp;
+    constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    constexpr int PT = 32 * SFP_WSUB;
+    extern __shared__ __align__(16) double s_tab[];
+    __shared__ char* s_desc[SFP_TILE / 32][6 + OD + 3 + 2];
+    sfp_step_state* st = R->st;
+    if (st->skip || st->n_mtiles == 0) return;
+    const long long n_tiles = st->n_mtiles;
+    const double t = st->t;
+    const double dt = R->dt;
+    const unsigned int step = (unsigned int)st->step;
+    const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
+    // learned photon-energy sampler: weights after the tables
+    sfp_mlp::Smem& M = *reinterpret_cast<sfp_mlp::Smem*>(reinterpret_cast<unsigned char*>(s_tab) + R->mlp_off);
+    if (OD && R->mlp_params) sfp_mlp::stage(M, R->mlp_params);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int SB = R->m_stage_bytes;
+    unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->m_ring_off + (size_t)warp * STAGES * SB;
+
+    int tk = 0;
+    if (lane == 0) tk = atomicAdd(&st->mticket, 1);
+    long long tile = __shfl_sync(0xffffffffu, tk, 0);
+    while (tile < n_tiles) {
+        if (lane == 0) tk = atomicAdd(&st->mticket, 1);  // next ticket, in flight during this tile
+        const int pos = sfp_find_group_pos(R->mg.tile_start, R->mg.n_seg, tile);
+        const sfp_segment& S = R->seg[R->mg.seg[pos]];
+        const long long N = R->n_buf_step[R->mg.seg[pos]];
+        const long long base = (tile - R->mg.tile_start[pos]) * (long long)PT;
+        unsigned int cnt = 0;
+        if (base < N) {  // else: alignment padding between segments
+            if (S.spin)
+                cnt = sfp_massive_tile<FORM, QED, STAGES, true>(R, T, M, S, s_desc[warp], ring, SB, base, N - base, t,
+                                                                dt, step);
+            else
+                cnt = sfp_massive_tile<FORM, QED, STAGES, false>(R, T, M, S, s_desc[warp], ring, SB, base, N - base, t,
+                                                                 dt, step);
+        }
+        if (lane == 0) {
+            R->mg.tile_cnt[tile] = cnt;
+            if (cnt) atomicAdd(&R->mg.super_cnt[tile / SFP_SUPER_TILE], cnt);
+        }
+        tile = __shfl_sync(0xffffffffu, tk, 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Photon group.  Same tiles, tickets and ring.  Per photon: the pair event
+// at t; a converted photon is marked (pruned = SFP_MARK, not pushed) and its
+// delta stored for the appends kernel; every other alive photon is pushed.
+// ---------------------------------------------------------------------------
 template <int FORM, int QED, int STAGES>
 __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
-    constexpr int NC = sfp_photon_ring<QED>::NC;
-    constexpr int SB = sfp_photon_ring<QED>::STAGE_BYTES;
-    constexpr int PT = 32 * SFP_PHOTON_WSUB;
+    constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    constexpr int NC = 6 + OD;
+    constexpr int SB = sfp_ring<NC>::STAGE_BYTES;
+    constexpr int PT = 32 * SFP_WSUB;
     extern __shared__ __align__(16) double s_tab[];
+    __shared__ char* s_desc[SFP_TILE / 32][NC + 2];
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
     const long long n_tiles = st->n_ptiles;
@@ -918,7 +780,6 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
-    __shared__ char* s_desc[SFP_TILE / 32][SFP_DESC_N];
     char* const* D = s_desc[warp];
 
     int tk = 0;
@@ -926,31 +787,31 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     long long tile = __shfl_sync(0xffffffffu, tk, 0);
     while (tile < n_tiles) {
         if (lane == 0) tk = atomicAdd(&st->pticket, 1);  // next ticket, in flight during this tile
-        const int pos = sfp_find_group_pos(R->ptile_start, R->n_pseg, tile);
-        const int si = R->pseg[pos];
+        const int pos = sfp_find_group_pos(R->pg.tile_start, R->pg.n_seg, tile);
+        const int si = R->pg.seg[pos];
         const sfp_segment& S = R->seg[si];
         const sfp_instance& I = R->inst[S.instance];
         const double* __restrict__ P = I.field_params;
         const long long N = R->n_buf_step[si];
-        const long long base = (tile - R->ptile_start[pos]) * (long long)PT;
+        const long long base = (tile - R->pg.tile_start[pos]) * (long long)PT;
         if (base >= N) {  // alignment padding between segments: no photons
-            if (lane == 0) R->ptile_cnt[tile] = 0u;
+            if (lane == 0) R->pg.tile_cnt[tile] = 0u;
             tile = __shfl_sync(0xffffffffu, tk, 0);
             continue;
         }
         const long long left = N - base;
         const bool bw = S.bw != 0, push = S.push != 0;
         __syncwarp();  // the previous tile's lanes are done with its descriptor and stages
-        if (lane < SFP_DESC_N) s_desc[warp][lane] = sfp_desc_slot(S, lane, base);
+        if (lane < NC + 2) s_desc[warp][lane] = sfp_desc_slot<QED, false>(S, lane, base);
         __syncwarp();
         unsigned int cnt = 0;
 #pragma unroll
-        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<QED>(D, k, left, ring + k * SB, lane);
+        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<NC>(D, k, left, ring + k * SB, lane);
 #pragma unroll 1
-        for (int sub = 0; sub < SFP_PHOTON_WSUB; ++sub) {
+        for (int sub = 0; sub < SFP_WSUB; ++sub) {
             __syncwarp();  // every lane has read the stage about to be refilled
             const int nsub = sub + STAGES - 1;
-            if (nsub < SFP_PHOTON_WSUB) sfp_ring_issue<QED>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
+            if (nsub < SFP_WSUB) sfp_ring_issue<NC>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
             else cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncwarp();  // the stage of `sub` is complete for the whole warp
@@ -961,15 +822,15 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             const bool alive = e < left && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
-            double tau = QED == SFP_QED_OPTICAL_DEPTH ? sd[192 + lane] : 0.0;
+            double tau = OD ? sd[192 + lane] : 0.0;
             bool ev = false;
             double delta = 0.0;
             if (alive && bw)
                 ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
             if (ev) {
-                // converted photons are pruned, not pushed (cpu.py:190); 2 marks this step's events
-                reinterpret_cast<unsigned char*>(D[SFP_DESC_PRUNED])[e] = 2;
-                reinterpret_cast<double*>(D[SFP_DESC_DELTA])[e] = delta;
+                // converted photons are pruned, not pushed (cpu.py:190); marked until their pairs are written
+                reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
+                reinterpret_cast<double*>(D[NC + 1])[e] = delta;
             } else if (alive && push) {
                 if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
                 else push_photon32(x, y, z, ux, uy, uz, dt);
@@ -977,28 +838,37 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                 reinterpret_cast<double*>(D[1])[e] = y;
                 reinterpret_cast<double*>(D[2])[e] = z;
             }
-            if (QED == SFP_QED_OPTICAL_DEPTH && alive && bw && D[SFP_DESC_TAU])
-                reinterpret_cast<double*>(D[SFP_DESC_TAU])[e] = tau;
+            if (OD && alive && bw && D[6]) reinterpret_cast<double*>(D[6])[e] = tau;
             cnt += __popc(__ballot_sync(0xffffffffu, ev));
         }
         if (lane == 0) {
-            R->ptile_cnt[tile] = cnt;
-            if (cnt) atomicAdd(&R->psuper_cnt[tile / SFP_SUPER_TILE], cnt);
+            R->pg.tile_cnt[tile] = cnt;
+            if (cnt) atomicAdd(&R->pg.super_cnt[tile / SFP_SUPER_TILE], cnt);
         }
         tile = __shfl_sync(0xffffffffu, tk, 0);
     }
 }
 
-// segment of super-tile s and whether s starts a chain (the first super-tile
-// of its instance's photon tiles)
-SFP_DEVICE_INLINE void sfp_super_info(const sfp_run_dev* __restrict__ R, long long s, int& si, bool& head) {
+// ---------------------------------------------------------------------------
+// Scan: one block.  For each group, an exclusive scan of the super-tile
+// event counts in tile order, restarted at each instance and kept per
+// append channel, so super_pre[s] is the number of children that the same
+// instance's earlier segments and tiles with the same destinations append
+// before super-tile s.  Adds every segment's events to its destinations'
+// append counts, then checks that every destination holds this step's
+// children; if one does not, the step waits for the host (append_wait).
+// ---------------------------------------------------------------------------
+// segment of super-tile s of group G and whether s starts a chain (the first
+// super-tile of its instance's tiles in that group)
+SFP_DEVICE_INLINE void sfp_super_info(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G, long long s, int& si,
+                                      bool& head) {
     const long long tile = s * SFP_SUPER_TILE;
-    si = R->pseg[sfp_find_group_pos(R->ptile_start, R->n_pseg, tile)];
+    si = G.seg[sfp_find_group_pos(G.tile_start, G.n_seg, tile)];
     if (s == 0) {
         head = true;
         return;
     }
-    const int prev = R->pseg[sfp_find_group_pos(R->ptile_start, R->n_pseg, tile - SFP_SUPER_TILE)];
+    const int prev = G.seg[sfp_find_group_pos(G.tile_start, G.n_seg, tile - SFP_SUPER_TILE)];
     head = R->seg[prev].instance != R->seg[si].instance;
 }
 
@@ -1021,19 +891,25 @@ SFP_DEVICE_INLINE void seg_scan_warp(unsigned int& h, uint4& v) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// Pair scan: one block.  Exclusive scan of the super-tile pair-event counts
-// in tile order, restarted at each instance and kept per append channel, so
-// psuper_pre[s] is the number of pairs that the same instance's photon
-// segments with the same destinations create before super-tile s.  Also
-// adds every photon segment's events to its destinations' append counts.
-// ---------------------------------------------------------------------------
-extern "C" __global__ void __launch_bounds__(1024) sfp_pair_scan_kernel(const sfp_run_dev* __restrict__ R) {
-    __shared__ unsigned int s_wh[32];
-    __shared__ uint4 s_wv[32];
-    const sfp_step_state* st = R->st;
-    if (st->skip) return;
-    const long long n_super = (st->n_ptiles + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
+// a segment's events become appends of its destinations: photons (massive
+// group) or one electron and one positron each (photon group)
+template <bool MASSIVE>
+SFP_DEVICE_INLINE void sfp_add_appends(const sfp_run_dev* __restrict__ R, int si, unsigned long long n) {
+    if (!n) return;
+    const sfp_segment& S = R->seg[si];
+    if (MASSIVE) {
+        atomicAdd(&R->appended[S.photon_dest], n);
+    } else {
+        atomicAdd(&R->appended[S.ele_dest], n);
+        atomicAdd(&R->appended[S.pos_dest], n);
+    }
+}
+
+// block-wide: every thread calls it (n_tiles is uniform)
+template <bool MASSIVE>
+__device__ __forceinline__ void sfp_scan_group(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G,
+                                               long long n_tiles, unsigned int* s_wh, uint4* s_wv) {
+    const long long n_super = (n_tiles + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE;
     if (n_super == 0) return;
     const long long per = (n_super + blockDim.x - 1) / blockDim.x;
     const long long s0 = min(n_super, (long long)threadIdx.x * per), s1 = min(n_super, s0 + per);
@@ -1044,14 +920,15 @@ extern "C" __global__ void __launch_bounds__(1024) sfp_pair_scan_kernel(const sf
     for (long long s = s0; s < s1; ++s) {
         int si;
         bool hd;
-        sfp_super_info(R, s, si, hd);
+        sfp_super_info(R, G, s, si, hd);
         if (hd) {
             h = 1;
             v = uint4{0u, 0u, 0u, 0u};
         }
-        v = sfp::u4_add(v, sfp::u4_one(R->seg[si].channel, R->psuper_cnt[s]));
+        v = sfp::u4_add(v, sfp::u4_one(R->seg[si].channel, G.super_cnt[s]));
     }
     seg_scan_warp(h, v);
+    __syncthreads();  // the previous user of s_wh / s_wv is done
     if (lane == 31) {
         s_wh[warp] = h;
         s_wv[warp] = v;
@@ -1087,46 +964,58 @@ extern "C" __global__ void __launch_bounds__(1024) sfp_pair_scan_kernel(const sf
     for (long long s = s0; s < s1; ++s) {
         int si;
         bool hd;
-        sfp_super_info(R, s, si, hd);
+        sfp_super_info(R, G, s, si, hd);
         if (hd) run = uint4{0u, 0u, 0u, 0u};
         const int ch = R->seg[si].channel;
-        R->psuper_pre[s] = (long long)sfp::u4_get(run, ch);
-        const unsigned int c = R->psuper_cnt[s];
+        G.super_pre[s] = (long long)sfp::u4_get(run, ch);
+        const unsigned int c = G.super_cnt[s];
         run = sfp::u4_add(run, sfp::u4_one(ch, c));
         if (si != cur) {
-            if (cur >= 0 && acc) {
-                atomicAdd(&R->appended[R->seg[cur].ele_dest], acc);
-                atomicAdd(&R->appended[R->seg[cur].pos_dest], acc);
-            }
+            if (cur >= 0) sfp_add_appends<MASSIVE>(R, cur, acc);
             cur = si;
             acc = 0ull;
         }
         acc += c;
     }
-    if (cur >= 0 && acc) {
-        atomicAdd(&R->appended[R->seg[cur].ele_dest], acc);
-        atomicAdd(&R->appended[R->seg[cur].pos_dest], acc);
-    }
-    __syncthreads();
-    // exact room check: the pairs kernel writes nothing unless every e-/e+
-    // destination holds its pairs; otherwise the step waits for the host
+    if (cur >= 0) sfp_add_appends<MASSIVE>(R, cur, acc);
+}
+
+extern "C" __global__ void __launch_bounds__(1024) sfp_scan_kernel(const sfp_run_dev* __restrict__ R) {
+    __shared__ unsigned int s_wh[32];
+    __shared__ uint4 s_wv[32];
     __shared__ int s_short;
+    const sfp_step_state* st = R->st;
+    if (st->skip) return;
+    if (R->any_rad) sfp_scan_group<true>(R, R->mg, st->n_mtiles, s_wh, s_wv);
+    if (R->any_bw) sfp_scan_group<false>(R, R->pg, st->n_ptiles, s_wh, s_wv);
     if (threadIdx.x == 0) s_short = 0;
-    __syncthreads();
-    for (int c = threadIdx.x; c < R->n_cseg; c += blockDim.x) {
-        const int d = R->cseg[c];
+    __syncthreads();  // every append count is in
+    // exact room check: the appends kernel writes nothing unless every
+    // destination holds its children; otherwise the step waits for the host
+    for (int c = threadIdx.x; c < R->n_dseg; c += blockDim.x) {
+        const int d = R->dseg[c];
         if (R->n_buf_step[d] + (long long)R->appended[d] > R->seg[d].capacity) atomicExch(&s_short, 1);
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_short) {
-        R->st->pair_wait = 1;
+        R->st->append_wait = 1;
         R->st->halted = 1;
     }
 }
 
-// one pair child: created at the converted photon's position with momentum
-// d * u (cpu.py:119-189), then pushed from t to t+dt like every pushed
-// particle of this step (simulation.py:128-137)
+// ---------------------------------------------------------------------------
+// Appends.  Each warp takes 32 tile counters at a time, the massive group's
+// and then the photon group's; for a tile with events it adds the counts of
+// the earlier tiles of its super-tile to the super-tile's prefix, gathers
+// the tile's marked particles in index order into shared memory (16 flags
+// per lane per pass) and then handles 32 of them at a time, so every lane
+// works: the k-th marked particle's children go to slot
+// n_buffered(start of step) + prefix + k.
+//   massive: the photon (cpu.py:89-116) from the parent's state at t,
+//            pushed; the parent's recoil (cpu.py:76-87) and push; unmarked;
+//   photon:  e- with delta u and e+ with (1 - delta) u (cpu.py:119-189),
+//            both pushed; the photon pruned.
+// ---------------------------------------------------------------------------
 template <int FORM>
 __device__ __forceinline__ void sfp_write_pair_child(const sfp_segment& D, long long slot, const double* __restrict__ P,
                                                      double x, double y, double z, double ux, double uy, double uz,
@@ -1152,78 +1041,164 @@ __device__ __forceinline__ void sfp_write_pair_child(const sfp_segment& D, long 
     D.pruned[slot] = 0;
 }
 
-// ---------------------------------------------------------------------------
-// Pairs: each warp scans 32 photon-tile counters at a time; for a tile with
-// events it adds the counts of the earlier tiles of its super-tile to the
-// super-tile's prefix, finds the marked photons in index order and writes
-// their e- (delta) and e+ (1 - delta) children, pushed, at
-// n_buffered(start of step) + prefix + rank.  The marks become plain prunes.
-// ---------------------------------------------------------------------------
 template <int FORM>
-__device__ __forceinline__ void sfp_pairs_body(const sfp_run_dev* __restrict__ R) {
+__device__ __forceinline__ void sfp_write_photon(const sfp_run_dev* __restrict__ R, const sfp_segment& S, long long i,
+                                                 long long rank, long long pre, const double* __restrict__ P, double t,
+                                                 double dt) {
     using namespace sfp;
-    constexpr int PT = 32 * SFP_PHOTON_WSUB;
+    const sfp_segment& D = R->seg[S.photon_dest];
+    const long long slot = R->n_buf_step[S.photon_dest] + pre + rank;
+    double x = S.x[i], y = S.y[i], z = S.z[i];
+    double ux = S.ux[i], uy = S.uy[i], uz = S.uz[i];
+    const double d = S.delta[i];
+    double cx = x, cy = y, cz = z;
+    const double cux = d * ux, cuy = d * uy, cuz = d * uz;
+    if (D.push) {
+        if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
+        else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
+    }
+    D.x[slot] = cx;
+    D.y[slot] = cy;
+    D.z[slot] = cz;
+    D.ux[slot] = cux;
+    D.uy[slot] = cuy;
+    D.uz[slot] = cuz;
+    if (D.tau) D.tau[slot] = 0.0;
+    D.pruned[slot] = 0;
+    if (S.rr == SFP_RR_PHOTON) {
+        const double f = 1.0 - d;
+        ux = ux * f;
+        uy = uy * f;
+        uz = uz * f;
+    }
+    if (S.push) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        if (S.spin) {
+            sx = S.sx[i];
+            sy = S.sy[i];
+            sz = S.sz[i];
+        }
+        if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+        S.x[i] = x;
+        S.y[i] = y;
+        S.z[i] = z;
+        if (S.spin) {
+            S.sx[i] = sx;
+            S.sy[i] = sy;
+            S.sz[i] = sz;
+        }
+    }
+    if (S.push || S.rr == SFP_RR_PHOTON) {
+        S.ux[i] = ux;
+        S.uy[i] = uy;
+        S.uz[i] = uz;
+    }
+    S.pruned[i] = 0;
+}
+
+template <int FORM>
+__device__ __forceinline__ void sfp_write_pair(const sfp_run_dev* __restrict__ R, const sfp_segment& S, long long i,
+                                               long long rank, long long pre, const double* __restrict__ P, double t,
+                                               double dt) {
+    const double d = S.delta[i];
+    const double px = S.x[i], py = S.y[i], pz = S.z[i];
+    const double pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
+    S.pruned[i] = 1;
+    const long long be = R->n_buf_step[S.ele_dest] + pre + rank;
+    const long long bp = R->n_buf_step[S.pos_dest] + pre + rank;
+    sfp_write_pair_child<FORM>(R->seg[S.ele_dest], be, P, px, py, pz, d * pux, d * puy, d * puz, t, dt);
+    const double d2 = 1.0 - d;
+    sfp_write_pair_child<FORM>(R->seg[S.pos_dest], bp, P, px, py, pz, d2 * pux, d2 * puy, d2 * puz, t, dt);
+}
+
+template <int FORM, bool MASSIVE>
+__device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G,
+                                                long long tile, unsigned int c, unsigned short* list, double t,
+                                                double dt) {
+    using namespace sfp;
+    constexpr int PT = 32 * SFP_WSUB;
+    const int lane = threadIdx.x & 31;
+    const long long s = tile / SFP_SUPER_TILE;
+    unsigned int part = 0u;
+    for (long long k = s * SFP_SUPER_TILE + lane; k < tile; k += 32) part += G.tile_cnt[k];
+    const long long pre = G.super_pre[s] + (long long)warp_sum(part);
+    const int pos = sfp_find_group_pos(G.tile_start, G.n_seg, tile);
+    const sfp_segment& S = R->seg[G.seg[pos]];
+    const double* __restrict__ P = R->inst[S.instance].field_params;
+    const long long N = R->n_buf_step[G.seg[pos]];
+    const long long base = (tile - G.tile_start[pos]) * (long long)PT;
+    // the tile's marked particles, in index order: lane q covers 16 flags per pass
+    unsigned int n = 0u;
+    for (int q0 = 0; q0 < PT && n < c; q0 += 512) {
+        const int e0 = q0 + 16 * lane;
+        const long long i0 = base + e0;
+        unsigned int m = 0u;
+        if (i0 + 16 <= N) {
+            m = marks16(*reinterpret_cast<const uint4*>(S.pruned + i0));
+        } else {
+            for (int b = 0; b < 16; ++b)
+                if (i0 + b < N && S.pruned[i0 + b] == SFP_MARK) m |= 1u << b;
+        }
+        const unsigned int k = __popc(m);
+        const unsigned int inc = warp_incl_scan(k);
+        unsigned int w = n + inc - k;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1u;
+            if (w < (unsigned int)PT) list[w] = (unsigned short)(e0 + b);
+            ++w;
+        }
+        n += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    __syncwarp();
+    n = min(n, (unsigned int)PT);
+    for (unsigned int j0 = 0; j0 < n; j0 += 32) {
+        const unsigned int j = j0 + lane;
+        if (j < n) {
+            const long long i = base + list[j];
+            if (MASSIVE) sfp_write_photon<FORM>(R, S, i, j, pre, P, t, dt);
+            else sfp_write_pair<FORM>(R, S, i, j, pre, P, t, dt);
+        }
+    }
+    __syncwarp();  // the list is read before the next tile rewrites it
+}
+
+template <int FORM>
+__device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__ R) {
+    __shared__ unsigned short s_list[SFP_TILE / 32][32 * SFP_WSUB];
     const sfp_step_state* st = R->st;
-    if (st->skip || st->pair_wait) return;
-    const long long n_tiles = st->n_ptiles;
+    if (st->skip || st->append_wait) return;
+    const long long nm = R->any_rad ? st->n_mtiles : 0, np = R->any_bw ? st->n_ptiles : 0;
+    const long long n_all = nm + np;
     const double t = st->t;
     const double dt = R->dt;
-    const int lane = threadIdx.x & 31;
-    const unsigned int lt = (1u << lane) - 1u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long c0 = gw * 32; c0 < n_tiles; c0 += nw * 32) {
+    for (long long c0 = gw * 32; c0 < n_all; c0 += nw * 32) {
         const long long mine = c0 + lane;
-        const unsigned int mc = mine < n_tiles ? R->ptile_cnt[mine] : 0u;
+        unsigned int mc = 0u;
+        if (mine < nm) mc = R->mg.tile_cnt[mine];
+        else if (mine < n_all) mc = R->pg.tile_cnt[mine - nm];
         unsigned int busy = __ballot_sync(0xffffffffu, mc != 0u);
         while (busy) {
             const int b = __ffs(busy) - 1;
             busy &= busy - 1u;
-            const long long tile = c0 + b;
+            const long long tg = c0 + b;
             const unsigned int c = __shfl_sync(0xffffffffu, mc, b);
-            const long long s = tile / SFP_SUPER_TILE;
-            unsigned int part = 0u;
-            for (long long k = s * SFP_SUPER_TILE + lane; k < tile; k += 32) part += R->ptile_cnt[k];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-            const long long pre = R->psuper_pre[s] + (long long)part;
-            const int pos = sfp_find_group_pos(R->ptile_start, R->n_pseg, tile);
-            const int si = R->pseg[pos];
-            const sfp_segment& S = R->seg[si];
-            const double* __restrict__ P = R->inst[S.instance].field_params;
-            const long long N = R->n_buf_step[si];
-            const long long base = (tile - R->ptile_start[pos]) * (long long)PT;
-            const sfp_segment& De = R->seg[S.ele_dest];
-            const sfp_segment& Dp = R->seg[S.pos_dest];
-            const long long be = R->n_buf_step[S.ele_dest] + pre;
-            const long long bp = R->n_buf_step[S.pos_dest] + pre;
-            unsigned int rank = 0u;
-            for (int sub = 0; sub < SFP_PHOTON_WSUB && rank < c; ++sub) {
-                const long long i = base + (long long)sub * 32 + lane;
-                const bool m = i < N && S.pruned[i] == 2;
-                const unsigned int bal = __ballot_sync(0xffffffffu, m);
-                if (m) {
-                    const long long r = (long long)(rank + __popc(bal & lt));
-                    const double d = S.delta[i];
-                    const double px = S.x[i], py = S.y[i], pz = S.z[i];
-                    const double pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
-                    S.pruned[i] = 1;
-                    sfp_write_pair_child<FORM>(De, be + r, P, px, py, pz, d * pux, d * puy, d * puz, t, dt);
-                    const double d2 = 1.0 - d;
-                    sfp_write_pair_child<FORM>(Dp, bp + r, P, px, py, pz, d2 * pux, d2 * puy, d2 * puz, t, dt);
-                }
-                rank += __popc(bal);
-            }
+            if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, tg, c, s_list[warp], t, dt);
+            else sfp_append_tile<FORM, false>(R, R->pg, tg - nm, c, s_list[warp], t, dt);
         }
     }
 }
 
-// kernels: sfp_massive_<form>_<qed>_i<items>_b<blocks>,
-// sfp_photon_<form>_<qed>_s<stages>_b<blocks>, sfp_pair_scan_kernel, sfp_pairs_<form>
-#define SFP_MASSIVE_KERNEL(FORM_S, QED_S, FORM, QED, ITEMS, MINB)                                              \
+// kernels: sfp_massive_<form>_<qed>_s<stages>_b<blocks>,
+// sfp_photon_<form>_<qed>_s<stages>_b<blocks>, sfp_scan_kernel, sfp_appends_<form>
+#define SFP_MASSIVE_KERNEL(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                             \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
-        sfp_massive_##FORM_S##_##QED_S##_i##ITEMS##_b##MINB(const sfp_run_dev* __restrict__ R) {              \
-        sfp_massive_body<FORM, QED, ITEMS>(R);                                                               \
+        sfp_massive_##FORM_S##_##QED_S##_s##STAGES##_b##MINB(const sfp_run_dev* __restrict__ R) {             \
+        sfp_massive_body<FORM, QED, STAGES>(R);                                                              \
     }
 #define SFP_PHOTON_KERNEL(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                              \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
@@ -1232,38 +1207,38 @@ __device__ __forceinline__ void sfp_pairs_body(const sfp_run_dev* __restrict__ R
     }
 
 #if defined(SFP_STEP_FORM_FP64)
-extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_pairs_fp64(const sfp_run_dev* __restrict__ R) {
-    sfp_pairs_body<SFP_FORM_FP64>(R);
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_appends_fp64(const sfp_run_dev* __restrict__ R) {
+    sfp_appends_body<SFP_FORM_FP64>(R);
 }
 #if defined(SFP_STEP_QED_RS)
-SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 1, 2)
 SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 2)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 3)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 3)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 2)
 #else
-SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 1, 2)
 SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 2)
 SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 3)
 SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif
 #endif
 #if defined(SFP_STEP_FORM_FP32)
-extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_pairs_fp32(const sfp_run_dev* __restrict__ R) {
-    sfp_pairs_body<SFP_FORM_FP32>(R);
+extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_appends_fp32(const sfp_run_dev* __restrict__ R) {
+    sfp_appends_body<SFP_FORM_FP32>(R);
 }
 #if defined(SFP_STEP_QED_RS)
-SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 3)
-SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 1, 4)
-SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 2)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 2)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 2)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 3)
 #else
-SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 1, 3)
-SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 3)
+SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 2)
 SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 4)
 SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif

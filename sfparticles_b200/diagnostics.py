@@ -24,6 +24,22 @@ def photon_spectrum(photons, bins: int = 64, lo: float = 2.0, hi: float = None, 
     return h.astype(float), (lo, hi)
 
 
+def photon_spectrum_device(photons, bins: int = 64, lo: float = 2.0, hi: float = 2500.0) -> np.ndarray:
+    """Counts in `bins` log10 bins over [lo, hi] of the alive photons of a
+    species whose state is on the device (a run in progress), computed there;
+    energies outside the range are not counted."""
+    import torch
+    n = photons.N_buffered
+    if n == 0:
+        return np.zeros(bins)
+    alive = photons._d("_to_be_pruned")[:n] == 0
+    ux, uy, uz = (photons._d(k)[:n] for k in ("ux", "uy", "uz"))
+    le = 0.5 * torch.log10(ux * ux + uy * uy + uz * uz)
+    le = le[alive & (le >= np.log10(lo)) & (le <= np.log10(hi))]
+    h = torch.histc(le, bins=bins, min=float(np.log10(lo)), max=float(np.log10(hi)))
+    return h.double().cpu().numpy()
+
+
 def spectrum_rel_l1(a: np.ndarray, b: np.ndarray) -> float:
     """sum |a - b| / sum b."""
     a = np.asarray(a, dtype=float)

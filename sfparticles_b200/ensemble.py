@@ -25,11 +25,11 @@ from typing import Sequence
 
 from . import _lib, program
 from .particles import _device, _stream_ptr
-from .simulation import Simulation, observe_rates, plan_chunk, resolve_pending_pairs
+from .simulation import Simulation, _release_cached_blocks, observe_rates, plan_chunk, resolve_pending
 
 
 class Ensemble(object):
-    def __init__(self, sims: Sequence[Simulation], graph_chunk: int = 64, items: int = 0, min_blocks: int = 0,
+    def __init__(self, sims: Sequence[Simulation], graph_chunk: int = 64, m_stages: int = 0, min_blocks: int = 0,
                  p_stages: int = 0, p_min_blocks: int = 0) -> None:
         sims = list(sims)
         if not sims:
@@ -52,7 +52,7 @@ class Ensemble(object):
         self.form, self.qed_method, self.dt = first.form, first.qed_method, first.dt
         self.step, self.t = first.step, first.t
         self.graph_chunk = int(graph_chunk)
-        self.items = int(items) or first.items
+        self.m_stages = int(m_stages) or first.m_stages
         self.min_blocks = int(min_blocks) or first.min_blocks
         self.p_stages = int(p_stages) or first.p_stages
         self.p_min_blocks = int(p_min_blocks) or first.p_min_blocks
@@ -82,21 +82,15 @@ class Ensemble(object):
             base += len(sim.all_particles)
         return segs
 
-    def _ensure_headroom(self) -> bool:
-        grew = False
-        for s in self.sims:
-            grew = s._ensure_headroom() or grew
-        return grew
-
     def _launches_per_step(self):
         ps = self.species
-        return (1 + any(p.m != 0 for p in ps) + any(p.m == 0 for p in ps) + 2 * any(p.bw for p in ps))
+        return (1 + any(p.m != 0 for p in ps) + any(p.m == 0 for p in ps)
+                + 2 * any(p.bw or p.radiating for p in ps))
 
     def _begin(self):
         for p in self.species:
             p._to_gpu()
             p._drop_scratch()
-        self._ensure_headroom()
         first = self.sims[0]
         mod = program.get_module(first.fields, form=self.form, qed=self.qed_method)
         dev = _device()
@@ -114,7 +108,7 @@ class Ensemble(object):
         nbuf = (ctypes.c_int64 * len(allp))(*[p.N_buffered for p in allp])
         cfg = first._run_config()
         cfg.t0, cfg.step0 = self.t, self.step
-        cfg.items, cfg.min_blocks = self.items, self.min_blocks
+        cfg.m_stages, cfg.min_blocks = self.m_stages, self.min_blocks
         cfg.p_stages, cfg.p_min_blocks = self.p_stages, self.p_min_blocks
         run = ctypes.c_void_p()
         _lib.call("sfp_run_create", mod.handle, ctypes.byref(cfg), len(self.sims), inst, len(allp), segs, nbuf,
@@ -161,9 +155,10 @@ class Ensemble(object):
         max_chunk = 4 * self.graph_chunk if self.graph_chunk > 0 else 256
         rates = self.__dict__.setdefault("_rates", {})
         while remaining > 0:
-            grew, fit = plan_chunk(allp, rates, max_chunk)
-            chunk = min(remaining, max_chunk, fit)
-            if self._ensure_headroom() or grew:
+            target = min(remaining, max_chunk if rates else (self.graph_chunk or 64))
+            grew, fit = plan_chunk(allp, rates, target)
+            chunk = min(target, fit)
+            if grew:
                 self._update_run()
             before = [p.N_buffered for p in allp]
             _lib.check(L.sfp_run_steps(self._run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
@@ -172,13 +167,11 @@ class Ensemble(object):
             done = self._sync_state(st, nbuf)
             halted = bool(st.halted)
             if halted:
-                if st.pairs_pending:
+                if st.appends_pending:
                     # finishing the stopped step completes it: count it
-                    resolve_pending_pairs(self._run, allp, lambda: self._update_run(counts=False))
+                    resolve_pending(self._run, allp, lambda: self._update_run(counts=False))
                     done += self._sync_state(st, nbuf)
                 else:
-                    self._ensure_headroom()
-                    self._update_run()
                     _lib.check(L.sfp_run_clear_halt(self._run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
             observe_rates(allp, before, done, rates)
@@ -187,7 +180,7 @@ class Ensemble(object):
 
     def time_step_kernel(self, nstep: int):
         """Advance `nstep` steps with eager launches and return, per step, the
-        CUDA-event durations [ms] of its (massive, photon, pair scan + pairs)
+        CUDA-event durations [ms] of its (massive, photon, scan + appends)
         kernels, with the buffered counts before and after."""
         if self._run is None:
             self._begin()
@@ -198,16 +191,14 @@ class Ensemble(object):
         nbuf = (ctypes.c_int64 * len(allp))()
         out = []
         for _ in range(int(nstep)):
-            if self._ensure_headroom():
-                self._update_run()
             ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             self.kernel_launches += self._launches_per_step() + 1
-            if st.error or (st.halted and not st.pairs_pending):
+            if st.error or (st.halted and not st.appends_pending):
                 raise _lib.SFPError("timed step did not complete")
-            if st.pairs_pending:  # finish the step; its pair kernels were not timed
-                resolve_pending_pairs(self._run, allp, lambda: self._update_run(counts=False))
+            if st.appends_pending:  # finish the step; its appends kernel was not timed
+                resolve_pending(self._run, allp, lambda: self._update_run(counts=False))
                 _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             else:
                 out.append((float(ms[0]), float(ms[1]), float(ms[2])))
@@ -232,6 +223,7 @@ class Ensemble(object):
         for p in self.species:
             p._prune()
             p._to_host()
+        _release_cached_blocks()
 
     def start(self, nstep: int):
         """Advance every member `nstep` steps and return host arrays, like
@@ -244,3 +236,4 @@ class Ensemble(object):
         for p in self.species:
             p._prune()
             p._to_host()
+        _release_cached_blocks()

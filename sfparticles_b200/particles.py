@@ -440,8 +440,12 @@ class Particles(object):
             self._resize(new)
 
     def _resize(self, new: int):
+        """Reallocate every array at `new` slots.  On the device the outgrown
+        blocks go back to the caching allocator, which reuses them or frees
+        them on a later allocation that would not fit; the simulation empties
+        the cache only once a run has ended, since emptying it synchronises
+        the device."""
         old = self.buffer_size
-        freed = 0
         for k, v in list(self._arr.items()):
             if self._gpu:
                 import torch
@@ -450,7 +454,6 @@ class Particles(object):
                 t[:m] = v[:m]
                 if new > old:
                     t[old:] = 1 if k == "_to_be_pruned" else 0
-                freed += v.numel() * v.element_size()
                 self._arr[k] = t
                 del v
             else:
@@ -461,10 +464,6 @@ class Particles(object):
                 self._arr[k] = a
         self.buffer_size = new
         self._touch()
-        if self._gpu and freed > (256 << 20):
-            # outgrown blocks are never reused by this buffer: return them
-            import torch
-            torch.cuda.empty_cache()
 
     def _prune(self) -> None:
         """Remove pruned particles and compact every array (particles.py:503-516)."""

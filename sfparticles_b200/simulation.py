@@ -10,21 +10,25 @@ particle (children included) from t to t+dt (simulation.py:102-144);
 ``start`` ends by pruning and returning host arrays (simulation.py:158-161).
 
 Each step is a one-block bookkeeping launch followed by the massive kernel
-(e+-: emission, recoil, push, photon children), the photon kernel (pair
-creation, photon push), a one-block scan of the pair-event counts and the
-pairs kernel (e-/e+ children written in order and pushed); steps between progress reports / callbacks run back to
-back on the device, replayed from CUDA graphs, with no host
-synchronisation.  The kernel never overruns a buffer: a device-side guard
-skips the step when a destination lacks room for the worst case (every
-emitter emits), and the host then grows that buffer by the reference rule
-and continues.
+(e+-: emission events; emitters marked, every other particle pushed), the
+photon kernel (pair events; converted photons marked, the others pushed), a
+one-block scan of both kinds of event counts and the appends kernel (photon
+children, the emitters' recoil and push, e-/e+ children, all written in the
+reference's order and pushed); steps between progress reports / callbacks
+run back to back on the device, replayed from CUDA graphs, with no host
+synchronisation.  No kernel overruns a buffer: the scan compares each
+destination's room with the step's exact number of children before any is
+written, and if one lacks room the step waits; the host grows that buffer
+by the reference rule and resumes the step.  Between device chunks the host
+grows destinations ahead of the append rates it has seen, so waits are rare.
 
 Extra keyword arguments (no reference counterpart):
   seed        -- 64-bit key of the Philox streams (default: random);
   form        -- 'fp64' (plain float64, the reference arithmetic) or 'fp32';
   graph_chunk -- steps per captured CUDA graph (0 disables graphs);
-  items, min_blocks -- massive-kernel variant: particles per thread per
-                 tile and minimum resident blocks per SM (see autotune.py);
+  m_stages, min_blocks -- massive-kernel variant: depth of the copy ring
+                 that streams e+- state into shared memory and minimum
+                 resident blocks per SM (see autotune.py);
   p_stages, p_min_blocks -- photon-kernel variant: depth of the copy ring
                  that streams photon state into shared memory and minimum
                  resident blocks per SM;
@@ -57,8 +61,8 @@ except Exception:  # pragma: no cover
     tqdm = None
 
 
-def resolve_pending_pairs(run, species, update):
-    """Finish a step that stopped before writing its pairs: grow every
+def resolve_pending(run, species, update):
+    """Finish a step that stopped before writing its children: grow every
     species to the size the step needs (the reference's _extend rule,
     particles.py:487-500), hand the new buffers to the run and resume it."""
     L = _lib.load()
@@ -78,7 +82,7 @@ def plan_chunk(species, rates, max_chunk):
     at 1.25x its rate grows by the reference rule (particles.py:487-500),
     each growth capped at half its count so memory stays near its use; the
     chunk is shortened to what then fits.  Buffer sizes do not change
-    results: they only decide how often the device stops for room."""
+    results: they only decide how often a step waits for room."""
     grew = False
     chunk = max_chunk
     for p in species:
@@ -97,6 +101,15 @@ def plan_chunk(species, rates, max_chunk):
     return grew, chunk
 
 
+def _release_cached_blocks():
+    """Return the device blocks that buffer growth outgrew to the driver.
+    Emptying the allocator's cache synchronises the device, so it is done
+    once a run has ended, never between its chunks."""
+    import torch
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.empty_cache()
+
+
 def observe_rates(species, before, steps, rates):
     """Update the append rates from the counts before and after `steps` steps."""
     if steps <= 0:
@@ -109,7 +122,7 @@ def observe_rates(species, before, steps, rates):
 class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
-                 items: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0,
+                 m_stages: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0,
                  engine: str = "fused", sampler: str = "table") -> None:
         self.all_particles = all_particles
         self.particles_push = []
@@ -137,7 +150,7 @@ class Simulation(object):
             raise ValueError("the learned photon-energy sampler runs in the fused engine")
         self.sampler = sampler
         self.graph_chunk = int(graph_chunk)
-        self.items = int(items)  # massive kernel: particles per thread per tile (0: the form's default)
+        self.m_stages = int(m_stages)  # massive kernel: depth of the copy ring (0: the form's default)
         self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
         self.p_stages = int(p_stages)  # photon kernel: depth of the copy ring (0: default)
         self.p_min_blocks = int(p_min_blocks)  # photon kernel: resident blocks per SM (0: default)
@@ -165,8 +178,8 @@ class Simulation(object):
                              "set SFPARTICLES_OPTICAL_DEPTH=1")
         from .autotune import DEFAULT
         dm, dp = DEFAULT[(self.form, self.qed_method)]
-        if self.items <= 0 or self.min_blocks <= 0:
-            self.items, self.min_blocks = dm
+        if self.m_stages <= 0 or self.min_blocks <= 0:
+            self.m_stages, self.min_blocks = dm
         if self.p_stages <= 0 or self.p_min_blocks <= 0:
             self.p_stages, self.p_min_blocks = dp
 
@@ -213,7 +226,9 @@ class Simulation(object):
             if spin:
                 s.sx, s.sy, s.sz = (p._d(k).data_ptr() for k in ("sx", "sy", "sz"))
             s.tau = p._d("tau").data_ptr() if "tau" in p.attrs else None
-            s.delta = p._d("pair_delta").data_ptr() if p.bw else None
+            # the delta of this step's events, kept until their children are written
+            s.delta = (p._d("pair_delta").data_ptr() if p.bw else
+                       p._d("photon_delta").data_ptr() if p.radiating else None)
             s.capacity = p.buffer_size
             s.q = p.q
             s.ae = getattr(p, "ae", 0.0) if spin else 0.0
@@ -235,24 +250,28 @@ class Simulation(object):
             s.stream = i
         return segs
 
-    def _worst_case_need(self):
-        """Photon appends of one step if every emitter emits.  Pair
-        destinations are grown on demand: the device counts a step's pairs
-        before writing them and stops when they do not fit."""
-        need = {id(p): 0 for p in self.all_particles}
-        for p in self.particles_rad:
-            need[id(p.photon_ref())] += p.N_buffered
-        return need
+    def _destinations(self):
+        """Species that receive children: photon and pair destinations."""
+        d = {id(p.photon_ref()): p.photon_ref() for p in self.particles_rad}
+        for p in self.particles_bw:
+            d[id(p.bw_electron_ref())] = p.bw_electron_ref()
+            d[id(p.bw_positron_ref())] = p.bw_positron_ref()
+        return list(d.values())
 
-    def _ensure_headroom(self) -> bool:
-        """Grow photon destinations that could overflow in one step; True if any grew."""
+    def reserve(self, nstep: int) -> bool:
+        """Grow every append destination ahead of `nstep` device steps to
+        twice the append rate observed so far, so that those steps run
+        without waiting for room (a run whose rate then doubles still waits
+        and grows, as always).  Updates a live run; True if any buffer grew."""
+        rates = self.__dict__.setdefault("_rates", {})
         grew = False
-        need = self._worst_case_need()
-        for p in self.all_particles:
-            n = need[id(p)]
-            if n and p.buffer_size - p.N_buffered < n:
-                p._extend(n)
+        for p in self._destinations():
+            want = int(2.0 * rates.get(id(p), 0.0) * int(nstep)) + 1024
+            if p.buffer_size - p.N_buffered < want:
+                p._extend(want)
                 grew = True
+        if grew and getattr(self, "_run", None) is not None:
+            self._update_run(self._run)
         return grew
 
     def _run_config(self):
@@ -265,7 +284,7 @@ class Simulation(object):
         cfg.step0 = self.step
         cfg.qed = _lib.SFP_QED_OPTICAL_DEPTH if self.qed_method == "od" else _lib.SFP_QED_REJECTION
         cfg.form = _lib.SFP_FORM_FP32 if self.form == "fp32" else _lib.SFP_FORM_FP64
-        cfg.items = self.items
+        cfg.m_stages = self.m_stages
         cfg.min_blocks = self.min_blocks
         cfg.p_stages = self.p_stages
         cfg.p_min_blocks = self.p_min_blocks
@@ -299,6 +318,7 @@ class Simulation(object):
         for p in self.all_particles:
             p._prune()
             p._to_host()
+        _release_cached_blocks()
 
     def _loop_ops(self, nstep, call_back):
         """The reference's step loop (simulation.py:102-144) over the per-op
@@ -345,7 +365,6 @@ class Simulation(object):
         for p in self.all_particles:
             p._to_gpu()
             p._drop_scratch()
-        self._ensure_headroom()
         mod = program.get_module(self.fields, form=self.form, qed=self.qed_method)
         params = self.fields.params_device(_device())
         inst = (_lib.Instance * 1)()
@@ -373,10 +392,10 @@ class Simulation(object):
 
     def set_kernel(self, massive=None, photon=None):
         """Switch the kernel variants of a device-resident run: `massive` =
-        (items, min_blocks), `photon` = (p_stages, p_min_blocks); None keeps
-        the current one."""
+        (m_stages, min_blocks), `photon` = (p_stages, p_min_blocks); None
+        keeps the current one."""
         if massive is not None:
-            self.items, self.min_blocks = int(massive[0]), int(massive[1])
+            self.m_stages, self.min_blocks = int(massive[0]), int(massive[1])
         if photon is not None:
             self.p_stages, self.p_min_blocks = int(photon[0]), int(photon[1])
         if getattr(self, "_run", None) is not None:
@@ -396,12 +415,14 @@ class Simulation(object):
         for p in self.all_particles:
             p._prune()
             p._to_host()
+        _release_cached_blocks()
 
     def time_step_kernel(self, nstep: int):
         """Advance `nstep` steps with eager launches and return, per step, the
-        CUDA-event durations [ms] of its (massive, photon, pair scan + pairs)
+        CUDA-event durations [ms] of its (massive, photon, scan + appends)
         kernels (recorded on the stream they run on; 0 for a kernel the run
-        does not launch), with the buffered counts before and after."""
+        does not launch), with the buffered counts before and after.  A step
+        that waited for room is finished untimed and not reported."""
         if getattr(self, "_run", None) is None:
             self._begin()
         before = [p.N_buffered for p in self.all_particles]
@@ -410,17 +431,14 @@ class Simulation(object):
         st = _lib.RunState()
         nbuf = (ctypes.c_int64 * len(self.all_particles))()
         for _ in range(int(nstep)):
-            if self._ensure_headroom():
-                self._update_run(self._run)
             ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             self.kernel_launches += self._launches_per_step() + 1
-            if st.error or (st.halted and not st.pairs_pending):
+            if st.error or (st.halted and not st.appends_pending):
                 raise _lib.SFPError("timed step did not complete")
-            if st.pairs_pending:  # finish the step; its pair kernels were not timed
-                resolve_pending_pairs(self._run, self.all_particles,
-                                      lambda: self._update_run(self._run, counts=False))
+            if st.appends_pending:  # finish the step; its appends kernel was not timed
+                resolve_pending(self._run, self.all_particles, lambda: self._update_run(self._run, counts=False))
                 _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             else:
                 out.append((float(ms[0]), float(ms[1]), float(ms[2])))
@@ -434,11 +452,11 @@ class Simulation(object):
 
     def _launches_per_step(self):
         """libsfp kernels one step launches: bookkeeping + the massive and
-        photon kernels that have species to work on + pair scan and pairs
-        when a species creates pairs."""
+        photon kernels that have species to work on + scan and appends when
+        a species emits photons or creates pairs."""
         ps = self.all_particles
         return (1 + any(p.m != 0 for p in ps) + any(p.m == 0 for p in ps)
-                + 2 * any(p.bw for p in ps))
+                + 2 * any(p.bw or p.radiating for p in ps))
 
     def _loop(self, run, nstep, call_back):
         L = _lib.load()
@@ -447,21 +465,24 @@ class Simulation(object):
         st = _lib.RunState()
         remaining = int(nstep)
         tic = perf_counter_ns()
-        # A step that meets a full destination halts the run and the rest of
-        # the queued chunk is launched as no-op kernels: bound the chunk so a
-        # halt wastes at most a few graphs (one host sync per chunk).
+        # A step that meets a full destination waits for the host and the rest
+        # of the queued chunk is launched as no-op kernels: bound the chunk so
+        # a wait wastes at most a few graphs (one host sync per chunk).
         max_chunk = 4 * self.graph_chunk if self.graph_chunk > 0 else 256
         rates = self.__dict__.setdefault("_rates", {})
         while remaining > 0:
-            grew, fit = plan_chunk(self.all_particles, rates, max_chunk)
-            chunk = min(remaining, max_chunk, fit)
+            # plan for the chunk about to run; before any append rate is known
+            # keep it to one graph, so a wait wastes little
+            target = min(remaining, max_chunk if rates else (self.graph_chunk or 64))
+            grew, fit = plan_chunk(self.all_particles, rates, target)
+            chunk = min(target, fit)
             if call_back:
                 chunk = 1
             if self.print_every:
                 chunk = min(chunk, self.print_every - (self.step % self.print_every))
             for tr in self._trajectories:
                 chunk = min(chunk, tr.steps_to_next(self.step))
-            if self._ensure_headroom() or grew:
+            if grew:
                 self._update_run(run)
             before = [p.N_buffered for p in self.all_particles]
             _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
@@ -470,13 +491,11 @@ class Simulation(object):
             done = self._sync_state(run, st, nbuf)
             halted = bool(st.halted)
             if halted:
-                if st.pairs_pending:
+                if st.appends_pending:
                     # finishing the stopped step completes it: count it
-                    resolve_pending_pairs(run, self.all_particles, lambda: self._update_run(run, counts=False))
+                    resolve_pending(run, self.all_particles, lambda: self._update_run(run, counts=False))
                     done += self._sync_state(run, st, nbuf)
                 else:
-                    self._ensure_headroom()
-                    self._update_run(run)
                     _lib.check(L.sfp_run_clear_halt(run, _stream_ptr()), "sfp_run_clear_halt")
             remaining -= done
             if done:

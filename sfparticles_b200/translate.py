@@ -62,6 +62,27 @@ def _lit(v) -> str:
     return "(" + repr(v) + ")" if v < 0 else repr(v) if "e" in repr(v) or "." in repr(v) else repr(v) + ".0"
 
 
+def _parse_lambda(src: str):
+    """The first lambda expression in `src`, the source lines that define
+    it.  Those lines need not form a statement on their own (``return
+    lambda ...``, a lambda inside a call), so the text from ``lambda`` on is
+    parsed as an expression, trimmed from the end until it parses."""
+    i = src.find("lambda")
+    if i < 0:
+        return None
+    s = src[i:].rstrip()
+    for end in range(len(s), 0, -1):
+        if s[end - 1] not in ")]},\n \t" and end != len(s):
+            continue  # only trim at the closing characters an enclosing expression can leave
+        try:
+            tree = ast.parse(s[:end], mode="eval")
+        except SyntaxError:
+            continue
+        if isinstance(tree.body, ast.Lambda):
+            return tree.body
+    return None
+
+
 class _Translator:
     def __init__(self, func):
         self.func = func
@@ -69,15 +90,18 @@ class _Translator:
             src = textwrap.dedent(inspect.getsource(func))
         except (OSError, TypeError) as e:
             raise FieldTranslationError(f"cannot read the source of {func!r}: {e}") from e
-        tree = ast.parse(src)
         node = None
-        for n in ast.walk(tree):
-            if isinstance(n, ast.FunctionDef) and n.name == func.__name__:
-                node = n
-                break
-            if isinstance(n, ast.Lambda) and func.__name__ == "<lambda>":
-                node = n
-                break
+        if func.__name__ == "<lambda>":
+            node = _parse_lambda(src)
+        else:
+            try:
+                tree = ast.parse(src)
+            except SyntaxError as e:
+                raise FieldTranslationError(f"cannot parse the source of {func.__name__}: {e}") from e
+            for n in ast.walk(tree):
+                if isinstance(n, ast.FunctionDef) and n.name == func.__name__:
+                    node = n
+                    break
         if node is None:
             raise FieldTranslationError(f"cannot find the definition of {func.__name__}")
         self.node = node

@@ -13,6 +13,8 @@ What is recorded, and from which reference code:
                       and the 256 golden total-rate values of tests/test_tables.py
 * ref_pushers.npz  -- cpu.py kernels on seeded random inputs
 * ref_fields.npz   -- fields.py presets and Fields.__add__ at seeded points
+* ref_user_fields.npz, ref_sim_user_sum.npz -- user callables (tests/user_fields.py)
+                      through Fields(callable) and Fields.__add__, and a whole run
 * ref_rates.npz    -- photon/pair_prob_rate_from_table on a (chi, delta) grid
 * ref_rs_events.npz-- rejection samplers (their Python bodies, .py_func) fed the
                       Philox draws of the oracle through a stand-in `random`
@@ -208,6 +210,54 @@ def gen_fields():
         res[f"pts_{i}"] = np.stack([x, y, z, t])
         res[f"out_{i}"] = outv
     np.savez(out("ref_fields.npz"), **res)
+
+
+def gen_user_fields():
+    """User callables (tests/user_fields.py) through the reference's
+    Fields(callable) (fields.py:11-50), alone and summed with a preset
+    (Fields.__add__, fields.py:52-61) at seeded points, and one whole
+    deterministic Simulation.start in the summed field."""
+    import sfparticles
+    from sfparticles import fields as F
+    from sfparticles.particles import RadiationReactionType as RRT
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import user_fields as U
+    rng = np.random.default_rng(11)
+    n = 256
+    cases = {"gaussian": ("gaussian", U.GAUSSIAN, False), "gaussian_plus_static": ("gaussian", U.GAUSSIAN, True),
+             "mixed": ("mixed", U.MIXED, False), "lambda": ("lambda", {}, False)}
+    res = {"cases": json.dumps(cases), "static": json.dumps(U.STATIC)}
+    for name, (builder, kw, plus_static) in cases.items():
+        fld = F.Fields(U.BUILDERS[builder](**kw))
+        if plus_static:
+            fld = fld + F.static_field(**U.STATIC)
+        x, y, z, t = field_points(rng, n, kw.get("x0", 0.0), kw.get("direction", 1))
+        if builder == "mixed":
+            x = rng.uniform(-1.5 * kw["L"], 1.5 * kw["L"], n)
+        outv = np.zeros((6, n))
+        for j in range(n):
+            o = [np.zeros(1) for _ in range(6)]
+            fld.field_func(x[j:j + 1], y[j:j + 1], z[j:j + 1], float(t[j]), 1, np.zeros(1, dtype=bool), *o)
+            outv[:, j] = [a[0] for a in o]
+        res[f"pts_{name}"] = np.stack([x, y, z, t])
+        res[f"out_{name}"] = outv
+    np.savez(out("ref_user_fields.npz"), **res)
+    # whole run: 32 electrons with Landau-Lifshitz through the user Gaussian + a static field
+    case = dict(kind="det", n_e=32, gamma0=2000.0, a0=U.GAUSSIAN["a0"], w0=U.GAUSSIAN["w0"],
+                ctau=U.GAUSSIAN["ctau"], dt_T0=1 / 50, steps=300, field="user", lead=U.GAUSSIAN["x0"], spin=False,
+                rr="LL", pairs=False, seed=0, thr=2.0)
+    rng = np.random.default_rng(sum(map(ord, "user_sum")))
+    props, spin = sim_initial(case, rng)
+    fld = F.Fields(U.gaussian_callable(**U.GAUSSIAN)) + F.static_field(**U.STATIC)
+    ele = sfparticles.Particles("ele", -1, 1, N=case["n_e"], props=tuple(np.array(a) for a in props), RR=RRT.LL)
+    dt = 0.8e-6 / 299792458.0 * case["dt_T0"]
+    sim = sfparticles.Simulation(ele, dt=dt, fields=fld, print_every=None, photon_threshold=case["thr"])
+    sim.start(case["steps"])
+    terms = [["user:gaussian", U.GAUSSIAN], ["static_field", U.STATIC]]
+    np.savez(out("ref_sim_user_sum.npz"), case=json.dumps(case), field_terms=json.dumps(terms),
+             field_comb=json.dumps([0, 1]), dt=dt, init=np.stack(props), spin_init=np.stack(spin),
+             s0_state=np.stack([getattr(ele, k) for k in ("x", "y", "z", "ux", "uy", "uz")]), s0_name="ele",
+             n_species=1)
 
 
 # ---------------------------------------------------------------------------
@@ -687,8 +737,8 @@ def gen_stats():
         json.dump(res, f, indent=1)
 
 
-PARTS = dict(tables=gen_tables, pushers=gen_pushers, fields=gen_fields, rates=gen_rates, rs_events=gen_rs_events,
-             sims=gen_sims, od=gen_od, od_sims=gen_od_sims, stats=gen_stats)
+PARTS = dict(tables=gen_tables, pushers=gen_pushers, fields=gen_fields, user_fields=gen_user_fields, rates=gen_rates,
+             rs_events=gen_rs_events, sims=gen_sims, od=gen_od, od_sims=gen_od_sims, stats=gen_stats)
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()

@@ -82,8 +82,17 @@ def sim_case_species(case, init, spin_init, api):
 
 
 def golden_case_fields(g):
+    """Product Fields of a whole-run fixture: presets by name, user callables
+    (tests/user_fields.py) as "user:<builder>"."""
     from sfparticles_b200 import fields as F
     terms = json.loads(str(g["field_terms"]))
     comb = json.loads(str(g["field_comb"]))
-    flds = [getattr(F, nm)(**kw) for nm, kw in terms]
+
+    def build(nm, kw):
+        if nm.startswith("user:"):
+            import user_fields
+            return F.Fields(user_fields.BUILDERS[nm[5:]](**kw))
+        return getattr(F, nm)(**kw)
+
+    flds = [build(nm, kw) for nm, kw in terms]
     return flds[0] if comb == 0 else flds[0] + flds[1]

@@ -20,7 +20,8 @@ pytestmark = pytest.mark.gpu
 
 # error bounds of the float32 form for deterministic runs, relative to each
 # component's largest magnitude
-FP32_RUN_BOUND = {"push_only": 1e-4, "spin_LL": 2e-4, "CLL_focused": 2e-4}
+FP32_RUN_BOUND = {"push_only": 1e-4, "spin_LL": 2e-4, "spin_CLL": 2e-4, "CLL_focused": 2e-4, "simple_LL": 2e-4,
+                  "simple_t4": 1e-4}
 
 
 def _run(g, form, seed=None):
@@ -33,19 +34,24 @@ def _run(g, form, seed=None):
     return species, sim
 
 
-@pytest.mark.parametrize("name", ["push_only", "spin_LL", "CLL_focused"])
+@pytest.mark.parametrize("name", sorted(FP32_RUN_BOUND))
 def test_fp32_deterministic_push_error_vs_reference(name):
+    """The float32 form's error against the reference's own float64 run, per
+    output: max |error| / max |reference| of each component, printed as one
+    table row (run with -s to see it) and bounded."""
     cuda_or_skip()
     g = golden(f"ref_sim_{name}.npz")
     species, _ = _run(g, "fp32")
     for i, p in enumerate(species):
         keys = ["x", "y", "z", "ux", "uy", "uz"] + (["sx", "sy", "sz"] if "sx" in p.attrs else [])
         ref = g[f"s{i}_state"]
+        errs = {}
         for j, k in enumerate(keys):
             got = getattr(p, k)
             scale = np.max(np.abs(ref[j])) + 1e-300
-            err = float(np.max(np.abs(got - ref[j])) / scale)
-            print(f"{name} {p.name}.{k}: max error / max |ref| = {err:.2e}")
+            errs[k] = float(np.max(np.abs(got - ref[j])) / scale)
+        print(f"\nFP32 error | {name} | {p.name} | " + " | ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+        for k, err in errs.items():
             assert err < FP32_RUN_BOUND[name], (name, k, err)
 
 

@@ -248,7 +248,8 @@ def _oracle_case(g):
     return species
 
 
-@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "spin_CLL", "CLL_focused", "push_only"])
+@pytest.mark.parametrize("name", ["cascade", "spin_photon", "spin_LL", "spin_CLL", "CLL_focused", "push_only",
+                                  "simple_LL", "simple_t4"])
 def test_fused_step_matches_oracle(name):
     """Fused Simulation.start on the GPU vs the oracle step loop, same Philox
     keys: identical particle counts and order, states within tolerance."""
@@ -311,9 +312,13 @@ def test_fused_optical_depth_matches_oracle_and_reference(name):
         assert _rel(got, g[f"s{i}_state"]) < RTOL_RUN, (p.name, _rel(got, g[f"s{i}_state"]))
 
 
-@pytest.mark.parametrize("name", ["spin_LL", "spin_CLL", "CLL_focused", "push_only"])
+@pytest.mark.parametrize("name", ["spin_LL", "spin_CLL", "CLL_focused", "push_only", "simple_LL", "simple_t4"])
 def test_fused_deterministic_push_matches_reference(name):
-    """Emission off: the GPU run vs the reference's own Simulation.start, 1e-10."""
+    """Emission off: the GPU run vs the reference's own Simulation.start, 1e-10.
+    simple_LL is Landau-Lifshitz on a plain (non-spin) species, whose chi is
+    recomputed after the Boris push with the t+dt/2 fields
+    (particles.py:264-281); simple_t4 is simple_laser_pulse with a
+    fourth-order temporal envelope (fields.py:69-118)."""
     cuda_or_skip()
     g = golden(f"ref_sim_{name}.npz")
     case, species, sim = _run_gpu_case(g)
@@ -377,7 +382,7 @@ def test_kernel_variants_give_the_same_results(form):
         p = p or pv[0]
         species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
         sim = S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
-                           photon_threshold=case["thr"], seed=case["seed"], form=form, items=m[0], min_blocks=m[1],
+                           photon_threshold=case["thr"], seed=case["seed"], form=form, m_stages=m[0], min_blocks=m[1],
                            p_stages=p[0], p_min_blocks=p[1])
         sim.start(case["steps"])
         got = [np.stack([getattr(q, k) for k in ("x", "y", "z", "ux", "uy", "uz")]) for q in species]
@@ -406,7 +411,7 @@ def test_autotune_selects_a_compiled_variant(tmp_path, monkeypatch):
     best, times = autotune.tune(sim, sample=10_000, steps=2)
     mv, pv = autotune.VARIANTS[("fp32", "rs")]
     assert tuple(best[0]) in mv and tuple(best[1]) in pv and len(times) == len(mv) + len(pv)
-    assert (sim.items, sim.min_blocks) == tuple(best[0]) and (sim.p_stages, sim.p_min_blocks) == tuple(best[1])
+    assert (sim.m_stages, sim.min_blocks) == tuple(best[0]) and (sim.p_stages, sim.p_min_blocks) == tuple(best[1])
     assert (sim.step, sim.t) == (step, t)  # tuning ran on a copy
     assert os.path.exists(os.path.join(str(tmp_path), "autotune.json"))
     sim.run_on_device(10)

@@ -1,8 +1,9 @@
 """Buffer-growth planning of the device loop, on host species: the
 reference's growth rule (particles.py:487-500) applied ahead of a chunk of
 device steps from the observed append rates (simulation.plan_chunk,
-observe_rates) and the one-step worst case for photon destinations
-(Simulation._ensure_headroom)."""
+observe_rates, Simulation.reserve).  The device checks each step's exact
+number of children against the room before writing them; planning only
+makes those waits rare."""
 import numpy as np
 
 import sfparticles_b200 as S
@@ -64,11 +65,29 @@ def test_observed_rates_decay_by_half_at_most():
     assert rates[id(p)] == 1.0
 
 
-def test_photon_destinations_hold_one_step_of_worst_case_emission():
-    ele = _species(300, "ele")
+def test_reserve_covers_a_window_at_twice_the_rate():
+    """Simulation.reserve: room for a window of steps at twice the append
+    rate seen, on destinations only; the window then plans one chunk."""
+    ele = _species(500, "ele")
     pho = S.Particles("pho", 0, 0)
     ele.set_photon(pho)
     sim = S.Simulation(ele, pho, dt=1e-17, fields=static_field(), print_every=None)
-    assert sim._ensure_headroom()
-    assert pho.buffer_size - pho.N_buffered >= ele.N_buffered
-    assert not sim._ensure_headroom()
+    sim._rates = {id(pho): 40.0, id(ele): 0.0}
+    size_e = ele.buffer_size
+    assert sim.reserve(20)
+    assert pho.buffer_size - pho.N_buffered >= 2 * 40 * 20
+    assert ele.buffer_size == size_e  # nothing is appended to the electrons
+    assert not sim.reserve(20)
+    grew, chunk = plan_chunk([ele, pho], sim._rates, 20)
+    assert not grew and chunk == 20
+
+
+def test_destinations_are_photon_and_pair_targets():
+    ele, pos = _species(10, "ele"), S.Particles("pos", 1, 1)
+    pho = S.Particles("pho", 0, 0)
+    ele.set_photon(pho)
+    pho.set_pair(ele, pos)
+    sim = S.Simulation(ele, pos, pho, dt=1e-17, fields=static_field(), print_every=None)
+    assert {id(p) for p in sim._destinations()} == {id(pho), id(ele), id(pos)}
+    sim2 = S.Simulation(_species(5, "ele"), dt=1e-17, fields=static_field(), print_every=None)
+    assert sim2._destinations() == []

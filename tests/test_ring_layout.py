@@ -1,13 +1,14 @@
-"""The photon kernel's copy ring, restated from its index arithmetic
-(sfparticles_b200/csrc/sfp_step.cuh: sfp_ring_issue and the reads of
-sfp_photon_body) and checked on the CPU: every staged double and flag of a
-sub-step lands where the compute loop reads it, exactly once, full 16-byte
-copies stay inside their arrays, and short copies cover exactly the photons
-that exist."""
+"""The copy ring of the massive and photon kernels, restated from its index
+arithmetic (sfparticles_b200/csrc/sfp_step.cuh: sfp_ring_issue and the
+reads of sfp_massive_tile / sfp_photon_body) and checked on the CPU: every
+staged double and flag of a sub-step lands where the compute loop reads it,
+exactly once, full 16-byte copies stay inside their arrays, and short copies
+cover exactly the particles that exist.  Layouts: 6 components (x..uz), 7
+(+ optical depth), 9 (+ spin), 10 (both)."""
 import numpy as np
 import pytest
 
-WSUB = 32  # sub-steps of 32 photons per warp tile (SFP_PHOTON_WSUB)
+WSUB = 32  # sub-steps of 32 particles per warp tile (SFP_WSUB)
 
 
 def issue(nc, sub, left):
@@ -31,10 +32,10 @@ def issue(nc, sub, left):
     return out
 
 
-@pytest.mark.parametrize("nc", [6, 7])
+@pytest.mark.parametrize("nc", [6, 7, 9, 10])
 @pytest.mark.parametrize("left", [1024, 1000, 33, 32, 31, 17, 16, 1])
 def test_every_staged_value_lands_where_it_is_read(nc, left):
-    stage = nc * 32 * 8 + 32  # sfp_photon_ring<QED>::STAGE_BYTES
+    stage = nc * 32 * 8 + 32  # sfp_ring<NC>::STAGE_BYTES
     for sub in range(WSUB):
         owner = np.full(stage, -1, dtype=np.int64)  # which (slot, element) fills each byte
         for dst, slot, e, nb in issue(nc, sub, left):
