@@ -8,9 +8,12 @@ creation; dt = T0/100; 3000 steps).  Synthetic, seeded inputs.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One "step" is one simulation step of the whole cascade (all species).
-Prints one JSON line (rank 0).  Under torchrun every rank runs its own
-instance (seed = rank): weak scaling with no data-path collective; the time
-is the max over ranks of CUDA-event time.
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own full
+collision (seed = 1000 + rank): weak scaling with no data-path collective;
+--split-beam instead gives each rank its slice of one beam (strong
+scaling).  After the timed window every rank joins one all-reduce of the
+job's counters and photon spectrum; the time is the max over ranks of
+CUDA-event time.
 """
 from __future__ import annotations
 
@@ -75,10 +78,16 @@ def beam(n, seed, steps=STEPS_FULL):
     return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
 
 
-def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64, engine="fused"):
+def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64, engine="fused", share=None):
+    """The scaled cascade with `n` electrons drawn from `seed`; `share` =
+    (start, count) keeps that slice of the beam (Philox key `seed` either way)."""
     import sfparticles_b200 as S
     from sfparticles_b200.fields import gaussian_laser_pulse
     props, L = beam(n, seed)
+    if share is not None:
+        a, c = share
+        props = tuple(np.ascontiguousarray(v[a:a + c]) for v in props)
+        n = c
     ele = S.Particles("electron", -1, 1, N=n, props=props)
     pos = S.Particles("positron", 1, 1)
     pho = S.Particles("photon", 0, 0)
@@ -219,7 +228,8 @@ def run_c3(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     clk_summary = None
-    for name, fn in (("table", lambda: mlp.sample_table(lc, u)), ("mlp", lambda: s.sample(lc, u))):
+    for name, fn in (("table", lambda: mlp.sample_table(lc, u)), ("mlp_warp", lambda: s.sample(lc, u, kernel="warp")),
+                     ("mlp", lambda: s.sample(lc, u))):
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
@@ -279,10 +289,11 @@ def run_c3(args):
             "vs_baseline": None, "dtype": "bf16/f32", "data": "synthetic",
             "config": {"workload": WORKLOAD_C3, "queries_per_step": n,
                        "l2": "inputs 0.8 GB + output 0.4 GB per step, larger than L2 (no flush needed)"},
-            "roofline": {"bound": "tensor", "kernel": "k_mlp_infer", "achieved": tflops, "peak": peak,
+            "roofline": {"bound": "tensor", "kernel": "k_mlp_infer_tc", "achieved": tflops, "peak": peak,
                          "unit": "TFLOP/s", "frac": tflops / peak, "traffic": None, "peak_kind": peak_kind,
                          "flop_per_query": MLP_FLOP_PER_QUERY},
             "table_sampler": {"ms_per_step": out["table"], "samples_per_s": n / (out["table"] * 1e-3)},
+            "warp_mma_sync_sampler": {"ms_per_step": out["mlp_warp"], "samples_per_s": n / (out["mlp_warp"] * 1e-3)},
             "mlp_over_table_speed": out["table"] / out["mlp"],
             "training": {"samples_per_s_fwd_bwd": train_sps},
             "accuracy_vs_table": acc,
@@ -537,7 +548,13 @@ def run_ours(args, rank, world):
     import sfparticles_b200 as S
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
+    from sfparticles_b200 import shard
+    # weak scaling: a full collision per rank; --split-beam: rank r's slice of one beam
     seed = 1000 + rank
+    share = None
+    if args.split_beam and world > 1:
+        share = shard.split_counts(args.electrons, world)[rank]
+        seed = 1000
     S0 = window_start(args)
     # warm-up: compile / load the module, W steps of a small instance, then a fresh timed instance
     wsim = make_sim(max(1000, args.electrons // 1000), seed, args.form)
@@ -545,7 +562,9 @@ def run_ours(args, rank, world):
     wsim.finish()
     del wsim
     sim = make_sim(args.electrons, seed, args.form, (args.m_stages, args.min_blocks), (args.p_stages, args.p_min_blocks),
-                   graph_chunk=0 if args.no_graphs else 64)
+                   graph_chunk=0 if args.no_graphs else 64, share=share)
+    if share is not None:
+        sim.seed = shard.rank_seed(seed, rank)  # the slice's own Philox key
     sim._begin()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -589,6 +608,11 @@ def run_ours(args, rank, world):
     ps = sim.particle_steps - ps0
     phases["window"] = (ms, ps, args.steps)
     counts = {p.name: p.N_buffered for p in sim.all_particles}
+    # job-wide counters and photon spectrum at the window's end: one all-reduce over the ranks
+    jd = shard.reduce_diagnostics(sim.all_particles, ps, bins=64, lo=2.0, hi=SPECTRUM_HI, device=dev)
+    job = {"buffered": jd["buffered"], "alive": jd["alive"], "window_particle_steps": jd["particle_steps"],
+           "photons_in_spectrum": float(jd["spectrum"].sum()), "spectrum_range": [2.0, SPECTRUM_HI],
+           "spectrum": [float(v) for v in jd["spectrum"]], "ranks": world}
     spectrum = None
     if not args.no_compare:
         from sfparticles_b200 import diagnostics as D
@@ -653,7 +677,9 @@ def run_ours(args, rank, world):
     # end to end through the public API from host arrays: the same window
     e2e = None
     if not args.no_e2e:
-        sim2 = make_sim(args.electrons, seed, args.form)
+        sim2 = make_sim(args.electrons, seed, args.form, share=share)
+        if share is not None:
+            sim2.seed = shard.rank_seed(seed, rank)
         if S0 > 0:
             sim2.start(S0)  # untimed: the approach, ending in host arrays
         h2d = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
@@ -682,7 +708,9 @@ def run_ours(args, rank, world):
     compare = None
     if not args.no_compare and args.form != "fp64":
         from sfparticles_b200 import diagnostics as D
-        s = make_sim(args.electrons, seed, "fp64")
+        s = make_sim(args.electrons, seed, "fp64", share=share)
+        if share is not None:
+            s.seed = shard.rank_seed(seed, rank)
         s._begin()
         if S0 > 0:
             s.run_on_device(S0)
@@ -732,7 +760,7 @@ def run_ours(args, rank, world):
                           "units_at_window_end": step_units, "per_kernel": per_kernel,
                           "variants_ms": {**{f"massive_s{a}_b{b}": v for (a, b), v in tm.items()},
                                           **{f"photon_s{a}_b{b}": v for (a, b), v in tp.items()}}},
-                e2e=e2e, compare=compare, start_step=S0, start_counts=start_counts, whole=whole)
+                e2e=e2e, compare=compare, start_step=S0, start_counts=start_counts, whole=whole, job=job)
 
 
 def _release():
@@ -759,6 +787,9 @@ def main():
                     help="c2: first step of the timed window (default: centred on the collision at step 1500 "
                          "when --steps < 3000, else 0); the steps before it run untimed")
     ap.add_argument("--no-whole-run", action="store_true", help="c2: skip the rest of the 3000-step run")
+    ap.add_argument("--split-beam", action="store_true",
+                    help="c2 under torchrun: split one beam of --electrons over the ranks (strong scaling) instead "
+                         "of a full collision per rank (weak scaling)")
     ap.add_argument("--no-compare", action="store_true", help="c2: skip the float64 run over the same window")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--m-stages", type=int, default=0)
@@ -859,15 +890,18 @@ def main():
         value = r["particle_steps"] / (r["ms"] * 1e-3)
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
+                "higher_is_better": True, "scaling": "strong" if (args.split_beam and world > 1) else "weak",
+                "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
                 "data": "synthetic",
-                "config": {"workload": window_label(r["start_step"], args.steps), "electrons_per_gpu": args.electrons,
+                "config": {"workload": window_label(r["start_step"], args.steps),
+                           "electrons_per_gpu": (args.electrons // world if (args.split_beam and world > 1)
+                                                 else args.electrons),
                            "form": args.form, "start_step": r["start_step"], "steps_timed": args.steps,
                            "l2": "state > 1 GB per step, larger than L2 (no flush needed)",
                            "counts_at_window_start": r["start_counts"], "counts_at_window_end": r["counts"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "particle_steps": r["particle_steps"], "whole_run": r["whole"],
-                "vs_fp64": r["compare"]}
+                "job_diagnostics": r["job"], "vs_fp64": r["compare"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

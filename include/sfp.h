@@ -103,8 +103,11 @@ int sfp_find_event_index(const uint8_t *event, int64_t N_event, int64_t N, int64
  * the library until exit, so N <= SFP_FEI_NOALLOC_MAX_N (2^28); larger N is
  * rejected with SFP_EINVAL.  The first call with a device current looks up
  * that device's scratch address (a call with N = 0 does only this); make it
- * before any stream capture.  Calls in flight at once on one device (other
- * streams or threads) share the scratch and race. */
+ * before any stream capture.  The address is kept for the life of the
+ * process: after cudaDeviceReset (or any end of the device's primary
+ * context) this entry point must not be called on that device again.
+ * Calls in flight at once on one device (other streams or threads) share
+ * the scratch and race. */
 #define SFP_FEI_NOALLOC_MAX_N (1LL << 28)
 int sfp_find_event_index_noalloc(const uint8_t *event, int64_t N_event, int64_t N, int64_t *index, void *stream);
 /* create_photon, cpu.py:89-116 */
@@ -217,9 +220,35 @@ int sfp_mlp_grad(const float *params, const float *features, const float *target
 /* one Adam step (step counts from 1) with gradient grad * grad_scale */
 int sfp_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t step, float lr, float beta1,
                  float beta2, float eps, float grad_scale, void *stream);
-/* batched inference on the tensor cores (BF16 weights, FP32 accumulation) */
+/* batched inference on the tensor cores (BF16 weights, FP32 accumulation):
+ * tcgen05.mma chains on 128-query tiles with the accumulators in tensor
+ * memory.  A wait on the tensor cores that gives up sets a device error
+ * flag (sfp_mlp_device_error) and leaves the rest of the batch unwritten. */
 int sfp_mlp_infer(const float *params, const double *log_chi, const double *u, double *delta, int64_t N,
                   void *stream);
+/* the same network on warp-level mma.sync tiles of 16 queries, the form the
+ * fused step uses for a warp's few emission events */
+int sfp_mlp_infer_warp(const float *params, const double *log_chi, const double *u, double *delta, int64_t N,
+                       void *stream);
+/* synchronous: 1 if an sfp_mlp_infer launch on the current device gave up
+ * waiting for its tensor cores since the last call, else 0; clears it */
+int sfp_mlp_device_error(int *code);
+
+/* ---- QED rate tables generated on the GPU --------------------------------
+ * The reference's table generators (qed/rejection_sampling_tables.py:80-112,
+ * qed/optical_depth_tables.py:136-198, scipy airy + quad) restated with the
+ * same quadrature algorithm (QUADPACK QAGS / QAGI as scipy.integrate.quad
+ * runs them, its default tolerances) so the entries agree with the
+ * reference's.  Grids and the rate prefactor (-alpha m c^2 / hbar for
+ * photons, +alpha m c^2 / hbar for pairs) are the caller's, on the device.
+ * rejection sampling: int_ai[i] = integral_{z_i}^inf Ai, aip[i] = Ai'(z_i) */
+int sfp_table_rs(const double *z, int64_t n, double *int_ai, double *aip, void *stream);
+/* optical depth, kind 0 photon emission / 1 pair creation: per chi row the
+ * total rate and the cumulative row over the delta grid (n_chi x n_delta,
+ * row-major); first: n_chi doubles of device scratch (the rows' first
+ * entries) */
+int sfp_table_od(int kind, double factor, const double *chi, int64_t n_chi, const double *delta, int64_t n_delta,
+                 double *total, double *cumulative, double *first, void *stream);
 
 #ifdef __cplusplus
 }

@@ -26,7 +26,7 @@ def nvcc() -> str:
 
 
 def library_sources():
-    return [os.path.join(CSRC, "sfp_capi.cu"), os.path.join(CSRC, "sfp_mlp.cu")]
+    return [os.path.join(CSRC, "sfp_capi.cu"), os.path.join(CSRC, "sfp_mlp.cu"), os.path.join(CSRC, "sfp_tables.cu")]
 
 
 def library_headers():

@@ -381,7 +381,9 @@ long long* g_fei_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the scratch on the current device.  Looked up once per
 // device, by the first call made with that device current; later calls on
-// that device reuse the cached address.
+// that device reuse the cached address.  The address belongs to the
+// device's primary context: a cudaDeviceReset ends it, and the entry point
+// is not to be used on that device afterwards (declared in sfp.h).
 int fei_noalloc_scratch(long long** out) {
     int dev = -1;
     SFP_CUDA(cudaGetDevice(&dev));

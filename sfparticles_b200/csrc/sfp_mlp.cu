@@ -15,8 +15,11 @@
 //   W0[64][2] b0[64] W1[64][64] b1[64] W2[64][64] b2[64] W3[64] b3
 // Row j of W holds the weights of output unit j.
 //
-// Inference (sfp_mlp.cuh): weights in BF16, FP32 accumulation; the two
-// 64x64 layers run on the tensor cores (mma.sync m16n8k16).
+// Inference: weights in BF16, FP32 accumulation.  The batched sampler
+// (sfp_mlp_infer) runs every layer but the output dot product as tcgen05.mma
+// chains with the accumulators in tensor memory (k_mlp_infer_tc below); the
+// in-step sampler, a warp's few events at a time, uses warp-level mma.sync
+// tiles (sfp_mlp.cuh), also reachable batched as sfp_mlp_infer_warp.
 //
 // Training: FP32 master weights.  The forward pass uses the weights rounded to
 // BF16, as inference does, and FP32 activations; the gradient is taken with
@@ -371,6 +374,278 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ P, 
     }
 }
 
+// ------------------------------------------------ inference on tcgen05 / TMEM
+// One CTA of 128 threads takes tiles of 128 queries, one query per thread
+// (row = thread).  Each layer is one tcgen05.mma chain issued by thread 0:
+// A (the tile's inputs or activations, BF16) and B (the layer's weights,
+// BF16) in shared memory, D (128 x 64 FP32) in tensor memory.  The input
+// layer and the biases are folded into the MMAs:
+//   layer 0: A = [x0_hi, x0_lo, x1_hi, x1_lo, 1, 1, 0 ...] (K = 16),
+//            B row n = [W0[n][0], W0[n][0], W0[n][1], W0[n][1], b0_hi, b0_lo, 0 ...];
+//   layers 1, 2: A = [h (64), 1, 1, 0 ...] (K = 80), B row n = [W[n][:], b_hi, b_lo, 0 ...];
+// with v_hi = bf16(v), v_lo = bf16(v - v_hi), so features and biases keep
+// ~16 bits where one BF16 would keep 8.  Each thread reads its row of D with
+// tcgen05.ld (the warp's 32-lane quarter of tensor memory), applies SiLU
+// (one packed half-precision tanh per two activations) and writes the next
+// layer's A row; the output layer is an FP32 dot product on the CUDA cores.
+// Shared-memory operands use the K-major layout without swizzle: 8 x 8 BF16
+// core matrices of 128 B, element (r, k) at (r/8) (K/8) 128 + (k/8) 128 +
+// (r%8) 16 + (k%8) 2 (leading-dimension byte offset 128, stride-dimension
+// byte offset (K/8) 128).  Every wait on the MMA barrier is bounded; on
+// timeout the block sets g_mlp_tc_error, stops, and still frees its tensor
+// memory.
+namespace tc {
+
+constexpr int TM = 128;  // queries per tile (the MMA's M)
+constexpr int K0 = 16;   // input layer K
+constexpr int KH = 80;   // hidden layers K
+constexpr int CM = 128;  // bytes of one core matrix
+constexpr unsigned TMEM_COLS = 64;
+// kind::f16 instruction descriptor: FP32 accumulator (bits 4-5 = 1), BF16 A
+// (bits 7-9 = 1) and B (bits 10-12 = 1), both K-major, N = 64 (bits 17-22 =
+// N/8), M = 128 (bits 24-28 = M/16)
+constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr long long WAIT_LIMIT = 1ll << 22;
+
+struct Smem {
+    alignas(128) unsigned char B0[64 * K0 * 2];
+    alignas(128) unsigned char B1[64 * KH * 2];
+    alignas(128) unsigned char B2[64 * KH * 2];
+    alignas(128) unsigned char A0[TM * K0 * 2];
+    alignas(128) unsigned char A1[TM * KH * 2];
+    float W3[64];
+    float b3;
+    unsigned tmem;
+    alignas(8) unsigned long long mbar;
+};
+
+__device__ __forceinline__ unsigned cm_off(int r, int k, int K) {
+    return (unsigned)((r >> 3) * (K / 8) * CM + (k >> 3) * CM + (r & 7) * 16 + (k & 7) * 2);
+}
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor (K-major, no swizzle) of a K-column operand
+__device__ __forceinline__ unsigned long long desc(const void* base, int K) {
+    const unsigned long long lbo = CM >> 4, sbo = (unsigned long long)((K / 8) * CM) >> 4;
+    return (unsigned long long)((smem_u32(base) >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma(unsigned d_tmem, unsigned long long a, unsigned long long b, unsigned acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc), "r"(0u));
+}
+__device__ __forceinline__ void commit(unsigned mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ bool wait_phase(unsigned mbar, unsigned phase) {
+    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// generic-proxy writes of shared memory become visible to the tensor cores
+__device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive FP32 columns of this thread's row of D
+__device__ __forceinline__ void ld16(unsigned taddr, float (&v)[16]) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// SiLU of two pre-activations through one packed half-precision tanh:
+// z sigma(z) = h (1 + tanh h), h = z / 2
+__device__ __forceinline__ void silu2(float za, float zb, float& a, float& b) {
+    const float ha = 0.5f * za, hb = 0.5f * zb;
+    unsigned hh, th;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(hh) : "f"(hb), "f"(ha));
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(th) : "r"(hh));
+    float ta, tb;
+    asm("{\n\t.reg .f16 l, h;\n\tmov.b32 {l, h}, %2;\n\tcvt.f32.f16 %0, l;\n\tcvt.f32.f16 %1, h;\n\t}"
+        : "=f"(ta), "=f"(tb)
+        : "r"(th));
+    a = fmaf(ha, ta, ha);
+    b = fmaf(hb, tb, hb);
+}
+
+__device__ __forceinline__ unsigned short bf(float f) { return (unsigned short)sfp_mlp::f2bf(f); }
+__device__ __forceinline__ void hi_lo(float v, unsigned short& h, unsigned short& l) {
+    h = bf(v);
+    l = bf(v - sfp_mlp::bf2f(h));
+}
+
+}  // namespace tc
+
+__device__ int g_mlp_tc_error;
+
+__global__ void __launch_bounds__(128, 4) k_mlp_infer_tc(const float* __restrict__ P, const double* __restrict__ lc,
+                                                         const double* __restrict__ u, double* __restrict__ out,
+                                                         long long n) {
+    using namespace tc;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights as B operands (BF16, core-matrix layout), the output layer in FP32
+    for (int k = tid; k < 64 * K0; k += blockDim.x) {
+        const int r = k / K0, c = k % K0;
+        float w = 0.0f;
+        unsigned short h, l;
+        if (c < 4) w = sfp_mlp::bf16r(P[OW0 + 2 * r + (c >> 1)]);
+        *reinterpret_cast<unsigned short*>(S.B0 + cm_off(r, c, K0)) = bf(w);
+        if (c == 4 || c == 5) {
+            hi_lo(P[OB0 + r], h, l);
+            *reinterpret_cast<unsigned short*>(S.B0 + cm_off(r, c, K0)) = c == 4 ? h : l;
+        }
+    }
+    for (int k = tid; k < 64 * KH; k += blockDim.x) {
+        const int r = k / KH, c = k % KH;
+        unsigned short v1 = 0, v2 = 0, h, l;
+        if (c < 64) {
+            v1 = bf(P[OW1 + r * 64 + c]);
+            v2 = bf(P[OW2 + r * 64 + c]);
+        } else if (c < 66) {
+            hi_lo(P[OB1 + r], h, l);
+            v1 = c == 64 ? h : l;
+            hi_lo(P[OB2 + r], h, l);
+            v2 = c == 64 ? h : l;
+        }
+        *reinterpret_cast<unsigned short*>(S.B1 + cm_off(r, c, KH)) = v1;
+        *reinterpret_cast<unsigned short*>(S.B2 + cm_off(r, c, KH)) = v2;
+    }
+    for (int k = tid; k < 64; k += blockDim.x) S.W3[k] = sfp_mlp::bf16r(P[OW3 + k]);
+    if (tid == 0) S.b3 = P[OB3];
+    // the constant columns of this thread's A rows: A0 chunk 1 (zeros), A1
+    // chunk 8 (the two bias ones) and chunk 9 (zeros)
+    {
+        const uint4 z{0u, 0u, 0u, 0u};
+        const unsigned one2 = 0x3F803F80u;  // two BF16 ones
+        *reinterpret_cast<uint4*>(S.A0 + cm_off(tid, 8, K0)) = z;
+        *reinterpret_cast<uint4*>(S.A1 + cm_off(tid, 64, KH)) = uint4{one2, 0u, 0u, 0u};
+        *reinterpret_cast<uint4*>(S.A1 + cm_off(tid, 72, KH)) = z;
+    }
+    const unsigned mbar = smem_u32(&S.mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {  // 64 columns of tensor memory: the 128 x 64 FP32 accumulator
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_smem_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const unsigned tmem = S.tmem;
+    const unsigned trow = tmem + ((unsigned)(32 * warp) << 16);  // this warp's lane quarter
+    const unsigned long long dA0 = desc(S.A0, K0), dA1 = desc(S.A1, KH);
+    const unsigned long long dB0 = desc(S.B0, K0), dB1 = desc(S.B1, KH), dB2 = desc(S.B2, KH);
+    unsigned phase = 0;
+    bool ok = true;
+    const long long n_tiles = (n + TM - 1) / TM;
+    for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const long long q = tile * TM + tid;
+        // layer 0 inputs: the features split into BF16 hi / lo parts
+        {
+            float x0 = 0.0f, x1 = 0.0f;
+            if (q < n) {
+                x0 = sfp_mlp::feat_chi(lc[q]);
+                x1 = sfp_mlp::feat_u(u[q]);
+            }
+            unsigned short a, b, c, d;
+            hi_lo(x0, a, b);
+            hi_lo(x1, c, d);
+            *reinterpret_cast<uint4*>(S.A0 + cm_off(tid, 0, K0)) =
+                uint4{(unsigned)a | ((unsigned)b << 16), (unsigned)c | ((unsigned)d << 16), 0x3F803F80u, 0u};
+        }
+        float y = 0.0f;
+        for (int layer = 0; layer < 3 && ok; ++layer) {
+            fence_smem_async();
+            fence_before();
+            __syncthreads();  // A written, D of the previous layer read
+            if (tid == 0) {
+                fence_after();
+                if (layer == 0) {
+                    mma(tmem, dA0, dB0, 0u);
+                } else {
+                    const unsigned long long dB = layer == 1 ? dB1 : dB2;
+#pragma unroll
+                    for (int kk = 0; kk < KH / 16; ++kk)  // K-steps of 16: start address + 256 B
+                        mma(tmem, dA1 + (unsigned long long)(16 * kk), dB + (unsigned long long)(16 * kk),
+                            kk ? 1u : 0u);
+                }
+                commit(mbar);
+            }
+            ok = __syncthreads_and(wait_phase(mbar, phase)) != 0;
+            phase ^= 1u;
+            if (!ok) break;
+            fence_after();
+            float v[64];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                float w[16];
+                ld16(trow + 16u * c, w);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[16 * c + i] = w[i];
+            }
+            ld_wait();
+            if (layer < 2) {  // next layer's A row, 8 columns (one core-matrix row) per store
+#pragma unroll
+                for (int ch = 0; ch < 8; ++ch) {
+                    unsigned p[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        float a, b;
+                        silu2(v[8 * ch + 2 * j], v[8 * ch + 2 * j + 1], a, b);
+                        p[j] = sfp_mlp::pack(a, b);
+                    }
+                    *reinterpret_cast<uint4*>(S.A1 + cm_off(tid, 8 * ch, KH)) = uint4{p[0], p[1], p[2], p[3]};
+                }
+            } else {  // output layer on the CUDA cores, FP32
+                y = S.b3;
+#pragma unroll
+                for (int k = 0; k < 64; k += 2) {
+                    float a, b;
+                    silu2(v[k], v[k + 1], a, b);
+                    y = fmaf(S.W3[k], a, y);
+                    y = fmaf(S.W3[k + 1], b, y);
+                }
+            }
+        }
+        if (!ok) break;
+        if (q < n) out[q] = sfp_mlp::delta_of(y);
+    }
+    if (!ok && tid == 0) {
+        atomicExch(&g_mlp_tc_error, 1);
+        tc::wait_phase(mbar, phase);  // the MMAs in flight, again bounded
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -432,12 +707,47 @@ int sfp_mlp_infer(const float* params, const double* log_chi, const double* u, d
                   void* stream) {
     if (!params || (N > 0 && (!log_chi || !u || !delta))) return sfp_set_error(SFP_EINVAL, "sfp_mlp_infer: NULL argument");
     if (N <= 0) return SFP_OK;
+    static int attr_dev = -1;
+    int dev = 0;
+    MLP_CUDA(cudaGetDevice(&dev));
+    const int smem = (int)sizeof(tc::Smem);
+    if (attr_dev != dev) {
+        MLP_CUDA(cudaFuncSetAttribute((const void*)k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_dev = dev;
+    }
+    const long long tiles = (N + tc::TM - 1) / tc::TM;
+    const long long cap = (long long)sm_count_here() * 4;  // four CTAs (4 x 64 tensor-memory columns) per SM
+    const long long grid = tiles < cap ? tiles : cap;
+    k_mlp_infer_tc<<<(unsigned)grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(params, log_chi, u, delta,
+                                                                                        N);
+    MLP_CUDA(cudaGetLastError());
+    return SFP_OK;
+}
+
+int sfp_mlp_infer_warp(const float* params, const double* log_chi, const double* u, double* delta, int64_t N,
+                       void* stream) {
+    if (!params || (N > 0 && (!log_chi || !u || !delta)))
+        return sfp_set_error(SFP_EINVAL, "sfp_mlp_infer_warp: NULL argument");
+    if (N <= 0) return SFP_OK;
     const long long warps = (N + 15) / 16;
     long long grid = (warps + 3) / 4;
     const long long cap = (long long)sm_count_here() * 16;
     if (grid > cap) grid = cap;
     k_mlp_infer<<<(unsigned)grid, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(params, log_chi, u, delta, N);
     MLP_CUDA(cudaGetLastError());
+    return SFP_OK;
+}
+
+int sfp_mlp_device_error(int* code) {
+    if (!code) return sfp_set_error(SFP_EINVAL, "sfp_mlp_device_error: NULL argument");
+    int v = 0;
+    MLP_CUDA(cudaDeviceSynchronize());
+    MLP_CUDA(cudaMemcpyFromSymbol(&v, g_mlp_tc_error, sizeof(int)));
+    if (v) {
+        const int zero = 0;
+        MLP_CUDA(cudaMemcpyToSymbol(g_mlp_tc_error, &zero, sizeof(int)));
+    }
+    *code = v;
     return SFP_OK;
 }
 

@@ -1152,7 +1152,8 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
         n += __shfl_sync(0xffffffffu, inc, 31);
     }
     __syncwarp();
-    n = min(n, (unsigned int)PT);
+    // never more children than the scan counted and made room for
+    n = min(min(n, c), (unsigned int)PT);
     for (unsigned int j0 = 0; j0 < n; j0 += 32) {
         const unsigned int j = j0 + lane;
         if (j < n) {

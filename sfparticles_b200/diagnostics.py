@@ -40,6 +40,21 @@ def photon_spectrum_device(photons, bins: int = 64, lo: float = 2.0, hi: float =
     return h.double().cpu().numpy()
 
 
+def photon_histogram(photons, bins: int = 64, lo: float = 2.0, hi: float = 2500.0) -> np.ndarray:
+    """Counts in `bins` log10 bins over [lo, hi] of the alive photons of a
+    species, wherever its state is (device: computed there; host: numpy)."""
+    if photons._gpu:
+        return photon_spectrum_device(photons, bins, lo, hi)
+    n = photons.N_buffered
+    if n == 0:
+        return np.zeros(bins)
+    alive = ~np.asarray(photons._arr["_to_be_pruned"][:n], dtype=bool)
+    ux, uy, uz = (np.asarray(photons._arr[k][:n])[alive] for k in ("ux", "uy", "uz"))
+    le = 0.5 * np.log10(ux * ux + uy * uy + uz * uz)
+    h, _ = np.histogram(le, bins=bins, range=(np.log10(lo), np.log10(hi)))
+    return h.astype(float)
+
+
 def spectrum_rel_l1(a: np.ndarray, b: np.ndarray) -> float:
     """sum |a - b| / sum b."""
     a = np.asarray(a, dtype=float)

@@ -108,14 +108,25 @@ class PhotonSampler(object):
         return s
 
     # --------------------------------------------------------- inference
-    def sample(self, log_chi, u):
-        """δ for each (log10 χ, u), float64 CUDA tensors, on the tensor cores."""
+    def sample(self, log_chi, u, kernel: str = "tcgen05"):
+        """δ for each (log10 χ, u), float64 CUDA tensors, on the tensor cores:
+        kernel 'tcgen05' (128-query tiles, accumulators in tensor memory) or
+        'warp' (the step's warp-level mma.sync tiles of 16 queries)."""
         import torch
         log_chi = log_chi.contiguous()
         u = u.contiguous()
         out = torch.empty_like(log_chi, dtype=torch.float64)
-        _lib.call("sfp_mlp_infer", _p(self.params), _p(log_chi), _p(u), _p(out), log_chi.numel(), _stream())
+        fn = {"tcgen05": "sfp_mlp_infer", "warp": "sfp_mlp_infer_warp"}[kernel]
+        _lib.call(fn, _p(self.params), _p(log_chi), _p(u), _p(out), log_chi.numel(), _stream())
         return out
+
+    @staticmethod
+    def device_error() -> int:
+        """1 if a tcgen05 inference launch gave up waiting for its tensor
+        cores since the last call (synchronises the device), else 0."""
+        code = ctypes.c_int(0)
+        _lib.call("sfp_mlp_device_error", ctypes.byref(code))
+        return int(code.value)
 
     # ---------------------------------------------------------- training
     @staticmethod

@@ -1,4 +1,8 @@
-"""QED rate tables: generation (scipy, CPU, build time) and loading.
+"""QED rate tables: generation and loading.
+
+Generation runs either on the GPU (generate_on_gpu: libsfp's own QUADPACK
+restatement and Airy functions, no scipy) or on the CPU with scipy at build
+time (rs_table_gen / od_table_gen); the two agree to ~1e-13.
 
 Two table families, as in the reference:
 
@@ -185,6 +189,58 @@ def _pmap(fn, items, processes=None):
     ctx = mp.get_context("spawn")  # never fork a process that may hold a CUDA context
     with ctx.Pool(n) as pool:
         return pool.map(fn, items, chunksize=max(1, len(items) // (4 * n)))
+
+
+def photon_factor() -> float:
+    """-alpha m c^2 / hbar, evaluated as the reference writes it."""
+    return -_ALPHA * _ME * _C ** 2 / _HBAR
+
+
+def pair_factor() -> float:
+    return _ALPHA * _ME * _C ** 2 / _HBAR
+
+
+def generate_on_gpu(z_N: int = RS_Z_N, z_max: float = RS_Z_MAX, delta_N: int = OD_DELTA_N,
+                    log_delta_min: float = OD_LOG_DELTA_MIN, chi=None):
+    """Both table families computed on the GPU by libsfp (sfp_table_rs,
+    sfp_table_od: QUADPACK's QAGS / QAGI as scipy runs them, with the
+    package's own Airy functions), without scipy.  Grids as the reference
+    builds them (numpy linspace / logspace); `chi` defaults to the product's
+    307 optical-depth rows.  Returns (rs dict, od dict) with the keys of
+    rs_tables' file and od_table_gen."""
+    import ctypes
+    import torch
+    from .. import _lib
+    from ..particles import _device, _stream_ptr
+    dev = _device()
+
+    def p(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    z = torch.as_tensor(np.linspace(0.0, z_max, z_N), device=dev)
+    ia = torch.empty_like(z)
+    dA = torch.empty_like(z)
+    _lib.call("sfp_table_rs", p(z), z_N, p(ia), p(dA), _stream_ptr())
+    if chi is None:
+        chi, step = od_chi_rows()
+    else:
+        step = (OD_LOG_CHI_MAX_REF - OD_LOG_CHI_MIN) / (OD_CHI_N_REF - 1)
+    chi_d = torch.as_tensor(np.asarray(chi, dtype=np.float64), device=dev)
+    delta = torch.as_tensor(np.logspace(log_delta_min, 0, delta_N), device=dev)
+    n = chi_d.numel()
+    out = {}
+    for kind, name, factor in ((0, "photon", photon_factor()), (1, "pair", pair_factor())):
+        tot = torch.empty(n, dtype=torch.float64, device=dev)
+        cum = torch.empty((n, delta_N), dtype=torch.float64, device=dev)
+        first = torch.empty(n, dtype=torch.float64, device=dev)
+        _lib.call("sfp_table_od", kind, factor, p(chi_d), n, p(delta), delta_N, p(tot), p(cum), p(first),
+                  _stream_ptr())
+        out[f"{name}_rate_total"] = tot.cpu().numpy()
+        out[f"{name}_cumulative"] = cum.cpu().numpy()
+    rs = dict(int_Ai=ia.cpu().numpy(), Aip=dA.cpu().numpy(), z_N=z_N, z_max=z_max)
+    od = dict(out, log_chi_min=OD_LOG_CHI_MIN, log_chi_delta=step, log_delta_min=log_delta_min,
+              log_delta_delta=(0 - log_delta_min) / (delta_N - 1), chi=np.asarray(chi, dtype=np.float64))
+    return rs, od
 
 
 def ensure_tables(verbose: bool = False):

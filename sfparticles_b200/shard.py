@@ -7,17 +7,24 @@ GPUs with no data exchange during the run:
   (``assign_instances``).
 
 Each rank then runs its share as an ordinary ``Simulation`` or ``Ensemble``
-with its own Philox key (``rank_seed``). The only collective is the
-reduction of a few scalars after the run (``reduce_job``): the maximum of
-the ranks' device times and the sum of their work (``sum_over_ranks`` for
-other totals, such as bytes copied). It works with any
-``torch.distributed`` backend: NCCL on GPUs, gloo on CPUs.
+with its own Philox key (``rank_seed``).  Nothing is exchanged per step.
+The collectives are reductions of kilobytes:
+- ``reduce_diagnostics``: every species' buffered and alive counts, the
+  particle-steps and the photon energy spectrum, summed over the ranks in
+  one all-reduce; ``JobDiagnostics`` runs it as a Simulation ``monitor`` at
+  every ``print_every`` boundary and at the end of ``start``;
+- ``reduce_job``: the maximum of the ranks' device times and the sum of
+  their work (``sum_over_ranks`` for other totals, such as bytes copied).
+They work with any ``torch.distributed`` backend: NCCL on GPUs (the vector
+on the rank's device), gloo on CPUs.
 
 This is an extension of the reference, which runs on one device.
 """
 from __future__ import annotations
 
 from typing import List, Sequence, Tuple
+
+import numpy as np
 
 
 def rank_seed(base: int, rank: int) -> int:
@@ -82,3 +89,63 @@ def reduce_job(ms: float, particle_steps: float, device=None) -> Tuple[float, fl
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dist.all_reduce(w, op=dist.ReduceOp.SUM)
     return float(t.item()), float(w.item())
+
+
+def _dist_on():
+    import torch.distributed as dist
+    return dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
+
+
+def local_diagnostics(species, particle_steps: float, bins: int = 64, lo: float = 2.0, hi: float = 2500.0):
+    """This rank's diagnostics as one float64 vector: per species its
+    buffered and its alive count, then the particle-steps, then the photon
+    spectrum (alive photons of every massless species, `bins` log10 bins of
+    energy / m_e c^2 over [lo, hi])."""
+    from .diagnostics import photon_histogram
+    v = []
+    for p in species:
+        v += [float(p.N_buffered), float(p.Npart)]
+    v.append(float(particle_steps))
+    h = np.zeros(bins)
+    for p in species:
+        if p.m == 0:
+            h = h + photon_histogram(p, bins, lo, hi)
+    return np.concatenate([np.asarray(v, dtype=np.float64), h])
+
+
+def reduce_diagnostics(species, particle_steps: float, bins: int = 64, lo: float = 2.0, hi: float = 2500.0,
+                       device=None) -> dict:
+    """Job-wide diagnostics: `local_diagnostics` of every rank summed by one
+    all-reduce (the local values when torch.distributed is not initialised).
+    Every rank must call it at the same point, with species in the same
+    order.  Returns {"buffered": {name: n}, "alive": {name: n},
+    "particle_steps": n, "spectrum": counts[bins], "spectrum_range": (lo, hi)}."""
+    v = local_diagnostics(species, particle_steps, bins, lo, hi)
+    if _dist_on():
+        import torch
+        import torch.distributed as dist
+        t = torch.as_tensor(v, dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        v = t.cpu().numpy()
+    n = len(species)
+    names = [p.name for p in species]
+    return {"buffered": {nm: float(v[2 * i]) for i, nm in enumerate(names)},
+            "alive": {nm: float(v[2 * i + 1]) for i, nm in enumerate(names)},
+            "particle_steps": float(v[2 * n]), "spectrum": np.asarray(v[2 * n + 1:]), "spectrum_range": (lo, hi)}
+
+
+class JobDiagnostics:
+    """A Simulation ``monitor``: at every ``print_every`` boundary and at the
+    end of ``start`` it reduces the counters and the photon spectrum over
+    the ranks (``reduce_diagnostics``) and keeps (step, result) in
+    ``history`` on every rank.  Every rank's Simulation must run the same
+    steps with the same ``print_every``, so that the ranks reduce together."""
+
+    def __init__(self, bins: int = 64, lo: float = 2.0, hi: float = 2500.0, device=None):
+        self.bins, self.lo, self.hi, self.device = bins, lo, hi, device
+        self.history = []
+
+    def __call__(self, sim):
+        r = reduce_diagnostics(sim.all_particles, sim.particle_steps, self.bins, self.lo, self.hi, self.device)
+        self.history.append((sim.step, r))
+        return r

@@ -36,6 +36,10 @@ Extra keyword arguments (no reference counterpart):
                  the reference) or 'mlp', the learned photon-energy sampler
                  (sfparticles_b200.mlp) evaluated on the tensor cores inside
                  the step;
+  monitor     -- a callable monitor(sim), run at every print_every
+                 boundary and at the end of start(); shard.JobDiagnostics
+                 reduces the counters and the photon spectrum over the ranks
+                 of a multi-GPU job there;
   engine      -- 'fused' (the persistent step kernels) or 'ops': the
                  reference's own step loop (simulation.py:102-144) over the
                  one-for-one kernels of the C-ABI (float64, materialised
@@ -123,7 +127,7 @@ class Simulation(object):
     def __init__(self, *all_particles: Particles, dt: float, fields: Fields, print_every: int = 100, t0=0.0,
                  photon_threshold=2.0, seed: int = None, form: str = "fp64", graph_chunk: int = 64,
                  m_stages: int = 0, min_blocks: int = 0, p_stages: int = 0, p_min_blocks: int = 0,
-                 engine: str = "fused", sampler: str = "table") -> None:
+                 engine: str = "fused", sampler: str = "table", monitor: Callable = None) -> None:
         self.all_particles = all_particles
         self.particles_push = []
         self.particles_bw = []
@@ -150,6 +154,7 @@ class Simulation(object):
             raise ValueError("the learned photon-energy sampler runs in the fused engine")
         self.sampler = sampler
         self.graph_chunk = int(graph_chunk)
+        self.monitor = monitor
         self.m_stages = int(m_stages)  # massive kernel: depth of the copy ring (0: the form's default)
         self.min_blocks = int(min_blocks)  # massive kernel: resident blocks per SM (0: default)
         self.p_stages = int(p_stages)  # photon kernel: depth of the copy ring (0: default)
@@ -315,6 +320,8 @@ class Simulation(object):
                 self._loop(self._run, nstep, call_back)
             finally:
                 self._end()
+        if self.monitor is not None:
+            self.monitor(self)
         for p in self.all_particles:
             p._prune()
             p._to_host()
@@ -356,8 +363,11 @@ class Simulation(object):
             self.t += dt
             self.step += 1
             self._record()
-            if self.print_every and self.step % self.print_every == 0 and self.progress_bar is not None:
-                self.progress_bar.update(self.print_every)
+            if self.print_every and self.step % self.print_every == 0:
+                if self.progress_bar is not None:
+                    self.progress_bar.update(self.print_every)
+                if self.monitor is not None:
+                    self.monitor(self)
 
     # -- device-resident driving (start() = _begin + _loop + _end + prune) --
     def _begin(self):
@@ -515,6 +525,8 @@ class Simulation(object):
                 particle_num_str = ','.join([f"{p.Npart} {p.name}" for p in self.all_particles])
                 self.progress_bar.set_postfix_str(f"{particle_num_str}, {ns_per_particle:.0f}ns/particle")
                 self.progress_bar.update(self.print_every)
+            if self.step % self.print_every == 0 and self.monitor is not None:
+                self.monitor(self)
 
     def _sync_state(self, run, st, nbuf) -> int:
         """Read the run's state into the species; returns the steps completed

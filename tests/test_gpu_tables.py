@@ -1,0 +1,69 @@
+"""The QED rate tables generated on the GPU (sfp_table_rs / sfp_table_od,
+csrc/sfp_tables.cu) against the reference's own entries and the package's
+build-time tables.
+
+The reference builds its tables with scipy (qed/rejection_sampling_tables.py:
+80-112, qed/optical_depth_tables.py:126-230); the GPU generator runs the
+same quadrature algorithm with the package's own Airy functions.  Bound:
+1e-12 relative on every entry above 1e-250 (rates in 1/s; below it the
+reference's scipy flushes Airy values to zero, and both are negligible).
+The reference's optical-depth pair rows below chi ~ 0.43 are NaN (scipy's
+airy fails at z ~ 1e8); there the GPU rows are compared with the package's
+build-time rows, which take the Airy terms as 0 from z = 108 on.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+from gpu_helpers import cuda_or_skip
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel_above_floor(got, ref, floor=1e-250):
+    got, ref = np.asarray(got, float), np.asarray(ref, float)
+    big = np.abs(ref) > floor
+    assert np.all(np.abs(got[~big]) <= floor)
+    return float(np.max(np.abs(got[big] - ref[big]) / np.abs(ref[big]))) if big.any() else 0.0
+
+
+def test_gpu_tables_match_the_reference_rows():
+    cuda_or_skip()
+    from sfparticles_b200.qed import tables as T
+    o = golden("ref_od.npz")
+    rs, od = T.generate_on_gpu(chi=o["chi_rows"])
+    g = golden("ref_tables.npz")
+    e_ia, e_da = _rel_above_floor(rs["int_Ai"], g["int_Ai"]), _rel_above_floor(rs["Aip"], g["Aip"])
+    print(f"rejection sampling: int_Ai {e_ia:.2e}, Ai' {e_da:.2e}")
+    assert e_ia < 1e-12 and e_da < 1e-12
+    worst = 0.0
+    for j in range(len(o["chi_rows"])):
+        worst = max(worst, _rel_above_floor(od["photon_rate_total"][j:j + 1], o["photon_total"][j:j + 1]),
+                    _rel_above_floor(od["photon_cumulative"][j], o["photon_cum"][j]),
+                    _rel_above_floor(od["pair_rate_total"][j:j + 1], o["pair_total"][j:j + 1]))
+        if np.isfinite(o["pair_cum"][j]).all():
+            worst = max(worst, _rel_above_floor(od["pair_cumulative"][j], o["pair_cum"][j]))
+    print(f"optical depth, 18 reference rows: worst {worst:.2e}")
+    assert worst < 1e-12
+
+
+def test_gpu_tables_match_the_build_time_tables():
+    """All 307 rows of both species and the full rejection-sampling table."""
+    cuda_or_skip()
+    import time
+    import torch
+    from sfparticles_b200.qed import tables as T
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rs, od = T.generate_on_gpu()
+    torch.cuda.synchronize()
+    print(f"both table families on the GPU: {time.perf_counter() - t0:.2f} s")
+    iA, dA, _, _ = T.rs_tables()
+    assert _rel_above_floor(rs["int_Ai"], iA) < 1e-12 and _rel_above_floor(rs["Aip"], dA) < 1e-12
+    ref = T.od_tables()
+    assert np.array_equal(od["chi"], ref["chi"])
+    for k in ("photon_rate_total", "pair_rate_total", "photon_cumulative", "pair_cumulative"):
+        assert np.isfinite(od[k]).all(), k
+        err = max(_rel_above_floor(a, b) for a, b in zip(np.atleast_2d(od[k]), np.atleast_2d(ref[k])))
+        print(f"{k}: worst {err:.2e}")
+        assert err < 1e-12, k

@@ -51,14 +51,21 @@ def test_noalloc_matches_workspace_entry_on_two_calls_in_a_row():
     evs = [_events(n, d, gen) for n, d in cases]
     n_events = [int(e.sum().item()) for e in evs]
     outs = [torch.full((max(k, 1),), -1, dtype=torch.int64, device="cuda") for k in n_events]
+    # set-up call (N = 0): looks up the scratch address, loading the module if needed;
+    # then one small call, so that the kernels' code is loaded before memory is measured
+    _lib.check(L.sfp_find_event_index_noalloc(_p(evs[0]), 0, 0, _p(outs[0]), stream), "set-up")
+    warm = torch.empty(max(n_events[1], 1), dtype=torch.int64, device="cuda")
+    _lib.check(L.sfp_find_event_index_noalloc(_p(evs[1]), n_events[1], evs[1].numel(), _p(warm), stream), "warm")
     torch.cuda.synchronize()
-    free0 = torch.cuda.mem_get_info()[0]
+    free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
     for ev, k, out in zip(evs, n_events, outs):  # two calls in a row, one stream, no sync between
         _lib.check(L.sfp_find_event_index_noalloc(_p(ev), k, ev.numel(), _p(out), stream),
                    "sfp_find_event_index_noalloc")
     torch.cuda.synchronize()
-    free1 = torch.cuda.mem_get_info()[0]
-    print(f"device free memory across the two no-alloc calls: {free0} -> {free1} bytes")
+    free1, alloc1 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+    # nothing was allocated: neither through torch nor from the driver
+    assert alloc1 == alloc0, (alloc0, alloc1)
+    assert free1 == free0, (free0, free1)
     for ev, k, out in zip(evs, n_events, outs):
         ref = _with_workspace(L, ev, k, stream)
         truth = torch.nonzero(ev).flatten()
