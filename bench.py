@@ -399,19 +399,22 @@ def run_c5(args):
 
 
 WORKLOAD_OPS = "the reference's step loop over the one-for-one float64 kernels (engine 'ops'): the scaled-cascade " \
-               "beam at the given electron count, from step 0"
+               "beam at the given electron count, over the window that config.start_step opens"
 
 
 def run_ops(args):
     """The plain float64 path on its own: particle-steps/s of the per-op
-    kernels (each launched once per species per step, fields materialised)."""
+    kernels (each launched once per species per step, fields materialised),
+    over the same window as the default line (advanced to it untimed, the
+    last `--warmup` steps of the advance serving as warm-up)."""
     import torch
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     sim = make_sim(args.electrons, 1000, "fp64", engine="ops")
     for p in sim.all_particles:
         p._to_gpu()
-    sim._loop_ops(args.warmup, None)
+    S0 = max(window_start(args), args.warmup)
+    sim._loop_ops(S0, None)
     torch.cuda.synchronize()
     ps0 = sim.particle_steps
     e0 = torch.cuda.Event(enable_timing=True)
@@ -428,7 +431,8 @@ def run_ops(args):
     line = {"metric": "particle-steps/s", "value": ps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_OPS, "electrons": args.electrons,
+            "config": {"workload": WORKLOAD_OPS, "electrons": args.electrons, "start_step": S0,
+                       "steps_timed": args.steps,
                        "l2": "80 MB per array at 1e7 electrons, larger than L2 for every kernel"},
             "roofline": None, "cpu_baseline": None, "e2e": None, "clocks": clk.summary(), "particle_steps": ps}
     print(json.dumps(line), flush=True)

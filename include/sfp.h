@@ -233,6 +233,11 @@ int sfp_mlp_infer_warp(const float *params, const double *log_chi, const double 
 /* synchronous: 1 if an sfp_mlp_infer launch on the current device gave up
  * waiting for its tensor cores since the last call, else 0; clears it */
 int sfp_mlp_device_error(int *code);
+/* test hook of that failure path: sfp_mlp_infer with every MMA and commit
+ * withheld, so each block's first wait runs out (after one second), sets the
+ * flag, frees its tensor memory and returns; delta is left unwritten */
+int sfp_mlp_infer_withheld(const float *params, const double *log_chi, const double *u, double *delta, int64_t N,
+                           void *stream);
 
 /* ---- QED rate tables generated on the GPU --------------------------------
  * The reference's table generators (qed/rejection_sampling_tables.py:80-112,

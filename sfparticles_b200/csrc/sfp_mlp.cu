@@ -391,9 +391,10 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ P, 
 // Shared-memory operands use the K-major layout without swizzle: 8 x 8 BF16
 // core matrices of 128 B, element (r, k) at (r/8) (K/8) 128 + (k/8) 128 +
 // (r%8) 16 + (k%8) 2 (leading-dimension byte offset 128, stride-dimension
-// byte offset (K/8) 128).  Every wait on the MMA barrier is bounded; on
-// timeout the block sets g_mlp_tc_error, stops, and still frees its tensor
-// memory.
+// byte offset (K/8) 128).  Every wait on the MMA barrier is bounded (one
+// second); on timeout the block sets g_mlp_tc_error, stops, and still frees
+// its tensor memory.  `withhold` (a test of that path) issues no MMA and no
+// commit, so the first wait runs out.
 namespace tc {
 
 constexpr int TM = 128;  // queries per tile (the MMA's M)
@@ -405,7 +406,10 @@ constexpr unsigned TMEM_COLS = 64;
 // (bits 7-9 = 1) and B (bits 10-12 = 1), both K-major, N = 64 (bits 17-22 =
 // N/8), M = 128 (bits 24-28 = M/16)
 constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
-constexpr long long WAIT_LIMIT = 1ll << 22;
+// bound of every wait on the MMA barrier: one second, far above the
+// microseconds an MMA group takes
+constexpr unsigned long long WAIT_NS = 1000000000ull;
+constexpr long long WAIT_TRIES = 1ll << 30;
 
 struct Smem {
     alignas(128) unsigned char B0[64 * K0 * 2];
@@ -440,8 +444,16 @@ __device__ __forceinline__ void commit(unsigned mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
 }
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// true once the barrier has completed the given phase; false after WAIT_NS
+// nanoseconds (or WAIT_TRIES polls, whichever comes first)
 __device__ __forceinline__ bool wait_phase(unsigned mbar, unsigned phase) {
-    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    const unsigned long long t0 = now_ns();
+    for (long long i = 0; i < WAIT_TRIES; ++i) {
         unsigned ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -449,6 +461,7 @@ __device__ __forceinline__ bool wait_phase(unsigned mbar, unsigned phase) {
             : "r"(mbar), "r"(phase)
             : "memory");
         if (ok) return true;
+        if (now_ns() - t0 > WAIT_NS) return false;
     }
     return false;
 }
@@ -497,7 +510,7 @@ __device__ int g_mlp_tc_error;
 
 __global__ void __launch_bounds__(128, 4) k_mlp_infer_tc(const float* __restrict__ P, const double* __restrict__ lc,
                                                          const double* __restrict__ u, double* __restrict__ out,
-                                                         long long n) {
+                                                         long long n, int withhold) {
     using namespace tc;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
@@ -582,7 +595,7 @@ __global__ void __launch_bounds__(128, 4) k_mlp_infer_tc(const float* __restrict
             fence_smem_async();
             fence_before();
             __syncthreads();  // A written, D of the previous layer read
-            if (tid == 0) {
+            if (tid == 0 && !withhold) {
                 fence_after();
                 if (layer == 0) {
                     mma(tmem, dA0, dB0, 0u);
@@ -596,8 +609,8 @@ __global__ void __launch_bounds__(128, 4) k_mlp_infer_tc(const float* __restrict
                 commit(mbar);
             }
             ok = __syncthreads_and(wait_phase(mbar, phase)) != 0;
+            if (!ok) break;  // phase stays the one of the commit still outstanding
             phase ^= 1u;
-            if (!ok) break;
             fence_after();
             float v[64];
 #pragma unroll
@@ -703,9 +716,14 @@ int sfp_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t s
     return SFP_OK;
 }
 
-int sfp_mlp_infer(const float* params, const double* log_chi, const double* u, double* delta, int64_t N,
-                  void* stream) {
-    if (!params || (N > 0 && (!log_chi || !u || !delta))) return sfp_set_error(SFP_EINVAL, "sfp_mlp_infer: NULL argument");
+}  // extern "C"
+
+namespace {
+
+int mlp_infer_tc(const char* name, const float* params, const double* log_chi, const double* u, double* delta,
+                 int64_t N, void* stream, int withhold) {
+    if (!params || (N > 0 && (!log_chi || !u || !delta)))
+        return sfp_set_error(SFP_EINVAL, std::string(name) + ": NULL argument");
     if (N <= 0) return SFP_OK;
     static int attr_dev = -1;
     int dev = 0;
@@ -719,9 +737,23 @@ int sfp_mlp_infer(const float* params, const double* log_chi, const double* u, d
     const long long cap = (long long)sm_count_here() * 4;  // four CTAs (4 x 64 tensor-memory columns) per SM
     const long long grid = tiles < cap ? tiles : cap;
     k_mlp_infer_tc<<<(unsigned)grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(params, log_chi, u, delta,
-                                                                                        N);
+                                                                                        N, withhold);
     MLP_CUDA(cudaGetLastError());
     return SFP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfp_mlp_infer(const float* params, const double* log_chi, const double* u, double* delta, int64_t N,
+                  void* stream) {
+    return mlp_infer_tc("sfp_mlp_infer", params, log_chi, u, delta, N, stream, 0);
+}
+
+int sfp_mlp_infer_withheld(const float* params, const double* log_chi, const double* u, double* delta, int64_t N,
+                           void* stream) {
+    return mlp_infer_tc("sfp_mlp_infer_withheld", params, log_chi, u, delta, N, stream, 1);
 }
 
 int sfp_mlp_infer_warp(const float* params, const double* log_chi, const double* u, double* delta, int64_t N,

@@ -123,6 +123,40 @@ def test_inference_kernel_matches_oracle():
 
 
 @pytest.mark.gpu
+def test_tensor_core_wait_runs_out_and_the_context_stays_usable():
+    """The tcgen05 kernel's bounded wait on its MMA barrier: with the MMAs
+    and their commit withheld (sfp_mlp_infer_withheld) nothing ever arrives
+    on the barrier, each block gives up after its one-second limit, sets the
+    device error flag, frees its tensor memory and returns with its outputs
+    unwritten.  The next launch on the same context then runs normally."""
+    _gpu()
+    import time
+    import torch
+    from sfparticles_b200 import _lib, mlp
+    s = mlp.PhotonSampler(mlp.init_params(4))
+    rng = np.random.default_rng(9)
+    n = 3 * 128 + 5  # four blocks
+    lc = torch.as_tensor(rng.uniform(-3, 3, n), device="cuda")
+    u = torch.as_tensor(rng.uniform(0, 1, n), device="cuda")
+    assert mlp.PhotonSampler.device_error() == 0
+    out = torch.full((n,), -7.0, dtype=torch.float64, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    t0 = time.perf_counter()
+    _lib.call("sfp_mlp_infer_withheld", p(s.params), p(lc), p(u), p(out), n, stream)
+    assert mlp.PhotonSampler.device_error() == 1  # synchronises: the launch has returned
+    waited = time.perf_counter() - t0
+    print(f"withheld launch returned after {waited:.2f} s")
+    assert 0.9 < waited < 10.0
+    assert bool((out == -7.0).all())  # nothing written
+    assert mlp.PhotonSampler.device_error() == 0  # read once, then cleared
+    got = s.sample(lc, u).cpu().numpy()
+    ref = mo.forward_infer(s.params.cpu().numpy(), lc.cpu().numpy(), u.cpu().numpy())
+    assert np.abs(np.log10(got) - np.log10(ref)).max() < 2e-2
+    assert mlp.PhotonSampler.device_error() == 0
+
+
+@pytest.mark.gpu
 def test_training_reduces_the_loss():
     """A short run of the training loop (2e6 samples, 2 epochs) lowers the
     mean squared error by more than 10x from the initial network's."""
