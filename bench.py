@@ -68,9 +68,9 @@ def window_label(start, steps):
         if start < STEPS_FULL // 2 < start + steps else "")
 
 
-def beam(n, seed, steps=STEPS_FULL):
+def beam(n, seed, steps=STEPS_FULL, dt=DT):
     rng = np.random.default_rng(seed)
-    L = C * (steps * DT) / 2
+    L = C * (steps * dt) / 2
     g = GAMMA0 * (1 + 0.01 * rng.normal(size=n))
     x = rng.normal(-L, 5e-6, n)
     y = rng.normal(0, 1e-6, n)
@@ -78,12 +78,15 @@ def beam(n, seed, steps=STEPS_FULL):
     return (x, y, z, np.sqrt(g * g - 1), np.zeros(n), np.zeros(n)), L
 
 
-def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64, engine="fused", share=None):
+def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64, engine="fused", share=None,
+             a0=A0, dt=DT, steps=STEPS_FULL):
     """The scaled cascade with `n` electrons drawn from `seed`; `share` =
-    (start, count) keeps that slice of the beam (Philox key `seed` either way)."""
+    (start, count) keeps that slice of the beam (Philox key `seed` either way).
+    a0, dt, steps: the pulse amplitude, the time step and the run length the
+    beam's offset is set for (the plain config: a0=50, dt=T0/50, 1500)."""
     import sfparticles_b200 as S
     from sfparticles_b200.fields import gaussian_laser_pulse
-    props, L = beam(n, seed)
+    props, L = beam(n, seed, steps, dt)
     if share is not None:
         a, c = share
         props = tuple(np.ascontiguousarray(v[a:a + c]) for v in props)
@@ -94,8 +97,8 @@ def make_sim(n, seed, form="fp64", massive=(0, 0), photon=(0, 0), graph_chunk=64
     ele.set_photon(pho)
     pos.set_photon(pho)
     pho.set_pair(ele, pos)
-    fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
-    sim = S.Simulation(ele, pos, pho, dt=DT, fields=fld, print_every=None, seed=seed, form=form,
+    fld = gaussian_laser_pulse(a0, W0, CTAU, direction=-1, x0=L)
+    sim = S.Simulation(ele, pos, pho, dt=dt, fields=fld, print_every=None, seed=seed, form=form,
                        m_stages=massive[0], min_blocks=massive[1], p_stages=photon[0], p_min_blocks=photon[1],
                        graph_chunk=graph_chunk, engine=engine)
     return sim
@@ -299,8 +302,39 @@ def run_c3(args):
             "accuracy_vs_table": acc,
             "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 8 * n},
-            "cpu_baseline": None, "gpu_launches": 2 * (args.steps + args.warmup), "clocks": clk_summary}
+            "cpu_baseline": None if args.no_cpu else c3_cpu_baseline(lc, u, mlp), "gpu_launches": args.steps,
+            "clocks": clk_summary}
     print(json.dumps(line), flush=True)
+
+
+def c3_cpu_baseline(lc, u, mlp, m=1_000_000, budget_s=10.0):
+    """The oracle's restatement of the reference's inverse-CDF bisection
+    (_bisect_interp, optical_depth_tables.py:59-102; C, OpenMP, all host
+    threads) on the first `m` queries of the same batch, checked against the
+    GPU table sampler on them."""
+    import ctypes
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    tab = orc.make_od_table(d["photon_rate_total"], d["photon_cumulative"], float(d["log_chi_min"]),
+                            float(d["log_chi_delta"]), float(d["log_delta_min"]), float(d["log_delta_delta"]))
+    a = np.ascontiguousarray(lc[:m].cpu().numpy())
+    b = np.ascontiguousarray(u[:m].cpu().numpy())
+    out = np.empty(m)
+    L = orc.lib()
+    L.orc_od_bisect_batch(orc._p(a), orc._p(b), m, ctypes.byref(tab), orc._p(out))  # warm-up
+    reps = 0
+    t0 = time.perf_counter()
+    while reps < 3 or (time.perf_counter() - t0 < budget_s and reps < 50):
+        L.orc_od_bisect_batch(orc._p(a), orc._p(b), m, ctypes.byref(tab), orc._p(out))
+        reps += 1
+    dt = time.perf_counter() - t0
+    gpu = mlp.sample_table(lc[:m], u[:m]).cpu().numpy()
+    return {"value": m * reps / dt, "unit": "samples/s", "cores": omp_threads(), "kind": "port",
+            "sample": f"{m} queries of the same batch, {reps} passes in {dt:.2f} s, through the oracle's "
+                      "_bisect_interp (the table sampler the network replaces)",
+            "max_rel_diff_vs_gpu_table_sampler": float(np.max(np.abs(gpu - out) / np.abs(out)))}
 
 
 WORKLOAD_C5 = "spin + radiation-reaction avalanche: 5e6 e- at rest (uniform 2um cube, spin +z) between two " \
@@ -438,11 +472,276 @@ def run_ops(args):
     print(json.dumps(line), flush=True)
 
 
-def make_oracle_sim(n, seed):
+WORKLOAD_C1 = "plain method, small: 1e4 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=50 " \
+              "(0.8um, w0 3um, 25fs FWHM), photons + pairs, float64, dt=T0/50, 1500 steps, beam seed 0; the whole run"
+C1_N, C1_A0, C1_DT, C1_STEPS = 10_000, 50.0, T0 / 50, 1500
+
+
+def run_c1(args):
+    """The plain config at full size in float64 (the reference arithmetic):
+    the whole 1500-step run device-resident (CUDA events), the same run
+    through Simulation.start from host arrays (e2e), and the oracle port on
+    the same run on the host cores beside it.  The state (<30 MB) sits in
+    L2: the run is launch- and latency-bound, so no roofline is claimed."""
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    kw = dict(a0=C1_A0, dt=C1_DT, steps=C1_STEPS)
+    w = make_sim(1000, 1, "fp64", **kw)  # warm-up: module load, graphs
+    w.run_on_device(max(args.warmup, 3))
+    w.finish()
+    del w
+    sim = make_sim(C1_N, 0, "fp64", **kw)
+    sim._begin()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ps0, l0 = sim.particle_steps, sim.kernel_launches
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        e0.record()
+        sim.run_on_device(C1_STEPS)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ps = sim.particle_steps - ps0
+    launches = sim.kernel_launches - l0
+    counts = {p.name: p.N_buffered for p in sim.all_particles}
+    sim._end()
+    del sim
+    _release()
+    # end to end: Simulation.start from host arrays, results back in host arrays
+    sim2 = make_sim(C1_N, 0, "fp64", **kw)
+    h2d = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    sim2.start(C1_STEPS)
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    d2h = sum(a.nbytes for p in sim2.all_particles for a in p._arr.values())
+    e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
+    e2e = {"value": sim2.particle_steps / (e2e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "wall_s": wall, "note": "one step = the whole 1500-step run"}
+    del sim2
+    cpu = None
+    if not args.no_cpu:
+        osim = make_oracle_sim(C1_N, 0, **kw)
+        t0 = time.perf_counter()
+        osim.run(C1_STEPS)
+        dt_cpu = time.perf_counter() - t0
+        osim_counts = {p.name: p.N_buffered for p in osim.all}
+        cpu = {"value": osim.particle_steps / dt_cpu, "unit": "particle-steps/s", "cores": omp_threads(),
+               "kind": "port", "sample": f"the full run: {osim.particle_steps:.3g} particle-steps in {dt_cpu:.2f} s",
+               "final_counts": osim_counts}
+    line = {"metric": "particle-steps/s", "value": ps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": C1_STEPS, "warmup": max(args.warmup, 3), "ms_per_step": ms / C1_STEPS, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_C1, "electrons": C1_N, "form": "fp64", "final_counts": counts,
+                       "l2": "the whole state (<30 MB) is L2-resident: launch- and latency-bound, no flush"},
+            "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+            "particle_steps": ps}
+    print(json.dumps(line), flush=True)
+
+
+WORKLOAD_KERNELS ="the per-op kernels one by one (the reference's one-for-one kernel boundary): N e- and N photons " \
+                   "at the collision (beam and pulse centred on the focus at t = 0, gamma0 2000 +-1%, photons at " \
+                   "gamma 500 along the beam, a0 200), float64 state; the learned sampler's training kernels on " \
+                   "2^22 samples"
+
+# algorithmic bytes of each per-op kernel: (per particle, per event); an
+# element is 8 B, a flag 1 B; see the kernels in csrc/sfp_capi.cu
+KERNEL_BYTES = {
+    "sfp_field_eval_kernel": (73, 0),   # x,y,z (24) + flag (1) read, 6 components written (48)
+    "k_update_chi": (89, 0),            # 6 components, u, 1/gamma (80) + flag read, chi written
+    "k_rs": (26, 0),                    # flag, chi, 1/gamma read (17), event + delta written (9)
+    "k_pick_hard": (1, 16),             # event read; per event delta + 1/gamma read
+    "k_bool_sum": (1, 0),
+    "k_fei": (2, 8),                    # count + scatter passes read the events, indices written
+    "k_create_photon": (0, 121),        # index, parent x,u, delta read (64), photon x,u,1/gamma + flag written (57)
+    "k_photon_recoil": (2, 64),         # flag + event; per event delta (8), u r/w (48), 1/gamma written
+    "k_push_position": (81, 0),         # flag, x,y,z r/w (48), u, 1/gamma read (32)
+    "k_boris": (105, 0),                # flag, 6 components (48), u r/w (48), 1/gamma written
+    "k_ll": (73, 0),                    # flag, u r/w (48), 1/gamma r/w (16), chi read
+    "k_boris_tbmt": (153, 0),           # k_boris + spin r/w (48)
+    "k_update_tau": (42, 0),            # flag, tau r/w (16), 1/gamma, chi read (16), event + delta written
+    "k_inv_gamma": (32, 0),
+    "k_create_pair": (0, 122),          # as k_create_photon + the photon's flag written
+}
+
+
+def run_kernels(args):
+    """Each per-op entry point launched alone, CUDA events around every
+    launch (median of 5 after 2 warm-ups), achieved GB/s from its
+    algorithmic bytes against the measured HBM peak.  Under an NVTX range
+    "kernels" so profilers can select these launches."""
+    import ctypes
+    import torch
+    from sfparticles_b200 import _lib, mlp, program
+    from sfparticles_b200.fields import gaussian_laser_pulse
+    from sfparticles_b200.qed import device_tables
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    HBM_PEAK, HBM_PEAK_KIND = measured_peak_hbm()
+    n = args.electrons
+    rng = np.random.default_rng(7)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    g = GAMMA0 * (1 + 0.01 * rng.normal(size=n))
+    e = {"x": T(rng.normal(0, 2e-6, n)), "y": T(rng.normal(0, 1e-6, n)), "z": T(rng.normal(0, 1e-6, n)),
+         "ux": T(np.sqrt(g * g - 1)), "uy": T(np.zeros(n)), "uz": T(np.zeros(n))}
+    e["ig"] = 1.0 / torch.sqrt(1.0 + e["ux"] ** 2)
+    ph = {"x": T(rng.normal(0, 2e-6, n)), "y": T(rng.normal(0, 1e-6, n)), "z": T(rng.normal(0, 1e-6, n)),
+          "ux": T(np.full(n, 500.0)), "uy": T(np.zeros(n)), "uz": T(np.zeros(n))}
+    ph["ig"] = 1.0 / ph["ux"]
+    for d in (e, ph):
+        for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "chi", "delta"):
+            d[k] = torch.zeros(n, dtype=torch.float64, device=dev)
+        d["pr"] = torch.zeros(n, dtype=torch.uint8, device=dev)
+        d["ev"] = torch.zeros(n, dtype=torch.uint8, device=dev)
+    e["tau"] = T(rng.exponential(size=n))
+    spin = {k: T(v) for k, v in (("sx", np.zeros(n)), ("sy", np.zeros(n)), ("sz", np.ones(n)))}
+    dst = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ("x", "y", "z", "ux", "uy", "uz", "ig")}
+    dst["pr"] = torch.empty(n, dtype=torch.uint8, device=dev)
+    fld = gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=0.0)
+    mod = program.get_module(fld, form=None, qed=None)
+    prm = fld.params_device(dev)
+    rs = device_tables.rs_table(dev)
+    od_ph, _ = device_tables.od_tables(dev)
+    ws = torch.empty(int(_lib.load().sfp_find_event_index_workspace(n)) + 8, dtype=torch.uint8, device=dev)
+    idx = torch.empty(n, dtype=torch.int64, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    F = lambda d: [P(d[k]) for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz")]  # noqa: E731
+    U = lambda d: [P(d[k]) for k in ("ux", "uy", "uz")]  # noqa: E731
+    X = lambda d: [P(d[k]) for k in ("x", "y", "z")]  # noqa: E731
+    q = -1.602176634e-19
+    rows = []
+    n_ev = {"e": 0, "ph": 0}
+
+    def count(d):
+        cnt.zero_()
+        _lib.call("sfp_bool_sum", P(d["ev"]), n, P(cnt), st)
+        return int(cnt.item())
+
+    def fei(d, key):
+        k = n_ev[key]
+        _lib.call("sfp_find_event_index", P(d["ev"]), k, n, P(idx), P(ws), ws.numel(), st)
+
+    def timed(name, fn, events=0, reps=5, bytes_name=None):
+        for _ in range(2):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        torch.cuda.synchronize()
+        for a, b in ev:
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        ms = float(np.median([a.elapsed_time(b) for a, b in ev]))
+        per, per_ev = KERNEL_BYTES[bytes_name or name]
+        alg = per * n + per_ev * events
+        gbs = alg / (ms * 1e-3) / 1e9
+        rows.append({"kernel": name, "ms": ms, "alg_bytes": alg, "events": events, "achieved_gbs": gbs,
+                     "frac": gbs / HBM_PEAK})
+
+    torch.cuda.nvtx.range_push("kernels")
+    # the e- side of a step at the pulse's peak
+    timed("sfp_field_eval_kernel", lambda: _lib.call("sfp_field_eval", mod.handle, P(prm), *X(e), 0.0, n, P(e["pr"]),
+                                                     *F(e), st))
+    timed("k_update_chi", lambda: _lib.call("sfp_update_chi", *F(e), *U(e), P(e["ig"]), P(e["chi"]), n, P(e["pr"]),
+                                            st))
+    timed("k_rs", lambda: _lib.call("sfp_photon_from_rejection_sampling", P(e["ig"]), P(e["chi"]), DT, n,
+                                    P(e["pr"]), P(e["ev"]), P(e["delta"]), ctypes.byref(rs), 1, 0, 7, st))
+    n_ev["e"] = count(e)
+    e_ev_all = e["ev"].clone()
+    timed("k_pick_hard", lambda: (e["ev"].copy_(e_ev_all), _lib.call("sfp_pick_hard_photon", P(e["ev"]),
+                                                                   P(e["delta"]), P(e["ig"]), 2.0, n, st))[1],
+          events=n_ev["e"])
+    n_ev["e"] = count(e)
+    timed("k_bool_sum", lambda: _lib.call("sfp_bool_sum", P(e["ev"]), n, P(cnt), st))
+    timed("k_fei", lambda: fei(e, "e"), events=n_ev["e"])
+    fei(e, "e")
+    k = n_ev["e"]
+    timed("k_create_photon", lambda: _lib.call("sfp_create_photon", *X(e), *U(e), *X(dst), *U(dst), P(dst["ig"]),
+                                               P(dst["pr"]), P(idx), P(e["delta"]), 0, k, st), events=k)
+    timed("k_photon_recoil", lambda: _lib.call("sfp_photon_recoil", *U(e), P(e["ig"]), P(e["ev"]), P(e["delta"]),
+                                               n, P(e["pr"]), st), events=k)
+    timed("k_push_position", lambda: _lib.call("sfp_push_position", *X(e), *U(e), P(e["ig"]), n, P(e["pr"]),
+                                               DT / 2, st))
+    timed("k_boris", lambda: _lib.call("sfp_boris", *U(e), P(e["ig"]), *F(e), q, n, P(e["pr"]), DT, st))
+    timed("k_ll(LL)", lambda: _lib.call("sfp_LL_push", *U(e), P(e["ig"]), P(e["chi"]), n, P(e["pr"]), DT, st),
+          bytes_name="k_ll")
+    timed("k_ll(CLL)", lambda: _lib.call("sfp_CLL_push", *U(e), P(e["ig"]), P(e["chi"]), n, P(e["pr"]), DT, st),
+          bytes_name="k_ll")
+    timed("k_boris_tbmt", lambda: _lib.call("sfp_boris_tbmt", *U(e), P(e["ig"]), P(spin["sx"]), P(spin["sy"]),
+                                            P(spin["sz"]), *F(e), q, 1.14e-3, n, P(e["pr"]), DT, st))
+    timed("k_update_tau", lambda: _lib.call("sfp_update_tau", P(e["tau"]), P(e["ig"]), P(e["chi"]), DT, n,
+                                            P(e["pr"]), P(e["ev"]), P(e["delta"]), ctypes.byref(od_ph), 1, 0, 7, st))
+    timed("k_inv_gamma", lambda: _lib.call("sfp_inv_gamma", *U(e), P(e["ig"]), n, 0, st))
+    # the photon side: fields, chi, pair events, the pairs
+    _lib.call("sfp_field_eval", mod.handle, P(prm), *X(ph), 0.0, n, P(ph["pr"]), *F(ph), st)
+    _lib.call("sfp_update_chi", *F(ph), *U(ph), P(ph["ig"]), P(ph["chi"]), n, P(ph["pr"]), st)
+    timed("k_rs(pair)", lambda: _lib.call("sfp_pair_from_rejection_sampling", P(ph["ig"]), P(ph["chi"]), DT, n,
+                                          P(ph["pr"]), P(ph["ev"]), P(ph["delta"]), ctypes.byref(rs), 1, 2, 7, st),
+          bytes_name="k_rs")
+    n_ev["ph"] = count(ph)
+    fei(ph, "ph")
+    kp = n_ev["ph"]
+    pr0 = ph["pr"].clone()
+    timed("k_create_pair", lambda: (ph["pr"].copy_(pr0),
+                                    _lib.call("sfp_create_pair", *X(ph), *U(ph), P(ph["pr"]), *X(dst), *U(dst),
+                                              P(dst["ig"]), P(dst["pr"]), P(idx), P(ph["delta"]), 0, kp, 0, st))[1],
+          events=kp)
+    # the learned sampler's training kernels
+    ns = 1 << 22
+    feats = torch.empty(ns * 2, dtype=torch.float32, device=dev)
+    targ = torch.empty(ns, dtype=torch.float32, device=dev)
+    tab = mlp._photon_table()
+    lo, hi = mlp.LOG_CHI_RANGE
+    params = torch.as_tensor(mlp.init_params(3), device=dev)
+    grad = torch.zeros_like(params)
+    m1, v1 = torch.zeros_like(params), torch.zeros_like(params)
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+    train = []
+
+    def ttime(name, fn, nbytes, flops=None):
+        for _ in range(2):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(5):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 5
+        r = {"kernel": name, "ms": ms, "alg_bytes": nbytes, "achieved_gbs": nbytes / (ms * 1e-3) / 1e9,
+             "frac": nbytes / (ms * 1e-3) / 1e9 / HBM_PEAK}
+        if flops:
+            r["tflops"] = flops / (ms * 1e-3) / 1e12
+        train.append(r)
+
+    ttime("k_mlp_samples", lambda: _lib.call("sfp_mlp_make_samples", ctypes.byref(tab), 1, 0, lo, hi, ns, P(feats),
+                                             P(targ), st), 12 * ns)
+    ttime("k_mlp_grad", lambda: _lib.call("sfp_mlp_grad", P(params), P(feats), P(targ), ns, P(grad), P(loss), st),
+          12 * ns, flops=3 * 16768 * ns)
+    ttime("k_mlp_adam", lambda: _lib.call("sfp_mlp_adam", P(params), P(grad), P(m1), P(v1), 1, 1e-3, 0.9, 0.999,
+                                          1e-8, 1.0, st), 28 * params.numel())
+    torch.cuda.nvtx.range_pop()
+    line = {"metric": "GB/s per kernel", "workload": "kernels", "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_KERNELS, "particles": n, "electron_events": n_ev["e"],
+                       "pair_events": n_ev["ph"],
+                       "l2": f"{n * 8 / 1e6:.0f} MB per array, every kernel's traffic larger than L2"},
+            "peak_gbs": HBM_PEAK, "peak_kind": HBM_PEAK_KIND, "kernels": rows, "training": train}
+    print(json.dumps(line), flush=True)
+
+
+def make_oracle_sim(n, seed, a0=A0, dt=DT, steps=STEPS_FULL):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as orc
     from sfparticles_b200.qed import tables
-    props, L = beam(n, seed)
+    props, L = beam(n, seed, steps, dt)
     ele = orc.Species("electron", -1, 1, N=n, props=props)
     pos = orc.Species("positron", 1, 1)
     pho = orc.Species("photon", 0, 0)
@@ -450,8 +749,8 @@ def make_oracle_sim(n, seed):
     pos.set_photon(pho)
     pho.set_pair(ele, pos)
     iA, dA, _, zmax = tables.rs_tables()
-    terms = orc.gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
-    return orc.OracleSim([ele, pos, pho], DT, terms, ("rs", iA, dA), seed=seed, z_max=zmax)
+    terms = orc.gaussian_laser_pulse(a0, W0, CTAU, direction=-1, x0=L)
+    return orc.OracleSim([ele, pos, pho], dt, terms, ("rs", iA, dA), seed=seed, z_max=zmax)
 
 
 def cpu_sample(n_e, start, max_steps, budget_s):
@@ -504,10 +803,15 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once sampling runs (short regions get samples)
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 3.0:
+                time.sleep(0.01)
+            self.rows.clear()
         except Exception:
             self.proc = None
         return self
@@ -778,10 +1082,11 @@ def main():
     ap.add_argument("--steps", type=int, default=STEPS_FULL)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "ops"],
-                    help="c2: the scaled cascade (default); c3: the learned photon-energy sampler on 5e7 "
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "ops", "kernels"],
+                    help="c1: the plain config (1e4 e-, float64, the whole run); c2: the scaled cascade (default); c3: the learned photon-energy sampler on 5e7 "
                          "queries per step; c4: 256 batched uneven instances (2000 steps); c5: the spin + "
-                         "radiation-reaction avalanche to 1e9 particles; ops: the per-op float64 kernels")
+                         "radiation-reaction avalanche to 1e9 particles; ops: the per-op float64 kernels; "
+                         "kernels: each per-op kernel launched alone (GB/s per kernel)")
     ap.add_argument("--queries", type=int, default=50_000_000, help="c3: queries per step")
     ap.add_argument("--electrons-c5", type=int, default=5_000_000, help="c5: electrons at rest")
     ap.add_argument("--particle-cap", type=int, default=1_000_000_000, help="c5: stop at this many particles")
@@ -819,6 +1124,20 @@ def main():
         if args.steps == STEPS_FULL:
             args.steps = 20
         run_c3(args)
+        return
+    if args.workload == "c1":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "c1",
+                              "unavailable": "the plain-config mode runs one GPU, product arm only"}))
+            return
+        run_c1(args)
+        return
+    if args.workload == "kernels":
+        if args.impl != "ours" or world != 1:
+            print(json.dumps({"impl": args.impl, "workload": "kernels",
+                              "unavailable": "the per-kernel mode runs one GPU, product arm only"}))
+            return
+        run_kernels(args)
         return
     if args.workload == "ops":
         if args.impl != "ours" or world != 1:

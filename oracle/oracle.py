@@ -98,6 +98,7 @@ def lib():
         L.orc_od_interp1d.restype = d
         L.orc_od_bisect.argtypes = [d, d, P]
         L.orc_od_bisect.restype = d
+        L.orc_od_bisect_batch.argtypes = [P, P, i64, P, P]
         L.orc_update_tau.argtypes = [P, P, P, d, i64, P, P, P, P, u64, u32, u32]
         _lib = L
     return _lib

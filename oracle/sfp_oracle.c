@@ -719,6 +719,13 @@ double orc_od_bisect(double chi, double r_uniform, const orc_od_table *t) {
     return dl + k * (r - y1);
 }
 
+/* _bisect_interp over a batch of (log10 chi, u) queries, OpenMP: the CPU
+ * counterpart of the batched table sampler (optical_depth_tables.py:59-102) */
+void orc_od_bisect_batch(const double *log_chi, const double *u, int64_t n, const orc_od_table *t, double *delta) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) delta[i] = orc_od_bisect(pow(10.0, log_chi[i]), u[i], t);
+}
+
 /* update_tau_e / update_tau_gamma, qed/optical_depth.py:15-111.
  * Draws: purpose 1 -> (tau reset, tau after event); purpose 2 -> (inverse-CDF r, unused) */
 void orc_update_tau(double *tau, const double *inv_gamma, const double *chi, double dt,

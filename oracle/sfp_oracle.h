@@ -123,6 +123,7 @@ typedef struct {
 
 double orc_od_interp1d(double chi, const orc_od_table *tab);
 double orc_od_bisect(double chi, double r_uniform, const orc_od_table *tab);
+void orc_od_bisect_batch(const double *log_chi, const double *u, int64_t n, const orc_od_table *tab, double *delta);
 void orc_update_tau(double *tau, const double *inv_gamma, const double *chi, double dt,
                     int64_t N, const uint8_t *to_be_pruned, uint8_t *event, double *delta,
                     const orc_od_table *tab, uint64_t seed, uint32_t stream, uint32_t step);

@@ -19,6 +19,22 @@ def test_bf16_rounding_known_values():
     np.testing.assert_array_equal(mo.bf16_round(x), [1.0, 1.0, 1.0 + 2 ** -6, 1.0, 1.0 + 2 ** -7, -2.5])
 
 
+def test_oracle_batched_bisection_equals_single_queries():
+    """orc_od_bisect_batch (the C3 CPU baseline) is orc_od_bisect per query."""
+    from sfparticles_b200.qed import tables
+    d = tables.od_tables()
+    tab = orc.make_od_table(d["photon_rate_total"], d["photon_cumulative"], float(d["log_chi_min"]),
+                            float(d["log_chi_delta"]), float(d["log_delta_min"]), float(d["log_delta_delta"]))
+    rng = np.random.default_rng(11)
+    lc = rng.uniform(-3, 3, 3000)
+    u = rng.uniform(0, 1, 3000)
+    L = orc.lib()
+    out = np.empty(3000)
+    L.orc_od_bisect_batch(orc._p(lc), orc._p(u), 3000, ctypes.byref(tab), orc._p(out))
+    ref = np.array([L.orc_od_bisect(10.0 ** a, r, ctypes.byref(tab)) for a, r in zip(lc, u)])
+    np.testing.assert_array_equal(out, ref)
+
+
 def test_oracle_gradient_matches_finite_differences():
     """The oracle's backward pass against central differences of its own loss
     (weights unrounded, so the loss is smooth)."""
