@@ -771,6 +771,55 @@ def cpu_sample(n_e, start, max_steps, budget_s):
     return ps / dt, steps, ps, dt
 
 
+def window_state_sample(sim, every):
+    """Every `every`-th alive particle of each species of a device-resident
+    run, as host arrays (x, y, z, ux, uy, uz), with the run's t and step."""
+    out = {}
+    for p in sim.all_particles:
+        N = p.N_buffered
+        if N == 0:
+            out[p.name] = None
+            continue
+        keep = (p._d("_to_be_pruned")[:N] == 0).nonzero().flatten()[::every]
+        out[p.name] = tuple(p._d(k)[keep].cpu().numpy() for k in ("x", "y", "z", "ux", "uy", "uz"))
+    return {"species": out, "t": float(sim.t), "step": int(sim.step), "every": every}
+
+
+def cpu_sample_from_state(state, seed, max_steps, budget_s):
+    """Oracle port (C, OpenMP, all host threads) stepping a subsample of the
+    GPU run's own state at the window's start over the same steps (up to
+    `max_steps`, fewer if `budget_s` runs out).  Returns (rate, steps timed,
+    particle-steps, seconds, counts at the start)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+    from sfparticles_b200.qed import tables
+    sp = state["species"]
+
+    def species(name, q, m):
+        props = sp.get(name)
+        return orc.Species(name, q, m, N=0 if props is None else len(props[0]), props=props)
+
+    ele, pos, pho = species("electron", -1, 1), species("positron", 1, 1), species("photon", 0, 0)
+    ele.set_photon(pho)
+    pos.set_photon(pho)
+    pho.set_pair(ele, pos)
+    iA, dA, _, zmax = tables.rs_tables()
+    _, L = beam(1, 0)
+    terms = orc.gaussian_laser_pulse(A0, W0, CTAU, direction=-1, x0=L)
+    osim = orc.OracleSim([ele, pos, pho], DT, terms, ("rs", iA, dA), seed=seed, t0=state["t"], z_max=zmax)
+    osim.step = state["step"]
+    counts = {p.name: p.N_buffered for p in osim.all}
+    ps0 = osim.particle_steps
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and time.perf_counter() - t0 < budget_s:
+        osim.run(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    ps = osim.particle_steps - ps0
+    return ps / dt, steps, ps, dt, counts
+
+
 def window_start(args):
     """First step of the timed window.  `--start-step` if given; else, when
     the window is shorter than the 3000-step run, the steps centred on the
@@ -901,6 +950,8 @@ def run_ours(args, rank, world):
     assert sim.step == S0, (sim.step, S0)
     sim.reserve(args.steps)  # room for the window at twice the rate seen, so no growth inside it
     start_counts = {p.name: p.N_buffered for p in sim.all_particles}
+    # the CPU baseline's sample: a subsample of this state, stepped by the oracle after the GPU work
+    cpu_state = window_state_sample(sim, args.cpu_every) if (rank == 0 and world == 1 and not args.no_cpu) else None
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -1068,7 +1119,8 @@ def run_ours(args, rank, world):
                           "units_at_window_end": step_units, "per_kernel": per_kernel,
                           "variants_ms": {**{f"massive_s{a}_b{b}": v for (a, b), v in tm.items()},
                                           **{f"photon_s{a}_b{b}": v for (a, b), v in tp.items()}}},
-                e2e=e2e, compare=compare, start_step=S0, start_counts=start_counts, whole=whole, job=job)
+                e2e=e2e, compare=compare, start_step=S0, start_counts=start_counts, whole=whole, job=job,
+                cpu_state=cpu_state)
 
 
 def _release():
@@ -1109,8 +1161,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--roofline-steps", type=int, default=8)
-    ap.add_argument("--cpu-electrons", type=int, default=20_000)
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-electrons", type=int, default=100_000,
+                    help="--impl reference: electrons of the CPU sample (advanced on the CPU to the window)")
+    ap.add_argument("--cpu-every", type=int, default=10,
+                    help="cpu_baseline: every n-th particle of the GPU run's state at the window's start")
+    ap.add_argument("--cpu-budget", type=float, default=30.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -1197,18 +1252,17 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
-    # CPU baseline first (rank 0, N=1), before any CUDA context exists
-    cpu = None
-    S0 = window_start(args)
-    if rank == 0 and world == 1 and not args.no_cpu:
-        rate, steps, ps, dt = cpu_sample(args.cpu_electrons, S0, args.steps, args.cpu_budget)
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": omp_threads(), "kind": "port",
-               "sample": f"{args.cpu_electrons} e- of the same beam (1/{args.electrons // args.cpu_electrons} of "
-                         f"it), advanced untimed to step {max(S0, 1)}, then steps {max(S0, 1)}-{max(S0, 1) + steps} "
-                         f"timed: {ps:.3g} particle-steps in {dt:.2f}s",
-               "start_step": max(S0, 1), "steps_timed": steps}
-
     r = run_ours(args, rank, world)
+    # CPU baseline (rank 0, N=1): the oracle port steps a subsample of the GPU run's state at the window's start
+    cpu = None
+    if r.get("cpu_state") is not None:
+        st = r.pop("cpu_state")
+        rate, steps, ps, dt, c0 = cpu_sample_from_state(st, 1000, args.steps, args.cpu_budget)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": omp_threads(), "kind": "port",
+               "sample": f"every {st['every']}th alive particle of each species of the GPU run at step {st['step']} "
+                         f"({', '.join(f'{k} {v}' for k, v in c0.items())}), stepped by the oracle over steps "
+                         f"{st['step']}-{st['step'] + steps}: {ps:.3g} particle-steps in {dt:.2f} s",
+               "start_step": st["step"], "steps_timed": steps}
     if rank == 0:
         value = r["particle_steps"] / (r["ms"] * 1e-3)
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,

@@ -68,6 +68,17 @@ def _device():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _host_empty(shape, dtype):
+    """Host tensor for device-to-host copies: page-locked memory from torch's
+    caching host allocator (DMA in both directions, blocks reused from call
+    to call), or pageable memory where page-locking fails."""
+    import torch
+    try:
+        return torch.empty(shape, dtype=dtype, pin_memory=True)
+    except RuntimeError:
+        return torch.empty(shape, dtype=dtype)
+
+
 def _random_seed() -> int:
     return int.from_bytes(os.urandom(8), "little")
 
@@ -225,11 +236,15 @@ class Particles(object):
         import torch
         dev = _device()
         _lib.load()
+        # host arrays that _to_host left in page-locked memory go by DMA,
+        # asynchronously; the sources stay referenced until the copies end
+        src = []
         for k, v in list(self._arr.items()):
-            if k in _BOOL_ATTRS:
-                self._arr[k] = torch.as_tensor(np.ascontiguousarray(v, dtype=np.uint8), device=dev)
-            else:
-                self._arr[k] = torch.as_tensor(np.ascontiguousarray(v, dtype=np.float64), device=dev)
+            a = np.ascontiguousarray(v, dtype=np.uint8 if k in _BOOL_ATTRS else np.float64)
+            src.append(a)
+            self._arr[k] = torch.from_numpy(a).to(dev, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        del src
         self.__dict__["_gpu"] = True
         self.__dict__["_host_cache"] = {}
 
@@ -237,9 +252,16 @@ class Particles(object):
         """Move every attribute back to host numpy arrays (particles.py:157-164)."""
         if not self._gpu:
             return
+        import torch
+        outs = []
         for k, v in list(self._arr.items()):
-            h = v.cpu().numpy()
-            self._arr[k] = h.astype(bool) if k in _BOOL_ATTRS else np.ascontiguousarray(h)
+            h = _host_empty(v.shape, v.dtype)
+            h.copy_(v, non_blocking=True)
+            outs.append((k, h))
+        torch.cuda.current_stream(_device()).synchronize()
+        for k, h in outs:
+            a = h.numpy()
+            self._arr[k] = a.astype(bool) if k in _BOOL_ATTRS else a
         self.__dict__["_gpu"] = False
         self.__dict__["_host_cache"] = {}
 

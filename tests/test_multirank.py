@@ -96,9 +96,9 @@ def test_two_gloo_ranks_reduce_counters_spectrum_time_and_work():
     import torch.multiprocessing as mp
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    ctx = mp.get_context("spawn")  # no fork of a process that already runs threads
+    with ctx.Manager() as m:
         out = m.dict()
-        ctx = mp.get_context("spawn")
         procs = [ctx.Process(target=_rank, args=(r, world, port, out)) for r in range(world)]
         for p in procs:
             p.start()
