@@ -77,7 +77,7 @@ typedef struct sfp_segment {
 /* One collision instance: its own RNG key and field parameters. */
 typedef struct sfp_instance {
     sfp_u64 seed;
-    const double *field_params; /* [n_terms * SFP_FIELD_PARAMS]          */
+    const double *field_params; /* [n_terms * SFP_FIELD_PARAMS], 16-byte aligned */
     sfp_i32 first_seg;
     sfp_i32 n_seg;
 } sfp_instance;

@@ -34,7 +34,7 @@ from . import program
 VARIANTS = {
     ("fp64", "rs"): ([(2, 2), (3, 2)], [(3, 3), (2, 3), (3, 2)]),
     ("fp64", "od"): ([(2, 2), (3, 2)], [(3, 3), (2, 3)]),
-    ("fp32", "rs"): ([(2, 3), (3, 3), (3, 2), (4, 2)], [(3, 4), (2, 4), (3, 3), (4, 3)]),
+    ("fp32", "rs"): ([(2, 3), (3, 3), (3, 2), (4, 2), (2, 4)], [(3, 4), (2, 4), (3, 3), (4, 3)]),
     ("fp32", "od"): ([(2, 3), (3, 2)], [(3, 4), (3, 3)]),
 }
 DEFAULT = {

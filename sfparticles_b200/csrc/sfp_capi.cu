@@ -353,6 +353,46 @@ __global__ void k_inv_gamma(const double* __restrict__ ux, const double* __restr
     }
 }
 
+// Per chi bin (sfp_pair_bin) an upper bound of the rejection-sampling pair
+// rate over every delta, for the photon kernel's skip of pair tests that no
+// draw can pass.  The rate is factor (iA + (2/z - chi sqrt z) dA) with
+// z = (delta (1 - delta) chi)^(-2/3) >= z_min = (4/chi)^(2/3) and iA, dA
+// linear between the table's grid points.  From the grid interval below
+// z_min on, each interval contributes its largest iA, its largest positive
+// dA times 2/z and chi sqrt(z at its right end) times its largest |dA|;
+// chi is the bin's upper edge (the bound grows with chi), z_min is taken an
+// interval early for the rounding of z, and the result is multiplied by 4
+// for the rounding of the device's float32 and float64 rate arithmetic.
+// The last bin, and any run without rejection-sampling tables, never skips.
+__global__ void k_pair_bound(const double* __restrict__ iA, const double* __restrict__ dA, int zN, double zmax,
+                             float* __restrict__ out) {
+    const int k = threadIdx.x;
+    if (k >= SFP_PAIR_BOUND_BINS) return;
+    if (zN < 2 || !iA || !dA || k == SFP_PAIR_BOUND_BINS - 1) {
+        out[k] = __int_as_float(0x7f800000);
+        return;
+    }
+    const double chi = (double)__uint_as_float((unsigned int)(k + SFP_PAIR_BOUND_BASE + 1) << 20);
+    const double zmin = pow(4.0 / chi, 2.0 / 3.0);
+    if (zmin * (1.0 - 1e-4) > zmax) {  // every z is beyond the table: rate 0
+        out[k] = 0.0f;
+        return;
+    }
+    const double dz = zmax / (double)(zN - 1);
+    long long j0 = (long long)floor(zmin / dz) - 1;
+    if (j0 < 0) j0 = 0;
+    double b = 0.0;
+    for (long long j = j0; j < zN - 1; ++j) {
+        const double zl = fmax((double)j * dz, zmin * (1.0 - 1e-4)), zr = (double)(j + 1) * dz;
+        const double ia = fmax(iA[j], iA[j + 1]);
+        const double dpos = fmax(fmax(dA[j], dA[j + 1]), 0.0);
+        const double dabs = fmax(fabs(dA[j]), fabs(dA[j + 1]));
+        b = fmax(b, ia + (dpos > 0.0 ? 2.0 / zl * dpos : 0.0) + chi * sqrt(zr) * dabs);
+    }
+    const double factor = ((sfp::kAlpha * sfp::kMe) * (sfp::kC * sfp::kC)) / sfp::kHbar;
+    out[k] = __double2float_ru(4.0 * factor * b);
+}
+
 }  // namespace
 
 int sfp_set_error(int code, const std::string& msg) { return fail(code, msg); }
@@ -807,6 +847,9 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
     for (int i = 0; i < n_inst; ++i) {
         if (inst[i].first_seg != expect || inst[i].n_seg <= 0)
             return fail(SFP_EINVAL, "instances must cover the segments contiguously in order");
+        // the step's float32 field presets read their constants 16 bytes at a time
+        if (reinterpret_cast<uintptr_t>(inst[i].field_params) % 16 != 0)
+            return fail(SFP_EINVAL, "instance field parameters must be 16-byte aligned");
         expect += inst[i].n_seg;
     }
     if (expect != n_seg) return fail(SFP_EINVAL, "instances do not cover all segments");
@@ -973,7 +1016,13 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     ALLOC(h.n_buf_step, n_seg * sizeof(long long));
     ALLOC(h.st, sizeof(sfp_step_state));
     ALLOC(r->d, sizeof(sfp_run_dev));
+    float* pb;
+    ALLOC(pb, SFP_PAIR_BOUND_BINS * sizeof(float));
+    h.pair_bound = pb;
 #undef ALLOC
+    k_pair_bound<<<1, SFP_PAIR_BOUND_BINS, 0, r->s>>>(cfg->qed == SFP_QED_REJECTION ? cfg->rs.int_Ai : nullptr,
+                                                      cfg->rs.Aip, cfg->rs.z_N, cfg->rs.z_max, pb);
+    if (cudaGetLastError() != cudaSuccess) return cleanup(fail(SFP_ECUDA, "pair-rate bound table"));
     if ((!r->mg.seg.empty() && cudaMemcpyAsync(r->mg.d_seg, r->mg.seg.data(), r->mg.seg.size() * sizeof(int),
                                                cudaMemcpyHostToDevice, r->s) != cudaSuccess) ||
         (!r->pg.seg.empty() && cudaMemcpyAsync(r->pg.d_seg, r->pg.seg.data(), r->pg.seg.size() * sizeof(int),
@@ -1241,6 +1290,7 @@ int sfp_run_destroy(sfp_run* r) {
         cudaFree(G->super_pre);
     }
     cudaFree(r->h.st);
+    cudaFree((void*)r->h.pair_bound);
     cudaFree(r->d);
     if (r->ev_in) cudaEventDestroy(r->ev_in);
     if (r->ev_out) cudaEventDestroy(r->ev_out);

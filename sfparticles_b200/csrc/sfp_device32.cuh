@@ -61,9 +61,13 @@ constexpr float kFieldCut32 = 10.5f;
 
 SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
                                       float F[6]) {
-    const float* __restrict__ G = reinterpret_cast<const float*>(P + 10);
-    const float E0 = G[0], k0 = G[1], inv_zR = G[2], cq = G[3], inv_w02 = G[4], inv_kc2 = G[5], dirc = G[6];
-    const float cep = G[7], cp = G[8], sp = G[9], cut_r = G[10], kc = G[11];
+    // three 16-byte loads (a term's block starts 16-byte aligned: 16 doubles
+    // per term, and the run requires an aligned parameter array)
+    const float4 g0 = *reinterpret_cast<const float4*>(P + 10);
+    const float4 g1 = *reinterpret_cast<const float4*>(P + 12);
+    const float4 g2 = *reinterpret_cast<const float4*>(P + 14);
+    const float E0 = g0.x, k0 = g0.y, inv_zR = g0.z, cq = g0.w, inv_w02 = g1.x, inv_kc2 = g1.y, dirc = g1.z;
+    const float cep = g1.w, cp = g2.x, sp = g2.y, cut_r = g2.z, kc = g2.w;
     const double dir = P[5], x0 = P[6];
     const float xf = (float)x, yf = (float)y, zf = (float)z;
     const float xr = (float)((x - x0) - (dir * sfp::kC) * t);

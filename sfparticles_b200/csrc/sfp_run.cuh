@@ -80,4 +80,18 @@ struct sfp_run_dev {
     long long* n_buf_step;        // [n_seg] counts at the start of the running step
     const float* mlp_params;      // learned photon-energy sampler (optical depth), or NULL: the table
     sfp_step_state* st;
+    // rejection sampling: per chi bin an upper bound of the pair rate over
+    // every delta (SFP_PAIR_BOUND_BINS floats, the bins of sfp_pair_bin), so
+    // photons whose pair test no draw can pass skip the draw
+    const float* pair_bound;
 };
+
+// chi bins of the pair-rate bound: the float's exponent and 3 mantissa bits
+// from chi = 2^-16 up; bin 0 also holds every smaller chi, the last bin
+// (bound +inf) every larger one
+#define SFP_PAIR_BOUND_BINS 256
+#define SFP_PAIR_BOUND_BASE ((127 - 16) << 3)
+SFP_DEVICE_INLINE int sfp_pair_bin(float chi) {
+    int k = (int)(__float_as_uint(chi) >> 20) - SFP_PAIR_BOUND_BASE;
+    return k < 0 ? 0 : (k > SFP_PAIR_BOUND_BINS - 1 ? SFP_PAIR_BOUND_BINS - 1 : k);
+}

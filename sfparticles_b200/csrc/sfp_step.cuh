@@ -620,6 +620,28 @@ __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long lon
     sfp::cp_async_commit();
 }
 
+// The copies of a full tile (no copy is short): copy c = lane + 32 k of
+// sub-step `sub` reads component c / 16 at byte offset 256 sub + 16 (c % 16)
+// of the tile (or the flags at 32 sub + 16 (c - 16 NC)), straight from the
+// descriptor, with none of the general issue's bounds arithmetic; a
+// component the segment lacks is zero-filled.
+template <int NC>
+__device__ __forceinline__ void sfp_ring_issue_full(char* const* D, int sub, unsigned char* dst, int lane) {
+    constexpr int NCOPY = NC * 16 + 2;
+    const unsigned int off = (unsigned int)sub * 256u + 16u * (unsigned int)(lane & 15);
+#pragma unroll
+    for (int k = 0; k < (NCOPY + 31) / 32; ++k) {
+        const int c = lane + 32 * k;
+        if (c < NC * 16) {
+            const char* p = D[c >> 4];
+            sfp::cp_async16(dst + c * 16, p ? (const void*)(p + off) : (const void*)D[NC], p ? 16u : 0u);
+        } else if (c < NCOPY) {
+            sfp::cp_async16(dst + c * 16, D[NC] + sub * 32 + 16 * (c - NC * 16), 16u);
+        }
+    }
+    sfp::cp_async_commit();
+}
+
 // ---------------------------------------------------------------------------
 // Massive group.  Each warp takes tiles of SFP_WSUB * 32 particles by ticket
 // (the next ticket in flight while the tile computes) and streams them
@@ -647,13 +669,18 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     __syncwarp();
     char* const* D = desc;
     unsigned int cnt = 0;
+    const bool full = left >= (long long)(32 * SFP_WSUB);
+    auto issue = [&](int sb, unsigned char* dst) {
+        if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
+        else sfp_ring_issue<NC>(D, sb, left, dst, lane);
+    };
 #pragma unroll
-    for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<NC>(D, k, left, ring + k * SB, lane);
+    for (int k = 0; k < STAGES - 1; ++k) issue(k, ring + k * SB);
 #pragma unroll 1
     for (int sub = 0; sub < SFP_WSUB; ++sub) {
         __syncwarp();  // every lane has read the stage about to be refilled
         const int nsub = sub + STAGES - 1;
-        if (nsub < SFP_WSUB) sfp_ring_issue<NC>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
+        if (nsub < SFP_WSUB) issue(nsub, ring + (nsub % STAGES) * SB);
         else cp_async_commit();
         cp_async_wait<STAGES - 1>();
         __syncwarp();  // the stage of `sub` is complete for the whole warp
@@ -760,16 +787,102 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 // Photon group.  Same tiles, tickets and ring.  Per photon: the pair event
 // at t; a converted photon is marked (pruned = SFP_MARK, not pushed) and its
 // delta stored for the appends kernel; every other alive photon is pushed.
+//
+// Rejection sampling: an event needs r2 < W(r1) dt / gamma, and r2 is never
+// below 2^-33 (float32 draws) or 2^-53 (float64 draws).  The pair-rate bound
+// of the photon's chi bin (R->pair_bound) times dt / gamma below that means
+// no draw passes: the photon is pushed at once, with no draw and no rate.
+// The photons it keeps (a few percent in a cascade) go, with their state,
+// to a 32-entry per-warp queue in shared memory and are tested in full 32
+// at a time, so the test's cost is paid by full warps instead of by every
+// warp that holds one such photon.  Results are those of testing
+// every photon.  Optical depth updates every photon's tau and tests each.
 // ---------------------------------------------------------------------------
+template <int FORM>
+__device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
+                                                  const float* __restrict__ pb, const sfp_segment& S,
+                                                  const double* __restrict__ P, double x, double y, double z,
+                                                  double ux, double uy, double uz, double t) {
+    using namespace sfp;
+    if (FORM == SFP_FORM_FP64) {
+        double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (S.push) sfp_field_program(x, y, z, t, P, F);
+        const double ig = inv_gamma_photon(ux, uy, uz);
+        const double chi = chi_of(F, ux, uy, uz, ig);
+        if (chi == 0.0 || chi < T.chi_pair_min) return false;
+        return !((double)pb[sfp_pair_bin(__double2float_ru(chi))] * (R->dt * ig) < 0x1p-53);
+    } else {
+        float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (S.push) sfp_field_program32(x, y, z, t, P, F);
+        if (!(F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f || F[5] != 0.f)) return false;
+        const float g = sfp32::gamma_of(ux, uy, uz, true);
+        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+        if (!(chi > 0.0f) || (double)chi < T.chi_pair_min) return false;
+        return !(pb[sfp_pair_bin(chi)] * ((float)R->dt / g) < 0x1p-33f);
+    }
+}
+
+// a warp's queue of kept photons: tile index and state at t
+struct sfp_pair_queue {
+    double x[32], y[32], z[32], ux[32], uy[32], uz[32];
+    unsigned short e[32];
+};
+
+// the full pair test of the n queued photons (n <= 32), one per lane: mark
+// and store delta, or push and store; returns the events
+template <int FORM>
+__device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
+                                                       const sfp_segment& S, const sfp_instance& I,
+                                                       const double* __restrict__ P, char* const* D,
+                                                       const sfp_pair_queue& q, unsigned int n, long long base,
+                                                       double t, double dt, unsigned int step) {
+    using namespace sfp;
+    const int lane = threadIdx.x & 31;
+    bool ev = false;
+    if ((unsigned int)lane < n) {
+        const int e = q.e[lane];
+        double x = q.x[lane], y = q.y[lane], z = q.z[lane];
+        const double ux = q.ux[lane], uy = q.uy[lane], uz = q.uz[lane];
+        double tau = 0.0, delta = 0.0;
+        ev = sfp_pair_event<FORM, SFP_QED_REJECTION>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, base + e, tau,
+                                                     delta);
+        if (ev) {
+            reinterpret_cast<unsigned char*>(D[6])[e] = SFP_MARK;
+            reinterpret_cast<double*>(D[7])[e] = delta;
+        } else if (S.push) {
+            if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
+            else push_photon32(x, y, z, ux, uy, uz, dt);
+            reinterpret_cast<double*>(D[0])[e] = x;
+            reinterpret_cast<double*>(D[1])[e] = y;
+            reinterpret_cast<double*>(D[2])[e] = z;
+        }
+    }
+    return __popc(__ballot_sync(0xffffffffu, ev));
+}
+
+__device__ __forceinline__ void sfp_pair_enqueue(sfp_pair_queue& q, unsigned int k, int e, double x, double y,
+                                                 double z, double ux, double uy, double uz) {
+    q.e[k] = (unsigned short)e;
+    q.x[k] = x;
+    q.y[k] = y;
+    q.z[k] = z;
+    q.ux[k] = ux;
+    q.uy[k] = uy;
+    q.uz[k] = uz;
+}
+
 template <int FORM, int QED, int STAGES>
 __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
     constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
+    constexpr bool QUEUE = QED == SFP_QED_REJECTION;
     constexpr int NC = 6 + OD;
     constexpr int SB = sfp_ring<NC>::STAGE_BYTES;
     constexpr int PT = 32 * SFP_WSUB;
     extern __shared__ __align__(16) double s_tab[];
     __shared__ char* s_desc[SFP_TILE / 32][NC + 2];
+    __shared__ sfp_pair_queue s_q[QUEUE ? SFP_TILE / 32 : 1];  // per-warp queue of kept photons
+    __shared__ float s_pb[QUEUE ? SFP_PAIR_BOUND_BINS : 1];
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
     const long long n_tiles = st->n_ptiles;
@@ -777,10 +890,13 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
     const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
+    if (QUEUE)
+        for (int k = threadIdx.x; k < SFP_PAIR_BOUND_BINS; k += blockDim.x) s_pb[k] = R->pair_bound[k];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
     char* const* D = s_desc[warp];
+    sfp_pair_queue& q = s_q[QUEUE ? warp : 0];
 
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&st->pticket, 1);
@@ -801,17 +917,22 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         }
         const long long left = N - base;
         const bool bw = S.bw != 0, push = S.push != 0;
-        __syncwarp();  // the previous tile's lanes are done with its descriptor and stages
+        __syncwarp();  // the previous tile's lanes are done with its descriptor, stages and queue
         if (lane < NC + 2) s_desc[warp][lane] = sfp_desc_slot<QED, false>(S, lane, base);
         __syncwarp();
-        unsigned int cnt = 0;
+        unsigned int cnt = 0, qn = 0;
+        const bool full = left >= (long long)PT;
+        auto issue = [&](int sb, unsigned char* dst) {
+            if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
+            else sfp_ring_issue<NC>(D, sb, left, dst, lane);
+        };
 #pragma unroll
-        for (int k = 0; k < STAGES - 1; ++k) sfp_ring_issue<NC>(D, k, left, ring + k * SB, lane);
+        for (int k = 0; k < STAGES - 1; ++k) issue(k, ring + k * SB);
 #pragma unroll 1
         for (int sub = 0; sub < SFP_WSUB; ++sub) {
             __syncwarp();  // every lane has read the stage about to be refilled
             const int nsub = sub + STAGES - 1;
-            if (nsub < SFP_WSUB) sfp_ring_issue<NC>(D, nsub, left, ring + (nsub % STAGES) * SB, lane);
+            if (nsub < SFP_WSUB) issue(nsub, ring + (nsub % STAGES) * SB);
             else cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncwarp();  // the stage of `sub` is complete for the whole warp
@@ -822,24 +943,53 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             const bool alive = e < left && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
-            double tau = OD ? sd[192 + lane] : 0.0;
-            bool ev = false;
-            double delta = 0.0;
-            if (alive && bw)
-                ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
-            if (ev) {
-                // converted photons are pruned, not pushed (cpu.py:190); marked until their pairs are written
-                reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
-                reinterpret_cast<double*>(D[NC + 1])[e] = delta;
-            } else if (alive && push) {
-                if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
-                else push_photon32(x, y, z, ux, uy, uz, dt);
-                reinterpret_cast<double*>(D[0])[e] = x;
-                reinterpret_cast<double*>(D[1])[e] = y;
-                reinterpret_cast<double*>(D[2])[e] = z;
+            if (QUEUE) {
+                const bool keep = alive && bw && sfp_pair_possible<FORM>(R, T, s_pb, S, P, x, y, z, ux, uy, uz, t);
+                if (!keep && alive && push) {
+                    if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
+                    else push_photon32(x, y, z, ux, uy, uz, dt);
+                    reinterpret_cast<double*>(D[0])[e] = x;
+                    reinterpret_cast<double*>(D[1])[e] = y;
+                    reinterpret_cast<double*>(D[2])[e] = z;
+                }
+                // kept photons fill the queue; a full queue is tested at once and
+                // the sub-step's remaining kept photons start the next one
+                const unsigned int kb = __ballot_sync(0xffffffffu, keep);
+                const unsigned int slot = qn + __popc(kb & ((1u << lane) - 1u)), nk = __popc(kb);
+                if (keep && slot < 32u) sfp_pair_enqueue(q, slot, e, x, y, z, ux, uy, uz);
+                if (qn + nk >= 32u) {
+                    __syncwarp();  // the queue entries are written
+                    cnt += sfp_pair_batch<FORM>(R, T, S, I, P, D, q, 32u, base, t, dt, step);
+                    __syncwarp();  // every lane has read its entry
+                    if (keep && slot >= 32u) sfp_pair_enqueue(q, slot - 32u, e, x, y, z, ux, uy, uz);
+                    qn = qn + nk - 32u;
+                } else {
+                    qn += nk;
+                }
+            } else {
+                double tau = OD ? sd[192 + lane] : 0.0;
+                bool ev = false;
+                double delta = 0.0;
+                if (alive && bw)
+                    ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
+                if (ev) {
+                    // converted photons are pruned, not pushed (cpu.py:190); marked until their pairs are written
+                    reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
+                    reinterpret_cast<double*>(D[NC + 1])[e] = delta;
+                } else if (alive && push) {
+                    if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
+                    else push_photon32(x, y, z, ux, uy, uz, dt);
+                    reinterpret_cast<double*>(D[0])[e] = x;
+                    reinterpret_cast<double*>(D[1])[e] = y;
+                    reinterpret_cast<double*>(D[2])[e] = z;
+                }
+                if (OD && alive && bw && D[6]) reinterpret_cast<double*>(D[6])[e] = tau;
+                cnt += __popc(__ballot_sync(0xffffffffu, ev));
             }
-            if (OD && alive && bw && D[6]) reinterpret_cast<double*>(D[6])[e] = tau;
-            cnt += __popc(__ballot_sync(0xffffffffu, ev));
+        }
+        if (QUEUE && qn) {  // the tile's last kept photons
+            __syncwarp();
+            cnt += sfp_pair_batch<FORM>(R, T, S, I, P, D, q, qn, base, t, dt, step);
         }
         if (lane == 0) {
             R->pg.tile_cnt[tile] = cnt;
@@ -1004,8 +1154,9 @@ extern "C" __global__ void __launch_bounds__(1024) sfp_scan_kernel(const sfp_run
 }
 
 // ---------------------------------------------------------------------------
-// Appends.  Each warp takes 32 tile counters at a time, the massive group's
-// and then the photon group's; for a tile with events it adds the counts of
+// Appends.  The massive group's tile counters and then the photon group's
+// are dealt to the warps by stride (warp w: tiles w, w + nw, ...), read 32
+// at a time, one per lane; for a tile with events the warp adds the counts of
 // the earlier tiles of its super-tile to the super-tile's prefix, gathers
 // the tile's marked particles in index order into shared memory (16 flags
 // per lane per pass) and then handles 32 of them at a time, so every lane
@@ -1177,8 +1328,11 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long c0 = gw * 32; c0 < n_all; c0 += nw * 32) {
-        const long long mine = c0 + lane;
+    // warp gw owns tiles gw, gw + nw, gw + 2 nw, ...: tiles with events
+    // (every massive tile in a cascade, a few photon tiles) spread over all
+    // warps instead of queueing behind one warp per 32 neighbours
+    for (long long j0 = 0; gw + j0 * nw < n_all; j0 += 32) {
+        const long long mine = gw + (j0 + lane) * nw;
         unsigned int mc = 0u;
         if (mine < nm) mc = R->mg.tile_cnt[mine];
         else if (mine < n_all) mc = R->pg.tile_cnt[mine - nm];
@@ -1186,7 +1340,7 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
         while (busy) {
             const int b = __ffs(busy) - 1;
             busy &= busy - 1u;
-            const long long tg = c0 + b;
+            const long long tg = gw + (j0 + b) * nw;
             const unsigned int c = __shfl_sync(0xffffffffu, mc, b);
             if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, tg, c, s_list[warp], t, dt);
             else sfp_append_tile<FORM, false>(R, R->pg, tg - nm, c, s_list[warp], t, dt);
@@ -1233,6 +1387,7 @@ SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 2)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 2)
+SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)

@@ -79,14 +79,20 @@ def resolve_pending(run, species, update):
     _lib.check(L.sfp_run_resume(run, _stream_ptr()), "sfp_run_resume")
 
 
+# a growth may always reach this many slots (about 60 MB per species), so a
+# destination that starts empty does not grow in many small, halting steps
+GROWTH_FLOOR = 1 << 20
+
+
 def plan_chunk(species, rates, max_chunk):
     """Size append destinations for the next chunk of device steps from the
     append rates seen so far (`rates`: id(species) -> particles per step),
     and return (grew, chunk).  A destination that cannot take a full chunk
     at 1.25x its rate grows by the reference rule (particles.py:487-500),
-    each growth capped at half its count so memory stays near its use; the
-    chunk is shortened to what then fits.  Buffer sizes do not change
-    results: they only decide how often a step waits for room."""
+    each growth capped at half its count (or GROWTH_FLOOR slots, whichever
+    is more) so memory stays near its use; the chunk is shortened to what
+    then fits.  Buffer sizes do not change results: they only decide how
+    often a step waits for room."""
     grew = False
     chunk = max_chunk
     for p in species:
@@ -96,7 +102,7 @@ def plan_chunk(species, rates, max_chunk):
         free = p.buffer_size - p.N_buffered
         want = int(r * max_chunk * 1.25) + 1
         if free < want:
-            extra = min(want, p.N_buffered // 2 + 1024)
+            extra = min(want, max(p.N_buffered // 2 + 1024, GROWTH_FLOOR))
             if free < extra:
                 p._extend(extra)
                 grew = True

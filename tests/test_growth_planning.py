@@ -8,7 +8,7 @@ import numpy as np
 
 import sfparticles_b200 as S
 from sfparticles_b200.fields import static_field
-from sfparticles_b200.simulation import observe_rates, plan_chunk
+from sfparticles_b200.simulation import GROWTH_FLOOR, observe_rates, plan_chunk
 
 
 def _species(n, name="pho"):
@@ -23,16 +23,24 @@ def test_no_rate_no_growth_full_chunk():
     assert p.buffer_size == 100
 
 
-def test_growth_by_the_reference_rule_capped_at_half_the_count():
+def test_growth_by_the_reference_rule_for_a_chunk():
     p = _species(1000)
     rates = {id(p): 10.0}
     grew, chunk = plan_chunk([p], rates, 256)
-    # want 1.25 * 10 * 256 + 1 = 3201, capped at 1000 // 2 + 1024 = 1524: the reference rule
-    # grows by N_buffered // 4 + N_new = 250 + 1524
-    assert grew and p.buffer_size == 1000 + 250 + 1524
-    assert chunk == int(1774 / 12.5)
+    # want 1.25 * 10 * 256 + 1 = 3201, below the cap: the reference rule grows by
+    # N_buffered // 4 + N_new = 250 + 3201, and a full chunk fits
+    assert grew and p.buffer_size == 1000 + 250 + 3201
+    assert chunk == 256
     assert np.all(p._arr["_to_be_pruned"][1000:]) and np.all(p._arr["x"][1000:] == 0)
     assert np.array_equal(p._arr["ux"][:1000], np.full(1000, 4.0))
+
+
+def test_growth_capped_at_half_the_count_or_the_floor():
+    p = _species(1000)
+    grew, chunk = plan_chunk([p], {id(p): 1e4}, 256)
+    # want 3.2e6 + 1, capped at max(1000 // 2 + 1024, GROWTH_FLOOR) = 2^20
+    assert grew and p.buffer_size == 1000 + 250 + GROWTH_FLOOR
+    assert chunk == int((250 + GROWTH_FLOOR) / 12500.0)
 
 
 def test_enough_room_keeps_the_buffers_and_bounds_the_chunk():
@@ -45,13 +53,13 @@ def test_enough_room_keeps_the_buffers_and_bounds_the_chunk():
 
 
 def test_a_capped_growth_shortens_the_chunk():
-    """b's growth is capped at N // 2 + 1024, below a chunk's worth at its
+    """b's growth is capped at GROWTH_FLOOR, below a chunk's worth at its
     rate, so b sets the chunk; a has room for a full one."""
     a, b = _species(100), _species(100)
     a._extend(100_000)
-    grew, chunk = plan_chunk([a, b], {id(a): 1.0, id(b): 10.0}, 1000)
-    assert grew and b.buffer_size == 100 + 25 + (100 // 2 + 1024)
-    assert chunk == int((b.buffer_size - 100) / 12.5) < 1000
+    grew, chunk = plan_chunk([a, b], {id(a): 1.0, id(b): 5000.0}, 1000)
+    assert grew and b.buffer_size == 100 + 25 + GROWTH_FLOOR
+    assert chunk == int((b.buffer_size - 100) / 6250.0) < 1000
 
 
 def test_observed_rates_decay_by_half_at_most():
