@@ -1074,8 +1074,14 @@ def run_ours(args, rank, world):
         if share is not None:
             s.seed = shard.rank_seed(seed, rank)
         s._begin()
-        if S0 > 0:
-            s.run_on_device(S0)
+        # the float64 form gets the same variant search, on its own state before the window
+        nvar64 = sum(len(v) for v in autotune.VARIANTS[("fp64", "rs")]) * 2
+        tune64 = not args.no_variants and S0 >= nvar64
+        if S0 - (nvar64 if tune64 else 0) > 0:
+            s.run_on_device(S0 - (nvar64 if tune64 else 0))
+        if tune64:
+            tm64, tp64 = autotune.measure(s, steps=2)
+            s.set_kernel(massive=min(tm64, key=tm64.get), photon=min(tp64, key=tp64.get))
         s.reserve(args.steps)
         torch.cuda.synchronize()
         ps_a = s.particle_steps

@@ -38,9 +38,9 @@ VARIANTS = {
     ("fp32", "od"): ([(2, 3), (3, 2)], [(3, 4), (3, 3)]),
 }
 DEFAULT = {
-    ("fp64", "rs"): ((2, 2), (3, 3)),
+    ("fp64", "rs"): ((2, 2), (3, 2)),
     ("fp64", "od"): ((2, 2), (3, 3)),
-    ("fp32", "rs"): ((3, 3), (3, 4)),
+    ("fp32", "rs"): ((2, 4), (3, 3)),
     ("fp32", "od"): ((2, 3), (3, 3)),
 }
 

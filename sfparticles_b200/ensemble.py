@@ -25,7 +25,7 @@ from typing import Sequence
 
 from . import _lib, program
 from .particles import _device, _stream_ptr
-from .simulation import Simulation, _release_cached_blocks, observe_rates, plan_chunk, resolve_pending
+from .simulation import MIN_ROOM, Simulation, _release_cached_blocks, observe_rates, plan_chunk, resolve_pending
 
 
 class Ensemble(object):
@@ -156,7 +156,8 @@ class Ensemble(object):
         rates = self.__dict__.setdefault("_rates", {})
         while remaining > 0:
             target = min(remaining, max_chunk if rates else (self.graph_chunk or 64))
-            grew, fit = plan_chunk(allp, rates, target)
+            # many members: a smaller minimum room each, so the total stays near one simulation's
+            grew, fit = plan_chunk(allp, rates, target, min_room=max(1 << 12, MIN_ROOM // max(1, len(self.sims))))
             chunk = min(target, fit)
             if grew:
                 self._update_run()

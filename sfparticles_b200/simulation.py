@@ -82,17 +82,21 @@ def resolve_pending(run, species, update):
 # a growth may always reach this many slots (about 60 MB per species), so a
 # destination that starts empty does not grow in many small, halting steps
 GROWTH_FLOOR = 1 << 20
+# free slots a destination with appends is given at least (about 15 MB per
+# species): append rates ramp up within a chunk as a beam enters a pulse,
+# and small runs would otherwise stop for room again and again
+MIN_ROOM = 1 << 18
 
 
-def plan_chunk(species, rates, max_chunk):
+def plan_chunk(species, rates, max_chunk, min_room=MIN_ROOM):
     """Size append destinations for the next chunk of device steps from the
     append rates seen so far (`rates`: id(species) -> particles per step),
     and return (grew, chunk).  A destination that cannot take a full chunk
-    at 1.25x its rate grows by the reference rule (particles.py:487-500),
-    each growth capped at half its count (or GROWTH_FLOOR slots, whichever
-    is more) so memory stays near its use; the chunk is shortened to what
-    then fits.  Buffer sizes do not change results: they only decide how
-    often a step waits for room."""
+    at 1.25x its rate (and at least `min_room` free slots) grows by the
+    reference rule (particles.py:487-500), each growth capped at half its
+    count (or GROWTH_FLOOR slots, whichever is more) so memory stays near
+    its use; the chunk is shortened to what then fits.  Buffer sizes do not
+    change results: they only decide how often a step waits for room."""
     grew = False
     chunk = max_chunk
     for p in species:
@@ -100,7 +104,7 @@ def plan_chunk(species, rates, max_chunk):
         if r <= 0.0:
             continue
         free = p.buffer_size - p.N_buffered
-        want = int(r * max_chunk * 1.25) + 1
+        want = max(int(r * max_chunk * 1.25) + 1, int(min_room))
         if free < want:
             extra = min(want, max(p.N_buffered // 2 + 1024, GROWTH_FLOOR))
             if free < extra:
@@ -271,13 +275,18 @@ class Simulation(object):
 
     def reserve(self, nstep: int) -> bool:
         """Grow every append destination ahead of `nstep` device steps to
-        twice the append rate observed so far, so that those steps run
-        without waiting for room (a run whose rate then doubles still waits
-        and grows, as always).  Updates a live run; True if any buffer grew."""
+        twice the append rate observed so far (and at least MIN_ROOM free
+        slots where appends were seen), so that those steps run without
+        waiting for room and without growing (a run whose rate then doubles
+        still waits and grows, as always).  Updates a live run; True if any
+        buffer grew."""
         rates = self.__dict__.setdefault("_rates", {})
         grew = False
         for p in self._destinations():
-            want = int(2.0 * rates.get(id(p), 0.0) * int(nstep)) + 1024
+            r = rates.get(id(p), 0.0)
+            want = int(2.0 * r * int(nstep)) + 1024
+            if r > 0.0:
+                want = max(want, MIN_ROOM)
             if p.buffer_size - p.N_buffered < want:
                 p._extend(want)
                 grew = True

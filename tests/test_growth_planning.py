@@ -8,7 +8,7 @@ import numpy as np
 
 import sfparticles_b200 as S
 from sfparticles_b200.fields import static_field
-from sfparticles_b200.simulation import GROWTH_FLOOR, observe_rates, plan_chunk
+from sfparticles_b200.simulation import GROWTH_FLOOR, MIN_ROOM, observe_rates, plan_chunk
 
 
 def _species(n, name="pho"):
@@ -26,7 +26,7 @@ def test_no_rate_no_growth_full_chunk():
 def test_growth_by_the_reference_rule_for_a_chunk():
     p = _species(1000)
     rates = {id(p): 10.0}
-    grew, chunk = plan_chunk([p], rates, 256)
+    grew, chunk = plan_chunk([p], rates, 256, min_room=0)
     # want 1.25 * 10 * 256 + 1 = 3201, below the cap: the reference rule grows by
     # N_buffered // 4 + N_new = 250 + 3201, and a full chunk fits
     assert grew and p.buffer_size == 1000 + 250 + 3201
@@ -37,7 +37,7 @@ def test_growth_by_the_reference_rule_for_a_chunk():
 
 def test_growth_capped_at_half_the_count_or_the_floor():
     p = _species(1000)
-    grew, chunk = plan_chunk([p], {id(p): 1e4}, 256)
+    grew, chunk = plan_chunk([p], {id(p): 1e4}, 256, min_room=0)
     # want 3.2e6 + 1, capped at max(1000 // 2 + 1024, GROWTH_FLOOR) = 2^20
     assert grew and p.buffer_size == 1000 + 250 + GROWTH_FLOOR
     assert chunk == int((250 + GROWTH_FLOOR) / 12500.0)
@@ -47,7 +47,7 @@ def test_enough_room_keeps_the_buffers_and_bounds_the_chunk():
     p = _species(100)
     p._extend(5000)  # free room
     size = p.buffer_size
-    grew, chunk = plan_chunk([p], {id(p): 4.0}, 256)
+    grew, chunk = plan_chunk([p], {id(p): 4.0}, 256, min_room=0)
     assert not grew and p.buffer_size == size
     assert chunk == min(256, int((size - 100) / 5.0))
 
@@ -57,9 +57,20 @@ def test_a_capped_growth_shortens_the_chunk():
     rate, so b sets the chunk; a has room for a full one."""
     a, b = _species(100), _species(100)
     a._extend(100_000)
-    grew, chunk = plan_chunk([a, b], {id(a): 1.0, id(b): 5000.0}, 1000)
+    grew, chunk = plan_chunk([a, b], {id(a): 1.0, id(b): 5000.0}, 1000, min_room=0)
     assert grew and b.buffer_size == 100 + 25 + GROWTH_FLOOR
     assert chunk == int((b.buffer_size - 100) / 6250.0) < 1000
+
+
+def test_a_destination_with_appends_gets_the_minimum_room():
+    """A small rate still gets MIN_ROOM free slots (by the reference rule's
+    growth), so a ramping rate does not stop a small run for room each
+    chunk; a destination without appends is left alone."""
+    p, q = _species(10), _species(10)
+    grew, chunk = plan_chunk([p, q], {id(p): 0.5}, 256)
+    assert grew and p.buffer_size - p.N_buffered == 10 // 4 + MIN_ROOM
+    assert q.buffer_size == 10 and chunk == 256
+    assert plan_chunk([p, q], {id(p): 0.5}, 256) == (False, 256)
 
 
 def test_observed_rates_decay_by_half_at_most():
