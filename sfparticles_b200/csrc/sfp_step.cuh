@@ -822,27 +822,42 @@ __device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict_
     }
 }
 
-// a warp's queue of kept photons: tile index and state at t
+// a warp's queue of kept photons: tile index and, with STATE, the state at t
+// (the float32 form: no second read of their rows); without it the batch
+// reads the rows again (the float64 form, whose kernel has no registers to
+// spare for the state held across a batch)
+template <bool STATE>
 struct sfp_pair_queue {
+    unsigned short e[32];
+};
+template <>
+struct sfp_pair_queue<true> {
     double x[32], y[32], z[32], ux[32], uy[32], uz[32];
     unsigned short e[32];
 };
 
 // the full pair test of the n queued photons (n <= 32), one per lane: mark
 // and store delta, or push and store; returns the events
-template <int FORM>
+template <int FORM, bool STATE>
 __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
                                                        const sfp_segment& S, const sfp_instance& I,
                                                        const double* __restrict__ P, char* const* D,
-                                                       const sfp_pair_queue& q, unsigned int n, long long base,
-                                                       double t, double dt, unsigned int step) {
+                                                       const sfp_pair_queue<STATE>& q, unsigned int n,
+                                                       long long base, double t, double dt, unsigned int step) {
     using namespace sfp;
     const int lane = threadIdx.x & 31;
     bool ev = false;
     if ((unsigned int)lane < n) {
         const int e = q.e[lane];
-        double x = q.x[lane], y = q.y[lane], z = q.z[lane];
-        const double ux = q.ux[lane], uy = q.uy[lane], uz = q.uz[lane];
+        double x, y, z, ux, uy, uz;
+        if constexpr (STATE) {
+            x = q.x[lane], y = q.y[lane], z = q.z[lane];
+            ux = q.ux[lane], uy = q.uy[lane], uz = q.uz[lane];
+        } else {  // the row, still as it was at t: the photon is written only below
+            x = reinterpret_cast<const double*>(D[0])[e], y = reinterpret_cast<const double*>(D[1])[e];
+            z = reinterpret_cast<const double*>(D[2])[e], ux = reinterpret_cast<const double*>(D[3])[e];
+            uy = reinterpret_cast<const double*>(D[4])[e], uz = reinterpret_cast<const double*>(D[5])[e];
+        }
         double tau = 0.0, delta = 0.0;
         ev = sfp_pair_event<FORM, SFP_QED_REJECTION>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, base + e, tau,
                                                      delta);
@@ -860,15 +875,18 @@ __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __rest
     return __popc(__ballot_sync(0xffffffffu, ev));
 }
 
-__device__ __forceinline__ void sfp_pair_enqueue(sfp_pair_queue& q, unsigned int k, int e, double x, double y,
+template <bool STATE>
+__device__ __forceinline__ void sfp_pair_enqueue(sfp_pair_queue<STATE>& q, unsigned int k, int e, double x, double y,
                                                  double z, double ux, double uy, double uz) {
     q.e[k] = (unsigned short)e;
-    q.x[k] = x;
-    q.y[k] = y;
-    q.z[k] = z;
-    q.ux[k] = ux;
-    q.uy[k] = uy;
-    q.uz[k] = uz;
+    if constexpr (STATE) {
+        q.x[k] = x;
+        q.y[k] = y;
+        q.z[k] = z;
+        q.ux[k] = ux;
+        q.uy[k] = uy;
+        q.uz[k] = uz;
+    }
 }
 
 template <int FORM, int QED, int STAGES>
@@ -881,7 +899,8 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     constexpr int PT = 32 * SFP_WSUB;
     extern __shared__ __align__(16) double s_tab[];
     __shared__ char* s_desc[SFP_TILE / 32][NC + 2];
-    __shared__ sfp_pair_queue s_q[QUEUE ? SFP_TILE / 32 : 1];  // per-warp queue of kept photons
+    constexpr bool QSTATE = FORM == SFP_FORM_FP32;  // the queue holds the kept photons' state
+    __shared__ sfp_pair_queue<QSTATE> s_q[QUEUE ? SFP_TILE / 32 : 1];  // per-warp queue of kept photons
     __shared__ float s_pb[QUEUE ? SFP_PAIR_BOUND_BINS : 1];
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
@@ -896,7 +915,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
     char* const* D = s_desc[warp];
-    sfp_pair_queue& q = s_q[QUEUE ? warp : 0];
+    sfp_pair_queue<QSTATE>& q = s_q[QUEUE ? warp : 0];
 
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&st->pticket, 1);
@@ -959,7 +978,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                 if (keep && slot < 32u) sfp_pair_enqueue(q, slot, e, x, y, z, ux, uy, uz);
                 if (qn + nk >= 32u) {
                     __syncwarp();  // the queue entries are written
-                    cnt += sfp_pair_batch<FORM>(R, T, S, I, P, D, q, 32u, base, t, dt, step);
+                    cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, 32u, base, t, dt, step);
                     __syncwarp();  // every lane has read its entry
                     if (keep && slot >= 32u) sfp_pair_enqueue(q, slot - 32u, e, x, y, z, ux, uy, uz);
                     qn = qn + nk - 32u;
@@ -989,7 +1008,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         }
         if (QUEUE && qn) {  // the tile's last kept photons
             __syncwarp();
-            cnt += sfp_pair_batch<FORM>(R, T, S, I, P, D, q, qn, base, t, dt, step);
+            cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, qn, base, t, dt, step);
         }
         if (lane == 0) {
             R->pg.tile_cnt[tile] = cnt;
