@@ -13,7 +13,10 @@ collision (seed = 1000 + rank): weak scaling with no data-path collective;
 --split-beam instead gives each rank its slice of one beam (strong
 scaling).  After the timed window every rank joins one all-reduce of the
 job's counters and photon spectrum; the time is the max over ranks of
-CUDA-event time.
+CUDA-event time.  On one GPU the line also carries, under `workloads`,
+summaries of the plain config (C1), the learned sampler (C3), the batched
+instances (C4) and the avalanche (C5), each measured after the window
+(`--no-extras` skips them; `--workload cN` prints one in full).
 """
 from __future__ import annotations
 
@@ -138,6 +141,17 @@ def make_c4(form="fp32", n_inst=256, steps=2000, scale=1.0):
     return ens
 
 
+_SINK = None  # a list while the default run collects the other workloads' lines
+
+
+def _emit(line):
+    """Print a workload's JSON line, or keep it for the default line's `workloads`."""
+    if _SINK is not None:
+        _SINK.append(line)
+    else:
+        print(json.dumps(line), flush=True)
+
+
 def run_c4(args):
     """Batched uneven instances on one GPU: value, per-kernel roofline."""
     import torch
@@ -199,7 +213,7 @@ def run_c4(args):
                          "per_kernel": per_kernel, "launches_timed": args.roofline_steps},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk.summary(),
             "particle_steps": ps}
-    print(json.dumps(line), flush=True)
+    _emit(line)
 
 
 WORKLOAD_C3 = "learned photon-energy sampler: 5e7 queries per step, log10 chi ~ U[-3,0] (the small plain config's " \
@@ -304,7 +318,7 @@ def run_c3(args):
                     "d2h_bytes_per_step": 8 * n},
             "cpu_baseline": None if args.no_cpu else c3_cpu_baseline(lc, u, mlp), "gpu_launches": args.steps,
             "clocks": clk_summary}
-    print(json.dumps(line), flush=True)
+    _emit(line)
 
 
 def c3_cpu_baseline(lc, u, mlp, m=1_000_000, budget_s=10.0):
@@ -429,7 +443,7 @@ def run_c5(args):
                          "per_kernel": per_kernel, "launches_timed": len(kms)},
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clk.summary(),
             "particle_steps": ps}
-    print(json.dumps(line), flush=True)
+    _emit(line)
 
 
 WORKLOAD_OPS = "the reference's step loop over the one-for-one float64 kernels (engine 'ops'): the scaled-cascade " \
@@ -541,7 +555,7 @@ def run_c1(args):
                        "l2": "the whole state (<30 MB) is L2-resident: launch- and latency-bound, no flush"},
             "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
             "particle_steps": ps}
-    print(json.dumps(line), flush=True)
+    _emit(line)
 
 
 WORKLOAD_KERNELS ="the per-op kernels one by one (the reference's one-for-one kernel boundary): N e- and N photons " \
@@ -1133,8 +1147,59 @@ def run_ours(args, rank, world):
 
 
 def _release():
+    import gc
     import torch
+    gc.collect()
     torch.cuda.empty_cache()
+
+
+def _summary(line):
+    """The parts of a workload's line that the default line carries."""
+    if not line:
+        return None
+    keep = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "dtype", "gpu_launches", "clocks",
+            "mlp_over_table_speed")
+    s = {k: line[k] for k in keep if k in line}
+    s["workload"] = (line.get("config") or {}).get("workload")
+    r = line.get("roofline")
+    if r:
+        s["roofline"] = {k: r.get(k) for k in ("bound", "kernel", "achieved", "peak", "unit", "frac")}
+    for k in ("cpu_baseline", "e2e"):
+        v = line.get(k)
+        if v:
+            s[k] = {kk: v.get(kk) for kk in ("value", "unit", "cores", "kind", "sample", "h2d_bytes_per_step",
+                                              "d2h_bytes_per_step") if kk in v}
+    if "table_sampler" in line:
+        s["table_sampler_samples_per_s"] = line["table_sampler"]["samples_per_s"]
+    return s
+
+
+def run_extras(args):
+    """The other configs, measured after the default line's window on the
+    same GPU, one after the other: C1 (the plain config's whole run, with the
+    oracle port on the same run), C3 (the learned sampler), C4 (256 batched
+    instances, 2000 steps), C5 (the avalanche to 1e9 particles).  Each entry
+    summarises the line `bench.py --workload cN` prints in full; a workload
+    that fails records its error and the others still run."""
+    import copy
+    global _SINK
+    out = {}
+    for name, fn, steps in (("c1", run_c1, None), ("c3", run_c3, 20), ("c4", run_c4, 2000), ("c5", run_c5, 2500)):
+        a = copy.copy(args)
+        a.workload = name
+        a.warmup = 3
+        if steps is not None:
+            a.steps = steps
+        _SINK = []
+        try:
+            fn(a)
+            out[name] = _summary(_SINK[-1] if _SINK else None)
+        except Exception as exc:  # recorded in the line; the headline stands
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+        finally:
+            _SINK = None
+            _release()
+    return out
 
 
 def main():
@@ -1168,6 +1233,8 @@ def main():
     ap.add_argument("--p-min-blocks", type=int, default=0)
     ap.add_argument("--no-graphs", action="store_true", help="one eager launch per kernel (for profilers)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c2 on one GPU: skip the summaries of C1, C3, C4 and C5 in the line")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--roofline-steps", type=int, default=8)
     ap.add_argument("--cpu-electrons", type=int, default=100_000,
@@ -1288,6 +1355,8 @@ def main():
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "particle_steps": r["particle_steps"], "whole_run": r["whole"],
                 "job_diagnostics": r["job"], "vs_fp64": r["compare"]}
+        if world == 1 and not args.no_extras:
+            line["workloads"] = run_extras(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

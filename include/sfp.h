@@ -239,6 +239,16 @@ int sfp_mlp_device_error(int *code);
 int sfp_mlp_infer_withheld(const float *params, const double *log_chi, const double *u, double *delta, int64_t N,
                            void *stream);
 
+/* The per-chi-bin upper bound of the rejection-sampling pair rate
+ * (qed/rejection_sampling_tables.py:56-78) over every delta, that the fused
+ * step's photon kernel uses to skip pair tests no draw can pass: out[k] for
+ * the chi of bin k (SFP_PAIR_BOUND_BINS = 256 bins: the float's exponent and
+ * 3 mantissa bits from chi = 2^-16; bin 0 takes every smaller chi, the last
+ * bin every larger one and is +inf), 4 times the tables' interval maxima
+ * from (4/chi)^(2/3) on.  No counterpart in the reference: exposed so that
+ * tests and tools can check the bound.  out: 256 floats on the device. */
+int sfp_pair_rate_bound(const double *int_ai, const double *aip, int z_n, double z_max, float *out, void *stream);
+
 /* ---- QED rate tables generated on the GPU --------------------------------
  * The reference's table generators (qed/rejection_sampling_tables.py:80-112,
  * qed/optical_depth_tables.py:136-198, scipy airy + quad) restated with the

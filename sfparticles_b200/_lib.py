@@ -113,6 +113,7 @@ _SIGS = {
     "sfp_mlp_device_error": ([P], c_i32),
     "sfp_mlp_infer_withheld": ([P, P, P, P, c_i64, P], c_i32),
     "sfp_table_rs": ([P, c_i64, P, P, P], c_i32),
+    "sfp_pair_rate_bound": ([P, P, c_i32, c_d, P, P], c_i32),
     "sfp_table_od": ([c_i32, c_d, P, c_i64, P, c_i64, P, P, P, P], c_i32),
     "sfp_run_destroy": ([P], c_i32),
 }

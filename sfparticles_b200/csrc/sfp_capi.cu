@@ -397,6 +397,15 @@ __global__ void k_pair_bound(const double* __restrict__ iA, const double* __rest
 
 int sfp_set_error(int code, const std::string& msg) { return fail(code, msg); }
 
+extern "C" int sfp_pair_rate_bound(const double* int_ai, const double* aip, int z_n, double z_max, float* out,
+                                   void* stream) {
+    if (!out || (z_n >= 2 && (!int_ai || !aip))) return fail(SFP_EINVAL, "sfp_pair_rate_bound: NULL argument");
+    k_pair_bound<<<1, SFP_PAIR_BOUND_BINS, 0, reinterpret_cast<cudaStream_t>(stream)>>>(int_ai, aip, z_n, z_max, out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("sfp_pair_rate_bound: ") + cudaGetErrorString(e));
+    return SFP_OK;
+}
+
 // ============== find_event_index without allocation (scratch) ===============
 //
 // sfp_find_event_index needs a scratch array of one count per 4096-entry
