@@ -59,8 +59,20 @@ SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, u
 // half the smallest denormal
 constexpr float kFieldCut32 = 10.5f;
 
-SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
-                                      float F[6]) {
+// The longitudinal focusing factors of a Gaussian term at a point:
+// 1/sqrt(q), 1/q and the Gouy phase atan(x/zR), q = 1 + (x/zR)^2.  They
+// depend on the point's x and on 1/zR only, so the terms of a sum with the
+// same zR (the polarisations and directions of one beam geometry) share
+// them: the first such term past its far-field cut forms them, the others
+// reuse them (`have`), with bitwise the same results.
+struct GaussXY {
+    float inv_zR;  // the 1/zR they were formed with
+    float rs, rq, gouy;
+};
+
+// one term, sharing G (see GaussXY); F receives the term's field
+SFP_DEVICE_INLINE void field_gaussian_g(const double* __restrict__ P, double x, double y, double z, double t,
+                                        GaussXY& G, bool& have, float F[6]) {
     // three 16-byte loads (a term's block starts 16-byte aligned: 16 doubles
     // per term, and the run requires an aligned parameter array)
     const float4 g0 = *reinterpret_cast<const float4*>(P + 10);
@@ -78,14 +90,20 @@ SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, do
         for (int k = 0; k < 6; ++k) F[k] = 0.0f;
         return;
     }
-    const float xz = xf * inv_zR;
-    const float q = 1.0f + xz * xz;
-    const float rs = rsqrtf(q);
-    const float rq = rs * rs;
-    const float gouy = atanf(xz);
-    const float phi = k0 * xr + (cq * r2) * (xf * rq) - gouy;
-    const float env = __expf(-((r2 * inv_w02) * rq + (phi * phi) * inv_kc2));
-    const float E = E0 * cos_r(phi + cep) * rs * env;
+    if (!have || G.inv_zR != inv_zR) {
+        const float xz = xf * inv_zR;
+        const float q = fmaf(xz, xz, 1.0f);
+        G.inv_zR = inv_zR;
+        G.rs = rsqrtf(q);
+        G.rq = G.rs * G.rs;
+        G.gouy = atanf(xz);
+        have = true;
+    }
+    const float curv = (cq * r2) * (xf * G.rq);  // (k0 / (2 zR^2)) r^2 x / q
+    const float tenv = (r2 * inv_w02) * G.rq;    // r^2 / w(x)^2
+    const float phi = fmaf(k0, xr, curv) - G.gouy;
+    const float env = __expf(-fmaf(phi * phi, inv_kc2, tenv));
+    const float E = E0 * cos_r(phi + cep) * G.rs * env;
     const float Ey = E * cp, Ez = E * sp;
     F[0] = 0.0f;
     F[1] = Ey;
@@ -93,6 +111,13 @@ SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, do
     F[3] = 0.0f;
     F[4] = -Ez * dirc;
     F[5] = Ey * dirc;
+}
+
+SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
+                                      float F[6]) {
+    GaussXY G;
+    bool have = false;
+    field_gaussian_g(P, x, y, z, t, G, have, F);
 }
 
 // simple_laser_pulse (fields.py:102-116)

@@ -98,6 +98,11 @@ class Fields:
         def program(real: str, fns) -> str:
             lines = []
             counter = [0, 0]
+            # float32 sums of Gaussian terms share the terms' transverse factors
+            # (sfp32::GaussXY: equal for terms of one beam geometry)
+            share = real == "float" and sum(t.kind == KIND_GAUSSIAN for t in self.terms()) >= 2
+            if share:
+                lines.append("    sfp32::GaussXY G; bool G_have = false;")
 
             def emit(n) -> str:
                 if isinstance(n, _Term):
@@ -117,6 +122,8 @@ class Fields:
                                          f" for (int i = 0; i < 6; ++i) {v}[i] = (float)D[i]; }}")
                     elif n.kind == KIND_STATIC:
                         lines.append(f"    {real} {v}[6]; {fns[n.kind]}(P + {k * N_PARAMS}, {v});")
+                    elif share and n.kind == KIND_GAUSSIAN:
+                        lines.append(f"    {real} {v}[6]; sfp32::field_gaussian_g(P + {k * N_PARAMS}, x, y, z, t, G, G_have, {v});")
                     else:
                         lines.append(f"    {real} {v}[6]; {fns[n.kind]}(P + {k * N_PARAMS}, x, y, z, t, {v});")
                     return v

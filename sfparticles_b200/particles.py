@@ -490,10 +490,12 @@ class Particles(object):
     def _prune(self) -> None:
         """Remove pruned particles and compact every array (particles.py:503-516)."""
         if self._gpu:
-            keep = self._arr["_to_be_pruned"] == 0
+            import torch
+            # the kept slots once, then one gather per array
+            idx = torch.nonzero(self._arr["_to_be_pruned"] == 0).flatten()
             for k, v in list(self._arr.items()):
-                self._arr[k] = v[keep].contiguous()
-            N = int(keep.sum().item())
+                self._arr[k] = torch.index_select(v, 0, idx)
+            N = int(idx.numel())
         else:
             keep = ~self._arr["_to_be_pruned"].astype(bool)
             for k, v in list(self._arr.items()):
