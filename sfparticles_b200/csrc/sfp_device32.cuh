@@ -2,7 +2,8 @@
 //
 // The particle state stays float64 in HBM.  Fields, chi, the QED samplers
 // and the Boris / Thomas-BMT / Landau-Lifshitz updates are evaluated in
-// float32 (MUFU transcendentals after explicit range reduction), and every
+// float32 (MUFU transcendentals after explicit range reduction, divisions
+// as __fdividef: a reciprocal and a product, within 2 ulp), and every
 // update is applied as a float32 INCREMENT to the float64 state:
 //   x += dx,  u += du,  s += ds          (float64 accumulation of float32 steps)
 // so rounding errors scale with the step, not with |x|, |u| (the role Kahan
@@ -86,8 +87,9 @@ constexpr float kFieldCut32 = 10.5f;
 // 1/sqrt(q), 1/q and the Gouy phase atan(x/zR), q = 1 + (x/zR)^2.  They
 // depend on the point's x and on 1/zR only, so the terms of a sum with the
 // same zR (the polarisations and directions of one beam geometry) share
-// them: the first such term past its far-field cut forms them, the others
-// reuse them (`have`), with bitwise the same results.
+// them: the first such term the warp evaluates (one not skipped by the
+// far-field cut) forms them, the others reuse them (`have`), with bitwise
+// the same results.
 struct GaussXY {
     float inv_zR;  // the 1/zR they were formed with
     float rs, rq, gouy;
@@ -108,8 +110,11 @@ SFP_DEVICE_INLINE void field_gaussian_g(const double* __restrict__ P, double x, 
     const float xr = (float)((x - x0) - (dir * sfp::kC) * t);
     const float r2 = yf * yf + zf * zf;
     // |phi| >= k0 |xr| - k0 r2 / (4 zR) - pi/2 (as in the float64 form):
-    // beyond kFieldCut32 kc the envelope is exactly 0, and so is the field
-    if (k0 * fabsf(xr) - cut_r * r2 - 1.5708f > kFieldCut32 * kc) {
+    // beyond kFieldCut32 kc the envelope is exactly 0, and so is the field.
+    // The work is skipped when every active lane is past the cut; a lane
+    // past it among others computes and takes exact zeros (no divergence)
+    const bool cut = k0 * fabsf(xr) - cut_r * r2 - 1.5708f > kFieldCut32 * kc;
+    if (__all_sync(__activemask(), cut)) {
         for (int k = 0; k < 6; ++k) F[k] = 0.0f;
         return;
     }
@@ -129,11 +134,11 @@ SFP_DEVICE_INLINE void field_gaussian_g(const double* __restrict__ P, double x, 
     const float E = E0 * cos_r(phi + cep) * G.rs * env;
     const float Ey = E * cp, Ez = E * sp;
     F[0] = 0.0f;
-    F[1] = Ey;
-    F[2] = Ez;
+    F[1] = cut ? 0.0f : Ey;
+    F[2] = cut ? 0.0f : Ez;
     F[3] = 0.0f;
-    F[4] = -Ez * dirc;
-    F[5] = Ey * dirc;
+    F[4] = cut ? 0.0f : -Ez * dirc;
+    F[5] = cut ? 0.0f : Ey * dirc;
 }
 
 SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, double y, double z, double t,
@@ -230,7 +235,7 @@ SFP_DEVICE_INLINE float rate_core(float chi_g, float base, const float* __restri
     const float z = exp2f(0.66666667f * __log2f(base));
     const float iA = ai_lerp(iAt, z, inv_dz, zN);
     const float dA = ai_lerp(dAt, z, inv_dz, zN);
-    return iA + (2.0f / z + sgn * chi_g * sqrtf(z)) * dA;
+    return iA + (__fdividef(2.0f, z) + sgn * chi_g * sqrtf(z)) * dA;
 }
 
 // _linear_interp1d (qed/optical_depth_tables.py:56-66) in float32: the float32

@@ -132,20 +132,40 @@ SFP_DEVICE_INLINE void push_photon(double& x, double& y, double& z, double ux, d
 }
 
 // float32 form of push_massive: float32 increments, float64 accumulation.
+// The float32 push's per-(segment, step) constants, formed once per tile
+// rather than once per particle (the same expressions, so the same values)
+struct sfp_pc32 {
+    double th;  // t + dt/2, the time of the push's field
+    float hc;   // c dt / 2
+    float eps;  // q dt / (2 m c)
+    float bq;   // q dt / (2 m)
+    float ll;   // the LL / CLL prefactor
+};
+
+SFP_DEVICE_INLINE sfp_pc32 push_consts32(const sfp_segment& S, double t, double dt) {
+    sfp_pc32 K;
+    K.th = t + 0.5 * dt;
+    K.hc = (float)(0.5 * kC * dt);
+    K.eps = (float)((S.q * dt) / ((2.0 * kMe) * kC));
+    K.bq = (float)((S.q * dt) / (2.0 * kMe));
+    K.ll = (float)ll_factor(dt);
+    return K;
+}
+
 SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& ux, double& uy, double& uz,
                                       double& sx, double& sy, double& sz, const sfp_segment& S,
-                                      const double* __restrict__ P, double t, double dt) {
-    const float hc = (float)(0.5 * kC * dt);
+                                      const double* __restrict__ P, const sfp_pc32& K) {
+    const float hc = K.hc;
     float g = sfp32::gamma_of(ux, uy, uz, false);
     float fx = (float)ux, fy = (float)uy, fz = (float)uz;
-    float a = hc / g;
+    float a = __fdividef(hc, g);
     x += (double)(a * fx);
     y += (double)(a * fy);
     z += (double)(a * fz);
     float F[6];
-    sfp_field_program32(x, y, z, t + 0.5 * dt, P, F);
-    const float eps = (float)((S.q * dt) / ((2.0 * kMe) * kC));
-    const float bq = (float)((S.q * dt) / (2.0 * kMe));
+    sfp_field_program32(x, y, z, K.th, P, F);
+    const float eps = K.eps;
+    const float bq = K.bq;
     const float ex = eps * F[0], ey = eps * F[1], ez = eps * F[2];
     const float umx = fx + ex, umy = fy + ey, umz = fz + ez;
     float gm;
@@ -155,16 +175,16 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
         const double dx = ux + (double)ex, dy = uy + (double)ey, dz = uz + (double)ez;
         gm = (float)sqrt(((1.0 + dx * dx) + dy * dy) + dz * dz);
     }
-    const float igm = 1.0f / gm;
+    const float igm = __fdividef(1.0f, gm);
     if (S.spin) {  // inline.py:39-70: spin rotation with B_eff(u-), as an increment
         const float ae = (float)S.ae;
         const float uB = umx * F[3] + umy * F[4] + umz * F[5];
-        const float a1 = ae + igm, a2 = ae * gm / (gm + 1.0f), a3 = ae + 1.0f / (gm + 1.0f);
+        const float a1 = ae + igm, a2 = __fdividef(ae * gm, gm + 1.0f), a3 = ae + __fdividef(1.0f, gm + 1.0f);
         const float bex = a1 * F[3] - a2 * uB * umx - a3 * (umy * F[2] - umz * F[1]);
         const float bey = a1 * F[4] - a2 * uB * umy - a3 * (umz * F[0] - umx * F[2]);
         const float bez = a1 * F[5] - a2 * uB * umz - a3 * (umx * F[1] - umy * F[0]);
         const float Tx = bq * bex, Ty = bq * bey, Tz = bq * bez;
-        const float f2 = 2.0f / (1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
+        const float f2 = __fdividef(2.0f, 1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
         const float s0x = (float)sx, s0y = (float)sy, s0z = (float)sz;
         const float spx = s0x + (s0y * Tz - s0z * Ty), spy = s0y + (s0z * Tx - s0x * Tz), spz = s0z + (s0x * Ty - s0y * Tx);
         sx += (double)(f2 * (spy * Tz - spz * Ty));
@@ -174,7 +194,7 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
     // Boris (inline.py:4-36) as u += 2 eps E + u' x S
     const float Tx = bq * F[3] * igm, Ty = bq * F[4] * igm, Tz = bq * F[5] * igm;
     const float upx = umx + (umy * Tz - umz * Ty), upy = umy + (umz * Tx - umx * Tz), upz = umz + (umx * Ty - umy * Tx);
-    const float f2 = 2.0f / (1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
+    const float f2 = __fdividef(2.0f, 1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
     ux += (double)(2.0f * ex + f2 * (upy * Tz - upz * Ty));
     uy += (double)(2.0f * ey + f2 * (upz * Tx - upx * Tz));
     uz += (double)(2.0f * ez + f2 * (upx * Ty - upy * Tx));
@@ -182,18 +202,18 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
     if (S.rr == SFP_RR_LL || (S.rr == SFP_RR_CLL && !S.spin)) {  // inline.py:104-123
         fx = (float)ux; fy = (float)uy; fz = (float)uz;
         const float chi = sfp32::chi_of(F, fx, fy, fz, g);
-        float factor = (float)ll_factor(dt);
+        float factor = K.ll;
         if (S.rr == SFP_RR_CLL) {
             const float q = 1.0f + 4.8f * (1.0f + chi) * __logf(1.0f + 1.7f * chi) + 2.44f * chi * chi;
             factor *= exp2f(-0.66666667f * __log2f(q));
         }
-        const float c = factor * chi * chi / g;
+        const float c = __fdividef(factor * chi * chi, g);
         ux += (double)(c * fx);
         uy += (double)(c * fy);
         uz += (double)(c * fz);
         g = sfp32::gamma_of(ux, uy, uz, false);
     }
-    a = hc / g;
+    a = __fdividef(hc, g);
     x += (double)(a * (float)ux);
     y += (double)(a * (float)uy);
     z += (double)(a * (float)uz);
@@ -325,9 +345,9 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
                 sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
                 const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
                 const float dl = r1 * r1 * r1;
-                const float base = dl / ((1.0f - dl) * chi);
+                const float base = __fdividef(dl, (1.0f - dl) * chi);
                 const float W = -kRate * sfp32::rate_core(dl * chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, 1.0f);
-                ev = r2 < 3.0f * r1 * r1 * W * ((float)dt / g);
+                ev = r2 < 3.0f * r1 * r1 * W * __fdividef((float)dt, g);
                 d = (double)dl;
                 if (ev && dl * g < (float)R->photon_threshold) ev = false;
             }
@@ -392,10 +412,10 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                     float r1, r2;
                     sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
                     const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
-                    const float base = 1.0f / ((r1 * (1.0f - r1)) * chi);
+                    const float base = __fdividef(1.0f, (r1 * (1.0f - r1)) * chi);
                     const float W =
                         kRate * sfp32::rate_core(chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, -1.0f);
-                    ev = r2 < W * ((float)dt / g);
+                    ev = r2 < W * __fdividef((float)dt, g);
                     d = (double)r1;
                 }
             } else {
@@ -664,6 +684,7 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     const sfp_instance& I = R->inst[S.instance];
     const double* __restrict__ P = I.field_params;
     const bool rad = S.radiating != 0, push = S.push != 0;
+    const sfp_pc32 K32 = push_consts32(S, t, dt);  // float32 form's push constants of this segment
     __syncwarp();  // the previous tile's lanes are done with the descriptor and the stages
     if (lane < NC + 2) desc[lane] = sfp_desc_slot<QED, SPIN>(S, lane, base);
     __syncwarp();
@@ -716,7 +737,7 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
             reinterpret_cast<double*>(D[NC + 1])[e] = delta;
         } else if (alive && push) {
             if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
-            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, K32);
             reinterpret_cast<double*>(D[0])[e] = x;
             reinterpret_cast<double*>(D[1])[e] = y;
             reinterpret_cast<double*>(D[2])[e] = z;
@@ -812,13 +833,15 @@ __device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict_
         if (chi == 0.0 || chi < T.chi_pair_min) return false;
         return !((double)pb[sfp_pair_bin(__double2float_ru(chi))] * (R->dt * ig) < 0x1p-53);
     } else {
-        float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (S.push) sfp_field_program32(x, y, z, t, P, F);
-        if (!(F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f || F[5] != 0.f)) return false;
+        // straight-line: every condition is combined at the end (no early exit)
+        float F[6];
+        sfp_field_program32(x, y, z, t, P, F);
+        const bool field = S.push && (F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f ||
+                                      F[5] != 0.f);
         const float g = sfp32::gamma_of(ux, uy, uz, true);
         const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
-        if (!(chi > 0.0f) || (double)chi < T.chi_pair_min) return false;
-        return !(pb[sfp_pair_bin(chi)] * ((float)R->dt / g) < 0x1p-33f);
+        const bool some = chi > 0.0f && !((double)chi < T.chi_pair_min);
+        return field & some & !(pb[sfp_pair_bin(chi)] * __fdividef((float)R->dt, g) < 0x1p-33f);
     }
 }
 
@@ -963,13 +986,16 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
             if (QUEUE) {
-                const bool keep = alive && bw && sfp_pair_possible<FORM>(R, T, s_pb, S, P, x, y, z, ux, uy, uz, t);
+                // every lane runs the filter and the push (dead lanes on their
+                // zero-filled stage entries); only the stores are conditional
+                const bool keep = alive & bw & sfp_pair_possible<FORM>(R, T, s_pb, S, P, x, y, z, ux, uy, uz, t);
+                double px = x, py = y, pz = z;
+                if (FORM == SFP_FORM_FP64) push_photon(px, py, pz, ux, uy, uz, dt);
+                else push_photon32(px, py, pz, ux, uy, uz, dt);
                 if (!keep && alive && push) {
-                    if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
-                    else push_photon32(x, y, z, ux, uy, uz, dt);
-                    reinterpret_cast<double*>(D[0])[e] = x;
-                    reinterpret_cast<double*>(D[1])[e] = y;
-                    reinterpret_cast<double*>(D[2])[e] = z;
+                    reinterpret_cast<double*>(D[0])[e] = px;
+                    reinterpret_cast<double*>(D[1])[e] = py;
+                    reinterpret_cast<double*>(D[2])[e] = pz;
                 }
                 // kept photons fill the queue; a full queue is tested at once and
                 // the sub-step's remaining kept photons start the next one
@@ -1194,7 +1220,7 @@ __device__ __forceinline__ void sfp_write_pair_child(const sfp_segment& D, long 
     if (D.push) {
         double sx = 0.0, sy = 0.0, sz = 0.0;
         if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, D, P, t, dt);
-        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, D, P, t, dt);
+        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, D, P, push_consts32(D, t, dt));
     }
     D.x[slot] = x;
     D.y[slot] = y;
@@ -1249,7 +1275,7 @@ __device__ __forceinline__ void sfp_write_photon(const sfp_run_dev* __restrict__
             sz = S.sz[i];
         }
         if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
-        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, push_consts32(S, t, dt));
         S.x[i] = x;
         S.y[i] = y;
         S.z[i] = z;
