@@ -54,10 +54,12 @@ BYTES_EMIT = 154    # emitter in the appends kernel: parent state + delta read (
                     # state + flag written (49)
 BYTES_PAIR = 155    # pair event in the appends kernel: parent state + delta read (56), flag (1), e- and e+
                     # written (98)
-# DRAM bytes (read + write, ncu) / algorithmic bytes of one launch, from an ncu capture of the same
-# cascade at 1e6 electrons at its final state (2.8 GB of photon state, larger than L2, so traffic
-# scales with the units processed).  Only kernels whose state exceeds L2 in that capture are listed.
-NCU_TRAFFIC_RATIO = {"photon": 2.768e9 / 2.806e9}
+# DRAM bytes (read + write) over algorithmic bytes of one launch, from a
+# one-kernel ncu capture of the collision window at 1e6 e- (photon kernel:
+# 2.36e7 photons, 1.72 GB of state, larger than L2, so traffic scales with
+# the units processed): 1.176e9 + 0.544e9 against 1.719e9.  Only kernels
+# whose state exceeds L2 in that capture are listed.
+NCU_TRAFFIC_RATIO = {"photon": (1.176e9 + 0.544e9) / 1.719e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"

@@ -340,17 +340,17 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
         const float g = sfp32::gamma_of(ux, uy, uz, false);
         const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
         if (QED == SFP_QED_REJECTION) {
-            if (chi > 0.0f) {
-                float r1, r2;
-                sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
-                const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
-                const float dl = r1 * r1 * r1;
-                const float base = __fdividef(dl, (1.0f - dl) * chi);
-                const float W = -kRate * sfp32::rate_core(dl * chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, 1.0f);
-                ev = r2 < 3.0f * r1 * r1 * W * __fdividef((float)dt, g);
-                d = (double)dl;
-                if (ev && dl * g < (float)R->photon_threshold) ev = false;
-            }
+            // straight-line: the draw and the rate for every lane, the
+            // conditions combined at the end (chi = 0 gives W = 0)
+            float r1, r2;
+            sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+            const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
+            const float dl = r1 * r1 * r1;
+            const float base = __fdividef(dl, (1.0f - dl) * chi);
+            const float W = -kRate * sfp32::rate_core(dl * chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, 1.0f);
+            ev = (chi > 0.0f) & (r2 < 3.0f * r1 * r1 * W * __fdividef((float)dt, g)) &
+                 !(dl * g < (float)R->photon_threshold);
+            d = (double)dl;
         } else {
             // float32 rate lookup, float64 optical depth
             double u = 0.0;
@@ -719,10 +719,15 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
             sy = sd[(7 + OD) * 32 + lane];
             sz = sd[(8 + OD) * 32 + lane];
         }
+        // every lane runs the event test and the push (dead lanes on their
+        // zero-filled stage entries); marks and stores are conditional
         bool ev = false;
         double delta = 0.0, hs = 0.0, lchi = 0.0;
-        if (alive && rad)
-            ev = sfp_photon_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta, hs, lchi);
+        if (rad) {
+            const bool e1 = sfp_photon_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta, hs,
+                                                        lchi);
+            ev = alive & e1;
+        }
         if (OD && R->mlp_params) {  // warp-uniform: the learned sampler draws the events' energies
             bool e1[1] = {ev};
             double d1[1] = {delta};
@@ -735,9 +740,10 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
             // the appends kernel writes the photon and pushes the parent
             reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
             reinterpret_cast<double*>(D[NC + 1])[e] = delta;
-        } else if (alive && push) {
-            if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
-            else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, K32);
+        }
+        if (FORM == SFP_FORM_FP64) push_massive(x, y, z, ux, uy, uz, sx, sy, sz, S, P, t, dt);
+        else push_massive32(x, y, z, ux, uy, uz, sx, sy, sz, S, P, K32);
+        if (!ev && alive && push) {
             reinterpret_cast<double*>(D[0])[e] = x;
             reinterpret_cast<double*>(D[1])[e] = y;
             reinterpret_cast<double*>(D[2])[e] = z;
