@@ -575,14 +575,34 @@ __global__ void __launch_bounds__(128, 4) k_mlp_infer_tc(const float* __restrict
     unsigned phase = 0;
     bool ok = true;
     const long long n_tiles = (n + TM - 1) / TM;
+    // this thread's inputs of the next tile are loaded while the current one
+    // runs its layers, so their latency is hidden behind the MMAs and SiLU
+    double lc_next = 0.0, u_next = 0.0;
+    {
+        const long long q0 = (long long)blockIdx.x * TM + tid;
+        if (blockIdx.x < n_tiles && q0 < n) {
+            lc_next = lc[q0];
+            u_next = u[q0];
+        }
+    }
     for (long long tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
         const long long q = tile * TM + tid;
+        const double lc_q = lc_next, u_q = u_next;
+        {
+            const long long qn = q + (long long)gridDim.x * TM;
+            lc_next = 0.0;
+            u_next = 0.0;
+            if (qn < n) {
+                lc_next = lc[qn];
+                u_next = u[qn];
+            }
+        }
         // layer 0 inputs: the features split into BF16 hi / lo parts
         {
             float x0 = 0.0f, x1 = 0.0f;
             if (q < n) {
-                x0 = sfp_mlp::feat_chi(lc[q]);
-                x1 = sfp_mlp::feat_u(u[q]);
+                x0 = sfp_mlp::feat_chi(lc_q);
+                x1 = sfp_mlp::feat_u(u_q);
             }
             unsigned short a, b, c, d;
             hi_lo(x0, a, b);
