@@ -12,8 +12,8 @@ numeric parameters (a0, waist, duration, ...) are per member.
 
 A member's results are the ones it gets when run alone.  Its particles draw
 from its own Philox key, with streams numbered by species within the member,
-and its children are appended in its own order (one look-back chain and one
-pair-scan segment per member).
+and its children are appended in its own order (the append scan restarts at
+each member's first tile, per destination).
 
 This is an extension with no reference counterpart: the reference runs one
 collision per ``Simulation``.
