@@ -1149,10 +1149,15 @@ def run_ours(args, rank, world):
 
 
 def _release():
+    """Return a finished workload's device blocks and page-locked host blocks
+    (its final state's copies) before the next workload: tens of GB each at
+    the C4 and C5 sizes, more than the host holds if they accumulate."""
     import gc
     import torch
     gc.collect()
     torch.cuda.empty_cache()
+    if hasattr(torch._C, "_host_emptyCache"):
+        torch._C._host_emptyCache()
 
 
 def _summary(line):
@@ -1186,6 +1191,7 @@ def run_extras(args):
     import copy
     global _SINK
     out = {}
+    _release()  # the default line's runs
     for name, fn, steps in (("c1", run_c1, None), ("c3", run_c3, 20), ("c4", run_c4, 2000), ("c5", run_c5, 2500)):
         a = copy.copy(args)
         a.workload = name

@@ -124,5 +124,6 @@ typedef struct sfp_run_state {
 /* device error codes */
 #define SFP_DEV_OK 0
 #define SFP_DEV_CAPACITY 2 /* more tiles than the run's counters hold */
+#define SFP_DEV_TILE 3     /* a long-tile kernel met a step planned with shorter tiles */
 
 #endif

@@ -66,7 +66,7 @@ class RunConfig(ctypes.Structure):
 SFP_QED_REJECTION, SFP_QED_OPTICAL_DEPTH = 0, 1
 SFP_FORM_FP64, SFP_FORM_FP32 = 0, 1
 SFP_FIELD_PARAMS = 16
-DEV_ERRORS = {2: "tile table too small"}
+DEV_ERRORS = {2: "tile table too small", 3: "a long-tile step kernel met a step planned with shorter tiles"}
 
 _SIGS = {
     "sfp_version": ([], ctypes.c_char_p),

@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <algorithm>
 #include <unordered_map>
 #include <vector>
 
@@ -27,7 +28,7 @@
 #include "sfp_run.cuh"
 
 #define SFP_VERSION_STRING "sfparticles_b200 0.1.0 (sm_100a)"
-// particles per tile of the fused step; the NVRTC modules are built with SFP_TILE equal to it
+// threads per block of the fused step's group kernels; the NVRTC modules are built with SFP_TILE equal to it
 #define SFP_TILE_HOST 256
 
 namespace {
@@ -774,10 +775,14 @@ int sfp_inv_gamma(const double* ux, const double* uy, const double* uz, double* 
 // take warp tiles by ticket; the scan is one block; the appends kernel is a
 // grid over both groups' tile counters.
 
-// warp tile of both groups: SFP_WSUB_HOST sub-steps of 32 particles; the
-// NVRTC modules are built with SFP_WSUB equal to it
-#define SFP_WSUB_HOST 32
 #define SFP_SUPER_TILE_HOST 64
+// the any-tile kernels (..._t) of each form: ring stages and blocks per SM
+#define SFP_T_M_STAGES 2
+#define SFP_T_P_STAGES 3
+#define SFP_T_P_MINB 3
+// a group of more particles than this has SFP_TILE_MAX-long tiles at every
+// step (the tile rule), so the long-tile kernels may run it
+#define SFP_LONG_TILE_POP ((long long)(SFP_TILE_MAX / 2) * SFP_TILE_TARGET)
 
 struct sfp_group_host {
     std::vector<int> seg;
@@ -788,8 +793,10 @@ struct sfp_group_host {
 struct sfp_run {
     sfp_module* mod = nullptr;
     cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_appends = nullptr, k_book = nullptr;
-    int grid_m = 0, grid_p = 0, grid_a = 0;
-    size_t smem_m = 0, smem_p = 0;
+    cudaKernel_t k_massive_t = nullptr, k_photon_t = nullptr;  // any tile length
+    int grid_m = 0, grid_p = 0, grid_a = 0, grid_mt = 0, grid_pt = 0;
+    size_t smem_m = 0, smem_p = 0, smem_mt = 0, smem_pt = 0;
+    std::vector<long long> nb_lo;  // lower bounds of the device's n_buffered (it only grows between reads)
     cudaStream_t s = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int n_seg = 0, n_inst = 0;
@@ -802,12 +809,15 @@ struct sfp_run {
     std::vector<int> dseg;
 };
 
-// tiles of a group at full capacity: each segment's tiles plus the padding
-// up to the next multiple of a super-tile
+// tile counters a group needs at full capacity: each segment's longest
+// tiles plus the padding up to the next multiple of a super-tile, and at
+// least what the shorter tiles of a small population take (at most
+// SFP_TILE_TARGET tiles plus one partial tile and the padding per segment)
 static long long tiles_for(const sfp_run* r, const std::vector<int>& segs) {
     long long t = 0;
-    for (int s : segs) t += (r->segs[s].capacity + r->h.tile - 1) / r->h.tile + SFP_SUPER_TILE_HOST;
-    return t + 1;
+    for (int s : segs) t += (r->segs[s].capacity + SFP_TILE_MAX - 1) / SFP_TILE_MAX + SFP_SUPER_TILE_HOST;
+    const long long small = SFP_TILE_TARGET + (long long)segs.size() * (SFP_SUPER_TILE_HOST + 1);
+    return (t > small ? t : small) + 1;
 }
 
 // (re)allocate a group's tile counters for the current capacities; a step
@@ -898,11 +908,25 @@ static int validate_segments(int n_inst, const sfp_instance* inst, int n_seg, co
     return SFP_OK;
 }
 
+// the counts last uploaded or read back: a lower bound of every later step's
+static void note_counts(sfp_run* r, const long long* nb) {
+    r->nb_lo.assign(nb, nb + r->n_seg);
+}
+
+// whether every step from here on gives the group SFP_TILE_MAX-long tiles
+static bool long_tiles(const sfp_run* r, const std::vector<int>& segs) {
+    long long n = 0;
+    for (int s : segs) n += r->nb_lo.empty() ? 0 : r->nb_lo[s];
+    return n > SFP_LONG_TILE_POP;
+}
+
 static int run_upload(sfp_run* r, const sfp_instance* inst, const int64_t* n_buffered) {
     if (inst) SFP_CUDA(cudaMemcpyAsync((void*)r->h.inst, inst, r->n_inst * sizeof(sfp_instance), cudaMemcpyHostToDevice, r->s));
     SFP_CUDA(cudaMemcpyAsync((void*)r->h.seg, r->segs.data(), r->n_seg * sizeof(sfp_segment), cudaMemcpyHostToDevice, r->s));
-    if (n_buffered)
+    if (n_buffered) {
         SFP_CUDA(cudaMemcpyAsync(r->h.n_buffered, n_buffered, r->n_seg * sizeof(long long), cudaMemcpyHostToDevice, r->s));
+        note_counts(r, reinterpret_cast<const long long*>(n_buffered));
+    }
     SFP_CUDA(cudaMemcpyAsync(r->d, &r->h, sizeof(sfp_run_dev), cudaMemcpyHostToDevice, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
     return SFP_OK;
@@ -968,7 +992,13 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     const std::string km = "sfp_massive_" + fq + "_s" + std::to_string(mstages) + "_b" + std::to_string(minb);
     const std::string kp = "sfp_photon_" + fq + "_s" + std::to_string(stages) + "_b" + std::to_string(pminb);
     const std::string ka = f64 ? "sfp_appends_fp64" : "sfp_appends_fp32";
+    const int t_minb = f64 ? 2 : 3;
+    const std::string kmt = "sfp_massive_" + fq + "_s" + std::to_string(SFP_T_M_STAGES) + "_b" +
+                            std::to_string(t_minb) + "_t";
+    const std::string kpt = "sfp_photon_" + fq + "_s" + std::to_string(SFP_T_P_STAGES) + "_b" +
+                            std::to_string(SFP_T_P_MINB) + "_t";
     if ((rc = module_kernel(m, km.c_str(), &r->k_massive)) || (rc = module_kernel(m, kp.c_str(), &r->k_photon)) ||
+        (rc = module_kernel(m, kmt.c_str(), &r->k_massive_t)) || (rc = module_kernel(m, kpt.c_str(), &r->k_photon_t)) ||
         (rc = module_kernel(m, ka.c_str(), &r->k_appends)) ||
         (rc = module_kernel(m, "sfp_scan_kernel", &r->k_scan)) ||
         (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
@@ -989,7 +1019,6 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     h.dt = cfg->dt;
     h.photon_threshold = cfg->photon_threshold;
     h.qed = cfg->qed;
-    h.tile = 32 * SFP_WSUB_HOST;
     h.any_rad = h.any_bw = 0;
     for (int s = 0; s < n_seg; ++s) {
         h.any_rad |= seg[s].radiating ? 1 : 0;
@@ -1066,19 +1095,25 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     r->smem_m = (size_t)h.m_ring_off + warps * mstages * (size_t)h.m_stage_bytes;
     h.ring_off = (int)((tab + 127) / 128 * 128);
     r->smem_p = (size_t)h.ring_off + warps * stages * ((6 + od) * 256 + 32);
+    r->smem_mt = (size_t)h.m_ring_off + warps * SFP_T_M_STAGES * (size_t)h.m_stage_bytes;
+    r->smem_pt = (size_t)h.ring_off + warps * SFP_T_P_STAGES * ((6 + od) * 256 + 32);
     if ((rc = run_alloc_tiles(r))) return cleanup(rc);
     if ((rc = run_upload(r, inst, n_buffered))) return cleanup(rc);
     const size_t cap = 200 * 1024;
-    if (r->smem_m > cap || r->smem_p > cap)
+    if (r->smem_m > cap || r->smem_p > cap || r->smem_mt > cap || r->smem_pt > cap)
         return cleanup(fail(SFP_EINVAL, "QED tables and copy rings too large for shared memory"));
     // always raised, never lowered: the kernels' static shared memory counts
     // toward the 48 KB a launch gets without it, and runs that share a module
     // need different amounts
     if (raise_dynamic_smem((const void*)r->k_massive, r->smem_m) != cudaSuccess ||
-        raise_dynamic_smem((const void*)r->k_photon, r->smem_p) != cudaSuccess)
+        raise_dynamic_smem((const void*)r->k_photon, r->smem_p) != cudaSuccess ||
+        raise_dynamic_smem((const void*)r->k_massive_t, r->smem_mt) != cudaSuccess ||
+        raise_dynamic_smem((const void*)r->k_photon_t, r->smem_pt) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "cannot raise dynamic shared memory"));
     r->grid_m = persistent_grid(r->k_massive, r->smem_m, minb);
     r->grid_p = persistent_grid(r->k_photon, r->smem_p, pminb);
+    r->grid_mt = persistent_grid(r->k_massive_t, r->smem_mt, t_minb);
+    r->grid_pt = persistent_grid(r->k_photon_t, r->smem_pt, SFP_T_P_MINB);
     r->grid_a = persistent_grid(r->k_appends, 0, 2);
     *out = r;
     return SFP_OK;
@@ -1102,19 +1137,31 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
 }
 
 // one step: book(prepare), massive, photon, scan + appends; ev (6 events)
-// brackets the massive, the photon and the scan + appends kernels when given
-static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev) {
-    int prep = 1;
+// brackets the massive, the photon and the scan + appends kernels when given.
+// mlong / plong: the group's steps all have SFP_TILE_MAX-long tiles, run by
+// the autotuned long-tile kernel; else by the any-tile kernel
+static int launch_unit(sfp_run* r, cudaStream_t s, cudaEvent_t* ev, bool mlong, bool plong) {
+    int prep = 1 | (mlong ? 2 : 0) | (plong ? 4 : 0);  // the book kernel checks the tiles the launches assume
     void* a_book[] = {&r->d, &prep};
     void* a[] = {&r->d};
     SFP_CUDA(cudaLaunchKernel((const void*)r->k_book, dim3(1), dim3(256), a_book, 0, s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[0], s));
-    if (!r->mg.seg.empty())
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem_m, s));
+    if (!r->mg.seg.empty()) {
+        if (mlong)
+            SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive, dim3(r->grid_m), dim3(SFP_TILE_HOST), a, r->smem_m, s));
+        else
+            SFP_CUDA(cudaLaunchKernel((const void*)r->k_massive_t, dim3(r->grid_mt), dim3(SFP_TILE_HOST), a,
+                                      r->smem_mt, s));
+    }
     if (ev) SFP_CUDA(cudaEventRecord(ev[1], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[2], s));
-    if (!r->pg.seg.empty())
-        SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem_p, s));
+    if (!r->pg.seg.empty()) {
+        if (plong)
+            SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon, dim3(r->grid_p), dim3(SFP_TILE_HOST), a, r->smem_p, s));
+        else
+            SFP_CUDA(cudaLaunchKernel((const void*)r->k_photon_t, dim3(r->grid_pt), dim3(SFP_TILE_HOST), a,
+                                      r->smem_pt, s));
+    }
     if (ev) SFP_CUDA(cudaEventRecord(ev[3], s));
     if (ev) SFP_CUDA(cudaEventRecord(ev[4], s));
     if (!r->dseg.empty()) {
@@ -1139,13 +1186,15 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
     SFP_CUDA(cudaEventRecord(r->ev_in, cs));
     SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
     int64_t done = 0;
+    const bool ml = long_tiles(r, r->mg.seg), pl = long_tiles(r, r->pg.seg);
     if (graph_chunk > 0 && nsteps >= graph_chunk) {
-        auto it = r->graphs.find(graph_chunk);
+        const int key = graph_chunk * 4 + (ml ? 2 : 0) + (pl ? 1 : 0);
+        auto it = r->graphs.find(key);
         if (it == r->graphs.end()) {
             cudaGraph_t g;
             SFP_CUDA(cudaStreamBeginCapture(r->s, cudaStreamCaptureModeThreadLocal));
             int rc = SFP_OK;
-            for (int k = 0; k < graph_chunk && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, nullptr);
+            for (int k = 0; k < graph_chunk && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, nullptr, ml, pl);
             cudaError_t e = cudaStreamEndCapture(r->s, &g);
             if (rc) return rc;
             if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -1153,12 +1202,12 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
             e = cudaGraphInstantiate(&ge, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            it = r->graphs.emplace(graph_chunk, ge).first;
+            it = r->graphs.emplace(key, ge).first;
         }
         for (; done + graph_chunk <= nsteps; done += graph_chunk) SFP_CUDA(cudaGraphLaunch(it->second, r->s));
     }
     for (; done < nsteps; ++done) {
-        int rc = launch_unit(r, r->s, nullptr);
+        int rc = launch_unit(r, r->s, nullptr, ml, pl);
         if (rc) return rc;
     }
     int rc = launch_fold(r);
@@ -1178,7 +1227,8 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     int rc = SFP_OK;
     for (auto& e : ev)
         if (cudaEventCreate(&e) != cudaSuccess) rc = fail(SFP_ECUDA, "cudaEventCreate");
-    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, &ev[6 * k]);
+    const bool ml = long_tiles(r, r->mg.seg), pl = long_tiles(r, r->pg.seg);
+    for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, &ev[6 * k], ml, pl);
     if (rc == SFP_OK) rc = launch_fold(r);
     if (rc == SFP_OK && cudaStreamSynchronize(r->s) != cudaSuccess) rc = fail(SFP_ECUDA, "synchronize");
     const bool has[3] = {!r->mg.seg.empty(), !r->pg.seg.empty(), !r->dseg.empty()};
@@ -1201,10 +1251,12 @@ int sfp_run_read_state(sfp_run* r, sfp_run_state* state, int64_t* n_buffered, vo
     if (!r || !state) return fail(SFP_EINVAL, "sfp_run_read_state: NULL argument");
     (void)stream;
     sfp_step_state st;
+    std::vector<long long> nb(r->n_seg);
     SFP_CUDA(cudaMemcpyAsync(&st, r->h.st, sizeof(st), cudaMemcpyDeviceToHost, r->s));
-    if (n_buffered)
-        SFP_CUDA(cudaMemcpyAsync(n_buffered, r->h.n_buffered, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
+    SFP_CUDA(cudaMemcpyAsync(nb.data(), r->h.n_buffered, r->n_seg * sizeof(long long), cudaMemcpyDeviceToHost, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
+    note_counts(r, nb.data());
+    if (n_buffered) std::copy(nb.begin(), nb.end(), n_buffered);
     state->t = st.t;
     state->step = st.step;
     state->halted = st.halted;

@@ -23,6 +23,19 @@
 #pragma once
 #include "sfp_types.h"
 
+// Tile length.  Each step the bookkeeping kernel gives each group the
+// shortest power-of-two tile from SFP_TILE_MIN to SFP_TILE_MAX particles
+// that cuts its population into at most SFP_TILE_TARGET tiles: a large
+// population keeps 1024-particle tiles (32 sub-steps of the copy ring per
+// ticket), a small one is spread over every warp of the grid instead of
+// running a few long tiles serially.  Results do not depend on the tile:
+// draws are keyed by particle index and children are written in index
+// order.  The tile counters hold SFP_TILE_TARGET tiles plus the segments'
+// padding at least, so the rule always fits.
+#define SFP_TILE_MIN 32
+#define SFP_TILE_MAX 1024
+#define SFP_TILE_TARGET 4096
+
 struct sfp_step_state {
     double t;                   // time of the prepared / running step
     long long step;             // steps completed
@@ -33,9 +46,11 @@ struct sfp_step_state {
     int skip;                   // 1: the prepared step must not run
     int halted;                 // sticky: a destination lacked room (host regrows, resumes)
     int error;                  // sticky device error (SFP_DEV_*)
-    int pad0;
+    int mtile;                  // particles per massive-group tile of the prepared step
     int pending;                // a prepared step awaits folding
     int append_wait;            // the prepared step stopped before writing its children (no room)
+    int ptile;                  // particles per photon-group tile of the prepared step
+    int pad0;
     long long particle_steps;   // sum over executed steps of all N_buffered
 };
 
@@ -60,7 +75,7 @@ struct sfp_run_dev {
     double dt;
     double photon_threshold;
     int qed;                    // SFP_QED_*
-    int tile;                   // particles per (warp) tile, both groups
+    int pad_tile;
     int any_rad;                // some massive segment radiates
     int any_bw;                 // some photon segment creates pairs
     int n_dseg;                 // segments receiving children (photons or pairs)

@@ -34,12 +34,9 @@
 #include "sfp_mlp.cuh"
 #include "sfp_run.cuh"
 
+// threads per block of the group kernels (8 warps, each on its own tiles)
 #ifndef SFP_TILE
 #define SFP_TILE 256
-#endif
-// warp tile of both groups: SFP_WSUB sub-steps of 32 particles
-#ifndef SFP_WSUB
-#define SFP_WSUB 32
 #endif
 // tiles per super-tile of the event scan
 #define SFP_SUPER_TILE 64
@@ -502,18 +499,35 @@ __device__ __forceinline__ int sfp_find_group_pos(const long long* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Bookkeeping: fold the appends of the step that ran, advance t; then
-// (prepare) the tile maps of both groups, tickets, super-tile counts.
-// One block of 256 threads.
+// (prepare, bit 0) each group's tile length and tile map, tickets,
+// super-tile counts.  Bits 1 and 2 of `prepare`: the step's massive /
+// photon launch is the long-tile kernel, so that group's tiles must be
+// SFP_TILE_MAX long.  One block of 256 threads.
 // ---------------------------------------------------------------------------
-SFP_DEVICE_INLINE long long sfp_group_map(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G) {
+SFP_DEVICE_INLINE long long sfp_group_map(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G, int tile) {
     long long acc = 0;
     for (int j = 0; j < G.n_seg; ++j) {
         acc = (acc + SFP_SUPER_TILE - 1) / SFP_SUPER_TILE * SFP_SUPER_TILE;
         G.tile_start[j] = acc;
-        acc += (R->n_buffered[G.seg[j]] + R->tile - 1) / R->tile;
+        acc += (R->n_buffered[G.seg[j]] + tile - 1) / tile;
     }
     G.tile_start[G.n_seg] = acc;
     return acc;
+}
+
+// the group's tile of this step (SFP_TILE_MIN..SFP_TILE_MAX, a power of two)
+// and its tile map; a map too long for the counters takes a longer tile
+SFP_DEVICE_INLINE long long sfp_group_plan(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G, int& tile) {
+    long long n = 0;
+    for (int j = 0; j < G.n_seg; ++j) n += R->n_buffered[G.seg[j]];
+    tile = SFP_TILE_MIN;
+    while (tile < SFP_TILE_MAX && (long long)tile * SFP_TILE_TARGET < n) tile <<= 1;
+    long long tiles = sfp_group_map(R, G, tile);
+    while (tiles > G.max_tiles && tile < SFP_TILE_MAX) {
+        tile <<= 1;
+        tiles = sfp_group_map(R, G, tile);
+    }
+    return tiles;
 }
 
 extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_dev* __restrict__ R, int prepare) {
@@ -547,14 +561,20 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
             ps += R->n_buffered[s];
         }
         // each segment's tiles start at a multiple of SFP_SUPER_TILE tiles
-        const long long m_tiles = sfp_group_map(R, R->mg);
-        const long long p_tiles = sfp_group_map(R, R->pg);
+        int mt = SFP_TILE_MAX, pt = SFP_TILE_MAX;
+        const long long m_tiles = sfp_group_plan(R, R->mg, mt);
+        const long long p_tiles = sfp_group_plan(R, R->pg, pt);
         if (m_tiles > R->mg.max_tiles || p_tiles > R->pg.max_tiles) {
             st->error = SFP_DEV_CAPACITY;
+            st->skip = 1;
+        } else if (((prepare & 2) && mt != SFP_TILE_MAX) || ((prepare & 4) && pt != SFP_TILE_MAX)) {
+            st->error = SFP_DEV_TILE;  // the long-tile kernels launched for a step with shorter tiles
             st->skip = 1;
         } else {
             st->n_mtiles = m_tiles;
             st->n_ptiles = p_tiles;
+            st->mtile = mt;
+            st->ptile = pt;
             st->mticket = 0;
             st->pticket = 0;
             st->skip = 0;
@@ -571,8 +591,8 @@ extern "C" __global__ void __launch_bounds__(256) sfp_book_kernel(const sfp_run_
 }
 
 // ---------------------------------------------------------------------------
-// The copy ring of both group kernels.  A warp streams its tile of
-// SFP_WSUB * 32 particles 32 at a time through STAGES shared-memory stages
+// The copy ring of both group kernels.  A warp streams its tile (32 to 1024
+// particles) 32 at a time through STAGES shared-memory stages
 // filled with cp.async, so the state of the next sub-steps is in flight
 // while the current one computes.  The copies and the stores address the
 // tile through a per-warp descriptor in shared memory, written once per
@@ -663,7 +683,7 @@ __device__ __forceinline__ void sfp_ring_issue_full(char* const* D, int sub, uns
 }
 
 // ---------------------------------------------------------------------------
-// Massive group.  Each warp takes tiles of SFP_WSUB * 32 particles by ticket
+// Massive group.  Each warp takes tiles of the step's length by ticket
 // (the next ticket in flight while the tile computes) and streams them
 // through the copy ring; after the tables are staged no block barrier is
 // taken.  Per particle: the photon event at t (rejection sampling or optical
@@ -672,11 +692,11 @@ __device__ __forceinline__ void sfp_ring_issue_full(char* const* D, int sub, uns
 // alive particle is pushed to t+dt (Boris / Boris-TBMT, LL/CLL) and stored.
 // The warp's event count goes to its tile's counter and its super-tile's.
 // ---------------------------------------------------------------------------
-template <int FORM, int QED, int STAGES, bool SPIN>
+template <int FORM, int QED, int STAGES, bool SPIN, bool LONG>
 __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
                                                          const sfp_mlp::Smem& M, const sfp_segment& S, char** desc,
-                                                         unsigned char* ring, int SB, long long base, long long left,
-                                                         double t, double dt, unsigned int step) {
+                                                         unsigned char* ring, int SB, int PT, long long base,
+                                                         long long left, double t, double dt, unsigned int step) {
     using namespace sfp;
     constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
     constexpr int NC = 6 + OD + (SPIN ? 3 : 0);
@@ -690,18 +710,25 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     __syncwarp();
     char* const* D = desc;
     unsigned int cnt = 0;
-    const bool full = left >= (long long)(32 * SFP_WSUB);
+    // LONG: a tile of SFP_TILE_MAX particles, 32 sub-steps of 32 with
+    // compile-time bounds; else the step's shorter tile, sub-steps up to its
+    // last particle (`len`, the tile length or fewer at a segment's end)
+    const int len = LONG ? SFP_TILE_MAX : (int)min(left, (long long)PT);
+    const bool full = LONG ? left >= (long long)SFP_TILE_MAX : len == PT;
     auto issue = [&](int sb, unsigned char* dst) {
         if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
-        else sfp_ring_issue<NC>(D, sb, left, dst, lane);
+        else sfp_ring_issue<NC>(D, sb, LONG ? left : (long long)len, dst, lane);
     };
 #pragma unroll
-    for (int k = 0; k < STAGES - 1; ++k) issue(k, ring + k * SB);
+    for (int k = 0; k < STAGES - 1; ++k) {
+        if (LONG || 32 * k < len) issue(k, ring + k * SB);
+        else cp_async_commit();  // a short tile: nothing to fetch, the group count stays
+    }
 #pragma unroll 1
-    for (int sub = 0; sub < SFP_WSUB; ++sub) {
+    for (int sub = 0; LONG ? sub < SFP_TILE_MAX / 32 : 32 * sub < len; ++sub) {
         __syncwarp();  // every lane has read the stage about to be refilled
         const int nsub = sub + STAGES - 1;
-        if (nsub < SFP_WSUB) issue(nsub, ring + (nsub % STAGES) * SB);
+        if (LONG ? nsub < SFP_TILE_MAX / 32 : 32 * nsub < len) issue(nsub, ring + (nsub % STAGES) * SB);
         else cp_async_commit();
         cp_async_wait<STAGES - 1>();
         __syncwarp();  // the stage of `sub` is complete for the whole warp
@@ -709,7 +736,7 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
         const double* sd = reinterpret_cast<const double*>(stg);
         const int e = sub * 32 + lane;  // particle index from the tile's first
         const long long i = base + e;
-        const bool alive = e < left && stg[NC * 256 + lane] == 0;
+        const bool alive = (LONG ? e < left : e < len) && stg[NC * 256 + lane] == 0;
         double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
         double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
         double tau = OD ? sd[192 + lane] : 0.0;
@@ -762,16 +789,19 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     return cnt;
 }
 
-template <int FORM, int QED, int STAGES>
+// LONG: the kernel of steps whose tiles are all SFP_TILE_MAX long (the host
+// launches it while the group's population guarantees that, and the
+// bookkeeping kernel refuses a step planned otherwise with SFP_DEV_TILE).
+template <int FORM, int QED, int STAGES, bool LONG>
 __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
     constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
-    constexpr int PT = 32 * SFP_WSUB;
     extern __shared__ __align__(16) double s_tab[];
     __shared__ char* s_desc[SFP_TILE / 32][6 + OD + 3 + 2];
     sfp_step_state* st = R->st;
     if (st->skip || st->n_mtiles == 0) return;
     const long long n_tiles = st->n_mtiles;
+    const int PT = LONG ? SFP_TILE_MAX : st->mtile;
     const double t = st->t;
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
@@ -796,11 +826,11 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
         unsigned int cnt = 0;
         if (base < N) {  // else: alignment padding between segments
             if (S.spin)
-                cnt = sfp_massive_tile<FORM, QED, STAGES, true>(R, T, M, S, s_desc[warp], ring, SB, base, N - base, t,
-                                                                dt, step);
+                cnt = sfp_massive_tile<FORM, QED, STAGES, true, LONG>(R, T, M, S, s_desc[warp], ring, SB, PT, base,
+                                                                      N - base, t, dt, step);
             else
-                cnt = sfp_massive_tile<FORM, QED, STAGES, false>(R, T, M, S, s_desc[warp], ring, SB, base, N - base, t,
-                                                                 dt, step);
+                cnt = sfp_massive_tile<FORM, QED, STAGES, false, LONG>(R, T, M, S, s_desc[warp], ring, SB, PT, base,
+                                                                       N - base, t, dt, step);
         }
         if (lane == 0) {
             R->mg.tile_cnt[tile] = cnt;
@@ -918,14 +948,13 @@ __device__ __forceinline__ void sfp_pair_enqueue(sfp_pair_queue<STATE>& q, unsig
     }
 }
 
-template <int FORM, int QED, int STAGES>
+template <int FORM, int QED, int STAGES, bool LONG>
 __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ R) {
     using namespace sfp;
     constexpr int OD = QED == SFP_QED_OPTICAL_DEPTH ? 1 : 0;
     constexpr bool QUEUE = QED == SFP_QED_REJECTION;
     constexpr int NC = 6 + OD;
     constexpr int SB = sfp_ring<NC>::STAGE_BYTES;
-    constexpr int PT = 32 * SFP_WSUB;
     extern __shared__ __align__(16) double s_tab[];
     __shared__ char* s_desc[SFP_TILE / 32][NC + 2];
     constexpr bool QSTATE = FORM == SFP_FORM_FP32;  // the queue holds the kept photons' state
@@ -934,6 +963,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
     const long long n_tiles = st->n_ptiles;
+    const int PT = LONG ? SFP_TILE_MAX : st->ptile;
     const double t = st->t;
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
@@ -963,24 +993,31 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             tile = __shfl_sync(0xffffffffu, tk, 0);
             continue;
         }
+        // LONG: 32 sub-steps of 32 with compile-time bounds; else sub-steps up
+        // to the tile's last photon (`len`: the tile length or fewer at a
+        // segment's end)
         const long long left = N - base;
+        const int len = LONG ? SFP_TILE_MAX : (int)min(left, (long long)PT);
         const bool bw = S.bw != 0, push = S.push != 0;
         __syncwarp();  // the previous tile's lanes are done with its descriptor, stages and queue
         if (lane < NC + 2) s_desc[warp][lane] = sfp_desc_slot<QED, false>(S, lane, base);
         __syncwarp();
         unsigned int cnt = 0, qn = 0;
-        const bool full = left >= (long long)PT;
+        const bool full = LONG ? left >= (long long)SFP_TILE_MAX : len == PT;
         auto issue = [&](int sb, unsigned char* dst) {
             if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
-            else sfp_ring_issue<NC>(D, sb, left, dst, lane);
+            else sfp_ring_issue<NC>(D, sb, LONG ? left : (long long)len, dst, lane);
         };
 #pragma unroll
-        for (int k = 0; k < STAGES - 1; ++k) issue(k, ring + k * SB);
+        for (int k = 0; k < STAGES - 1; ++k) {
+            if (LONG || 32 * k < len) issue(k, ring + k * SB);
+            else cp_async_commit();  // a short tile: nothing to fetch, the group count stays
+        }
 #pragma unroll 1
-        for (int sub = 0; sub < SFP_WSUB; ++sub) {
+        for (int sub = 0; LONG ? sub < SFP_TILE_MAX / 32 : 32 * sub < len; ++sub) {
             __syncwarp();  // every lane has read the stage about to be refilled
             const int nsub = sub + STAGES - 1;
-            if (nsub < SFP_WSUB) issue(nsub, ring + (nsub % STAGES) * SB);
+            if (LONG ? nsub < SFP_TILE_MAX / 32 : 32 * nsub < len) issue(nsub, ring + (nsub % STAGES) * SB);
             else cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncwarp();  // the stage of `sub` is complete for the whole warp
@@ -988,7 +1025,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             const double* sd = reinterpret_cast<const double*>(stg);
             const int e = sub * 32 + lane;  // photon index from the tile's first
             const long long i = base + e;
-            const bool alive = e < left && stg[NC * 256 + lane] == 0;
+            const bool alive = (LONG ? e < left : e < len) && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
             if (QUEUE) {
@@ -1315,11 +1352,10 @@ __device__ __forceinline__ void sfp_write_pair(const sfp_run_dev* __restrict__ R
 }
 
 template <int FORM, bool MASSIVE>
-__device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G,
+__device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G, int PT,
                                                 long long tile, unsigned int c, unsigned short* list, double t,
                                                 double dt) {
     using namespace sfp;
-    constexpr int PT = 32 * SFP_WSUB;
     const int lane = threadIdx.x & 31;
     const long long s = tile / SFP_SUPER_TILE;
     unsigned int part = 0u;
@@ -1330,17 +1366,18 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
     const double* __restrict__ P = R->inst[S.instance].field_params;
     const long long N = R->n_buf_step[G.seg[pos]];
     const long long base = (tile - G.tile_start[pos]) * (long long)PT;
+    const int len = (int)min(N - base, (long long)PT);  // the tile's particles
     // the tile's marked particles, in index order: lane q covers 16 flags per pass
     unsigned int n = 0u;
-    for (int q0 = 0; q0 < PT && n < c; q0 += 512) {
+    for (int q0 = 0; q0 < len && n < c; q0 += 512) {
         const int e0 = q0 + 16 * lane;
-        const long long i0 = base + e0;
+        const unsigned char* f = S.pruned + base + e0;
         unsigned int m = 0u;
-        if (i0 + 16 <= N) {
-            m = marks16(*reinterpret_cast<const uint4*>(S.pruned + i0));
+        if (e0 + 16 <= len) {
+            m = marks16(*reinterpret_cast<const uint4*>(f));
         } else {
             for (int b = 0; b < 16; ++b)
-                if (i0 + b < N && S.pruned[i0 + b] == SFP_MARK) m |= 1u << b;
+                if (e0 + b < len && f[b] == SFP_MARK) m |= 1u << b;
         }
         const unsigned int k = __popc(m);
         const unsigned int inc = warp_incl_scan(k);
@@ -1348,14 +1385,14 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
         while (m) {
             const int b = __ffs(m) - 1;
             m &= m - 1u;
-            if (w < (unsigned int)PT) list[w] = (unsigned short)(e0 + b);
+            if (w < (unsigned int)len) list[w] = (unsigned short)(e0 + b);
             ++w;
         }
         n += __shfl_sync(0xffffffffu, inc, 31);
     }
     __syncwarp();
     // never more children than the scan counted and made room for
-    n = min(min(n, c), (unsigned int)PT);
+    n = min(min(n, c), (unsigned int)len);
     for (unsigned int j0 = 0; j0 < n; j0 += 32) {
         const unsigned int j = j0 + lane;
         if (j < n) {
@@ -1369,10 +1406,11 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
 
 template <int FORM>
 __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__ R) {
-    __shared__ unsigned short s_list[SFP_TILE / 32][32 * SFP_WSUB];
+    __shared__ unsigned short s_list[SFP_TILE / 32][SFP_TILE_MAX];
     const sfp_step_state* st = R->st;
     if (st->skip || st->append_wait) return;
     const long long nm = R->any_rad ? st->n_mtiles : 0, np = R->any_bw ? st->n_ptiles : 0;
+    const int mt = st->mtile, pt = st->ptile;
     const long long n_all = nm + np;
     const double t = st->t;
     const double dt = R->dt;
@@ -1393,23 +1431,35 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
             busy &= busy - 1u;
             const long long tg = gw + (j0 + b) * nw;
             const unsigned int c = __shfl_sync(0xffffffffu, mc, b);
-            if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, tg, c, s_list[warp], t, dt);
-            else sfp_append_tile<FORM, false>(R, R->pg, tg - nm, c, s_list[warp], t, dt);
+            if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, mt, tg, c, s_list[warp], t, dt);
+            else sfp_append_tile<FORM, false>(R, R->pg, pt, tg - nm, c, s_list[warp], t, dt);
         }
     }
 }
 
 // kernels: sfp_massive_<form>_<qed>_s<stages>_b<blocks>,
 // sfp_photon_<form>_<qed>_s<stages>_b<blocks>, sfp_scan_kernel, sfp_appends_<form>
+// (long-tile kernels) and sfp_massive_<form>_<qed>_s<stages>_b<blocks>_t,
+// sfp_photon_..._t (any tile length: the steps of small populations)
 #define SFP_MASSIVE_KERNEL(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                             \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
         sfp_massive_##FORM_S##_##QED_S##_s##STAGES##_b##MINB(const sfp_run_dev* __restrict__ R) {             \
-        sfp_massive_body<FORM, QED, STAGES>(R);                                                              \
+        sfp_massive_body<FORM, QED, STAGES, true>(R);                                                        \
     }
 #define SFP_PHOTON_KERNEL(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                              \
     extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
         sfp_photon_##FORM_S##_##QED_S##_s##STAGES##_b##MINB(const sfp_run_dev* __restrict__ R) {              \
-        sfp_photon_body<FORM, QED, STAGES>(R);                                                               \
+        sfp_photon_body<FORM, QED, STAGES, true>(R);                                                         \
+    }
+#define SFP_MASSIVE_KERNEL_T(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                           \
+    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
+        sfp_massive_##FORM_S##_##QED_S##_s##STAGES##_b##MINB##_t(const sfp_run_dev* __restrict__ R) {         \
+        sfp_massive_body<FORM, QED, STAGES, false>(R);                                                       \
+    }
+#define SFP_PHOTON_KERNEL_T(FORM_S, QED_S, FORM, QED, STAGES, MINB)                                            \
+    extern "C" __global__ void __launch_bounds__(SFP_TILE, MINB)                                              \
+        sfp_photon_##FORM_S##_##QED_S##_s##STAGES##_b##MINB##_t(const sfp_run_dev* __restrict__ R) {          \
+        sfp_photon_body<FORM, QED, STAGES, false>(R);                                                        \
     }
 
 #if defined(SFP_STEP_FORM_FP64)
@@ -1422,11 +1472,15 @@ SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 2)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 3)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 3)
 SFP_PHOTON_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 2)
+SFP_MASSIVE_KERNEL_T(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
+SFP_PHOTON_KERNEL_T(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 3, 3)
 #else
 SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
 SFP_MASSIVE_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 2)
 SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 3)
 SFP_PHOTON_KERNEL(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 3)
+SFP_MASSIVE_KERNEL_T(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 2, 2)
+SFP_PHOTON_KERNEL_T(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif
 #endif
 #if defined(SFP_STEP_FORM_FP32)
@@ -1443,11 +1497,15 @@ SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 4)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
 SFP_PHOTON_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 4, 3)
+SFP_MASSIVE_KERNEL_T(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)
+SFP_PHOTON_KERNEL_T(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 3, 3)
 #else
 SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 3)
 SFP_MASSIVE_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 2)
 SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 4)
 SFP_PHOTON_KERNEL(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 3)
+SFP_MASSIVE_KERNEL_T(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 2, 3)
+SFP_PHOTON_KERNEL_T(fp32, od, SFP_FORM_FP32, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #endif
 #endif
 #endif  // SFP_WANT_STEP

@@ -116,12 +116,16 @@ def plan_chunk(species, rates, max_chunk, min_room=MIN_ROOM):
 
 
 def _release_cached_blocks():
-    """Return the device blocks that buffer growth outgrew to the driver.
-    Emptying the allocator's cache synchronises the device, so it is done
-    once a run has ended, never between its chunks."""
+    """Return the device blocks that buffer growth outgrew to the driver, and
+    the page-locked host blocks of earlier runs' copies that nothing holds any
+    more (the caching host allocator keeps them otherwise, rounded up to a
+    power of two).  Emptying the caches synchronises the device, so it is
+    done once a run has ended, never between its chunks."""
     import torch
     if torch.cuda.is_available() and torch.cuda.is_initialized():
         torch.cuda.empty_cache()
+        if hasattr(torch._C, "_host_emptyCache"):
+            torch._C._host_emptyCache()
 
 
 def observe_rates(species, before, steps, rates):

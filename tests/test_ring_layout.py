@@ -8,7 +8,6 @@ cover exactly the particles that exist.  Layouts: 6 components (x..uz), 7
 import numpy as np
 import pytest
 
-WSUB = 32  # sub-steps of 32 particles per warp tile (SFP_WSUB)
 
 
 def issue(nc, sub, left):
@@ -32,16 +31,19 @@ def issue(nc, sub, left):
     return out
 
 
+@pytest.mark.parametrize("tile", [32, 256, 1024])
 @pytest.mark.parametrize("nc", [6, 7, 9, 10])
 @pytest.mark.parametrize("left", [1024, 1000, 33, 32, 31, 17, 16, 1])
-def test_every_staged_value_lands_where_it_is_read(nc, left):
+def test_every_staged_value_lands_where_it_is_read(nc, left, tile):
+    """Sub-steps 0..tile/32-1 of a tile (32 to 1024 particles, a multiple of
+    32 from the segment's start, so its base stays 16-byte aligned)."""
     stage = nc * 32 * 8 + 32  # sfp_ring<NC>::STAGE_BYTES
-    for sub in range(WSUB):
+    for sub in range(tile // 32):
         owner = np.full(stage, -1, dtype=np.int64)  # which (slot, element) fills each byte
         for dst, slot, e, nb in issue(nc, sub, left):
             assert dst % 16 == 0 and dst + 16 <= stage
             if slot < nc:
-                assert e % 2 == 0  # 16-byte aligned source for a 1024-aligned tile base
+                assert e % 2 == 0  # 16-byte aligned source for a tile base at a multiple of 32
                 for b in range(nb):  # 8-byte elements e, e+1
                     assert owner[dst + b] == -1  # no byte is written twice
                     owner[dst + b] = slot * 1_000_000 + e + b // 8

@@ -1,16 +1,20 @@
 """The step's tile maps, event scan and children's slots, restated from
-their index arithmetic (sfparticles_b200/csrc/sfp_step.cuh: sfp_group_map,
-sfp_super_info, sfp_scan_group, marks16, sfp_append_tile) and checked on
-the CPU against the order the reference appends in: every particle in
-exactly one tile, segments on super-tile boundaries so a super-tile never
-spans two segments, each super-tile's prefix equal to the children that the
-same instance's earlier segments and tiles create on the same channel, and
-a tile's marked particles gathered in index order."""
+their index arithmetic (sfparticles_b200/csrc/sfp_step.cuh: sfp_group_plan,
+sfp_group_map, sfp_super_info, sfp_scan_group, marks16, sfp_append_tile;
+sfp_capi.cu: tiles_for) and checked on the CPU against the order the
+reference appends in: every particle in exactly one tile, segments on
+super-tile boundaries so a super-tile never spans two segments, each
+super-tile's prefix equal to the children that the same instance's earlier
+segments and tiles create on the same channel, a tile's marked particles
+gathered in index order, and the step's tile length (32 to 1024 by the
+population) always fitting the tile counters."""
 import numpy as np
 import pytest
 
 SUPER = 64  # SFP_SUPER_TILE
-TILE = 1024  # 32 * SFP_WSUB
+TILE = 1024  # SFP_TILE_MAX
+TILE_MIN, TILE_TARGET = 32, 4096  # SFP_TILE_MIN, SFP_TILE_TARGET
+TILES = [32, 64, 128, 256, 512, 1024]
 MARK = 2    # SFP_MARK
 
 
@@ -22,6 +26,26 @@ def group_map(n_buf, segs, tile=TILE):
         start.append(acc)
         acc += (n_buf[s] + tile - 1) // tile
     return start + [acc]
+
+
+def tiles_for(capacity, segs):
+    """sfp_capi.cu tiles_for: the tile counters a group is given."""
+    t = sum((capacity[s] + TILE - 1) // TILE + SUPER for s in segs)
+    return max(t, TILE_TARGET + len(segs) * (SUPER + 1)) + 1
+
+
+def group_plan(n_buf, segs, max_tiles):
+    """sfp_group_plan: the shortest power-of-two tile from 32 with at most
+    TILE_TARGET tiles of population, longer while the map overflows."""
+    n = sum(n_buf[s] for s in segs)
+    tile = TILE_MIN
+    while tile < TILE and tile * TILE_TARGET < n:
+        tile <<= 1
+    start = group_map(n_buf, segs, tile)
+    while start[-1] > max_tiles and tile < TILE:
+        tile <<= 1
+        start = group_map(n_buf, segs, tile)
+    return tile, start
 
 
 def find_group_pos(start, n, tk):
@@ -60,9 +84,9 @@ def scan(start, segs, inst, channel, sup):
     return pre
 
 
-def check_group(rng, n_buf, segs, inst, channel):
-    start = group_map(n_buf, segs)
-    own_tiles = [-(-n_buf[s] // TILE) for s in segs]  # the rest up to the next start is padding
+def check_group(rng, n_buf, segs, inst, channel, tile=TILE):
+    start = group_map(n_buf, segs, tile)
+    own_tiles = [-(-n_buf[s] // tile) for s in segs]  # the rest up to the next start is padding
     for j, s in enumerate(segs):
         assert start[j] % SUPER == 0 and start[j] + own_tiles[j] <= start[j + 1]
     if not segs or start[-1] == 0:
@@ -93,8 +117,9 @@ def check_group(rng, n_buf, segs, inst, channel):
         assert first == want, (tile, first, want)
 
 
+@pytest.mark.parametrize("tile", [32, 256, 1024])
 @pytest.mark.parametrize("seed", range(6))
-def test_tile_maps_and_prefixes_of_both_groups(seed):
+def test_tile_maps_and_prefixes_of_both_groups(seed, tile):
     rng = np.random.default_rng(seed)
     n_inst = int(rng.integers(1, 5))
     segs = []  # (instance, massless, channel)
@@ -106,8 +131,33 @@ def test_tile_maps_and_prefixes_of_both_groups(seed):
     n_buf = [int(rng.choice([0, 1, 31, 1023, 1024, 1025, int(rng.integers(0, 300_000))])) for _ in segs]
     mseg = [k for k, s in enumerate(segs) if not s[1]]
     pseg = [k for k, s in enumerate(segs) if s[1]]
-    check_group(rng, n_buf, mseg, inst, channel)  # photon children of the massive group
-    check_group(rng, n_buf, pseg, inst, channel)  # pair children of the photon group
+    check_group(rng, n_buf, mseg, inst, channel, tile)  # photon children of the massive group
+    check_group(rng, n_buf, pseg, inst, channel, tile)  # pair children of the photon group
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_the_step_tile_fits_the_counters(seed):
+    """For populations up to the capacities, the planned tile's map fits the
+    counters sized by tiles_for, the tile is the rule's (no fallback to a
+    longer one is ever needed), and a large population keeps 1024."""
+    rng = np.random.default_rng(100 + seed)
+    n_seg = int(rng.integers(1, 7))
+    segs = list(range(n_seg))
+    cap = [int(rng.choice([0, 1, 1000, 1 << 18, int(rng.integers(1, 1 << 24))])) for _ in segs]
+    max_tiles = tiles_for(cap, segs)
+    for _ in range(50):
+        n_buf = [int(rng.integers(0, c + 1)) for c in cap]
+        tile, start = group_plan(n_buf, segs, max_tiles)
+        assert tile in TILES and start[-1] <= max_tiles
+        n = sum(n_buf)
+        want = TILE_MIN
+        while want < TILE and want * TILE_TARGET < n:
+            want <<= 1
+        assert tile == want
+        if n > TILE * TILE_TARGET // 2:
+            assert tile == TILE
+        if tile < TILE:  # a short tile only where the population leaves warps idle at 1024
+            assert n <= tile * TILE_TARGET
 
 
 def vcmpeq4(a, b):
@@ -138,27 +188,31 @@ def test_marks16_finds_the_marked_bytes(seed):
         assert marks16(words) == want
 
 
+@pytest.mark.parametrize("tile", [32, 128, 1024])
 @pytest.mark.parametrize("left,frac", [(1024, 0.1), (1024, 1.0), (1000, 0.3), (513, 0.5), (17, 0.9), (1, 1.0)])
-def test_appends_gather_marks_in_index_order(left, frac):
+def test_appends_gather_marks_in_index_order(left, frac, tile):
     """sfp_append_tile's gather: lane q of a pass covers flags 16q..16q+15 of
     the pass's 512; each lane writes its marks at the warp's exclusive prefix
-    of mark counts; passes stop once the tile's count is reached."""
+    of mark counts; passes stop once the tile's count is reached.  Flags are
+    read up to the tile's end (min(N, base + tile)): a tile shorter than a
+    pass never reads the next tile's marks, which are planted here."""
     rng = np.random.default_rng(left)
-    flags = np.where(rng.random(TILE) < frac, MARK, rng.choice([0, 1], TILE)).astype(np.uint8)
-    flags[left:] = 0  # not part of the segment
-    c = int((flags[:left] == MARK).sum())
+    flags = np.where(rng.random(2 * TILE) < frac, MARK, rng.choice([0, 1], 2 * TILE)).astype(np.uint8)
+    flags[left:TILE] = 0  # past the segment's end
+    lim = min(left, tile)
+    c = int((flags[:lim] == MARK).sum())
     lst = [None] * TILE
     n = 0
-    for q0 in range(0, TILE, 512):
+    for q0 in range(0, tile, 512):
         if n >= c:
             break
         counts, masks = [], []
         for lane in range(32):
             e0 = q0 + 16 * lane
-            if e0 + 16 <= left:
+            if e0 + 16 <= lim:
                 m = marks16([int(x) for x in flags[e0:e0 + 16].view("<u4")])
             else:
-                m = sum(1 << b for b in range(16) if e0 + b < left and flags[e0 + b] == MARK)
+                m = sum(1 << b for b in range(16) if e0 + b < lim and flags[e0 + b] == MARK)
             masks.append(m)
             counts.append(bin(m).count("1"))
         incl = np.cumsum(counts)
@@ -172,4 +226,4 @@ def test_appends_gather_marks_in_index_order(left, frac):
                 w += 1
         n += int(incl[-1])
     assert n == c
-    assert lst[:n] == list(np.flatnonzero(flags[:left] == MARK))
+    assert lst[:n] == list(np.flatnonzero(flags[:lim] == MARK))
