@@ -165,6 +165,14 @@ typedef struct sfp_run_config {
     sfp_od_table od_pair;
 } sfp_run_config;
 
+/* A step module compiled with SFP_CONST_FIELD_N (a module for runs of one
+ * instance) holds the field parameters in its constant bank: a run on it
+ * must have n_inst == 1, and each sfp_run_steps / sfp_run_steps_timed /
+ * sfp_run_resume call first copies inst[0].field_params (SFP_CONST_FIELD_N
+ * doubles) there on the run's stream, after the launches of the previous
+ * call made on the same module by any run.  Calls on one module from
+ * several host threads are serialised.  Other modules read each instance's
+ * parameters from global memory. */
 int sfp_run_create(sfp_module *m, const sfp_run_config *cfg, int n_inst, const sfp_instance *inst, int n_seg,
                    const sfp_segment *seg, const int64_t *n_buffered, sfp_run **out);
 /* after buffers were regrown / moved: new segment table and counts

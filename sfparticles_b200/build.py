@@ -61,7 +61,8 @@ def prebuild_modules(verbose: bool = False):
     for f in fields.preset_structures():
         for form in ("fp64", "fp32"):
             for qed in ("rs", "od"):
-                program.get_module(f, form=form, qed=qed, load=False)
+                for single in (True, False):
+                    program.get_module(f, form=form, qed=qed, load=False, single=single)
         program.get_module(f, form=None, qed=None, load=False)
 
 

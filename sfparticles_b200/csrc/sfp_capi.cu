@@ -461,6 +461,12 @@ struct sfp_module {
     cudaLibrary_t lib = nullptr;
     std::mutex mu;
     std::unordered_map<std::string, cudaKernel_t> kernels;
+    // a module for runs of one instance holds that instance's field
+    // parameters in its constant bank (sfp_cfield); every run on the module
+    // copies its own block there before launching, after the launches of
+    // the run that used the module last (cf_done), under cf_mu
+    std::mutex cf_mu;
+    cudaEvent_t cf_done = nullptr;
 };
 
 static int module_kernel(sfp_module* m, const char* name, cudaKernel_t* out) {
@@ -552,6 +558,7 @@ int sfp_module_load(const void* image, size_t image_size, sfp_module** out) {
 
 int sfp_module_unload(sfp_module* m) {
     if (!m) return SFP_OK;
+    if (m->cf_done) cudaEventDestroy(m->cf_done);
     cudaError_t e = cudaLibraryUnload(m->lib);
     delete m;
     if (e != cudaSuccess) return fail(SFP_ECUDA, std::string("cudaLibraryUnload: ") + cudaGetErrorString(e));
@@ -792,6 +799,8 @@ struct sfp_group_host {
 
 struct sfp_run {
     sfp_module* mod = nullptr;
+    void* cfield = nullptr;  // the module's sfp_cfield (runs of one instance), or NULL
+    size_t cfield_bytes = 0;
     cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_appends = nullptr, k_book = nullptr;
     cudaKernel_t k_massive_t = nullptr, k_photon_t = nullptr;  // any tile length
     int grid_m = 0, grid_p = 0, grid_a = 0, grid_mt = 0, grid_pt = 0;
@@ -1005,6 +1014,24 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
         delete r;
         return rc;
     }
+    {
+        // a module built for runs of one instance reads the field parameters
+        // from its constant bank
+        void* cf = nullptr;
+        size_t cb = 0;
+        if (cudaLibraryGetGlobal(&cf, &cb, m->lib, "sfp_cfield") == cudaSuccess && cf) {
+            if (n_inst != 1) {
+                delete r;
+                return fail(SFP_EINVAL, "sfp_run_create: this step module serves runs of one instance (its field "
+                                        "parameters sit in its constant bank); compile it without that option for " +
+                                            std::to_string(n_inst) + " instances");
+            }
+            r->cfield = cf;
+            r->cfield_bytes = cb;
+        } else {
+            cudaGetLastError();  // no such symbol: parameters are read from global memory
+        }
+    }
     auto cleanup = [&](int code) {
         sfp_run_destroy(r);
         return code;
@@ -1136,6 +1163,31 @@ int sfp_run_update(sfp_run* r, int n_seg, const sfp_segment* seg, const int64_t*
     return run_upload(r, nullptr, n_buffered);
 }
 
+// Runs of one instance: their field parameters into the module's constant
+// bank on the run's stream, after the launches of every earlier call on the
+// same module (which read the bank).  The guard holds the module's lock
+// until the call has recorded its own launches (`done`).
+struct cfield_guard {
+    sfp_run* r;
+    std::unique_lock<std::mutex> lk;
+    explicit cfield_guard(sfp_run* run) : r(run) {
+        if (r->cfield) lk = std::unique_lock<std::mutex>(r->mod->cf_mu);
+    }
+    int put() {
+        if (!r->cfield) return SFP_OK;
+        sfp_module* m = r->mod;
+        if (!m->cf_done) SFP_CUDA(cudaEventCreateWithFlags(&m->cf_done, cudaEventDisableTiming));
+        else SFP_CUDA(cudaStreamWaitEvent(r->s, m->cf_done, 0));
+        SFP_CUDA(cudaMemcpyAsync(r->cfield, r->insts[0].field_params, r->cfield_bytes, cudaMemcpyDeviceToDevice, r->s));
+        return SFP_OK;
+    }
+    int done() {
+        if (!r->cfield) return SFP_OK;
+        SFP_CUDA(cudaEventRecord(r->mod->cf_done, r->s));
+        return SFP_OK;
+    }
+};
+
 // one step: book(prepare), massive, photon, scan + appends; ev (6 events)
 // brackets the massive, the photon and the scan + appends kernels when given.
 // mlong / plong: the group's steps all have SFP_TILE_MAX-long tiles, run by
@@ -1185,6 +1237,8 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
     cudaStream_t cs = as_stream(stream);
     SFP_CUDA(cudaEventRecord(r->ev_in, cs));
     SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    cfield_guard cg(r);
+    if (const int rc0 = cg.put()) return rc0;
     int64_t done = 0;
     const bool ml = long_tiles(r, r->mg.seg), pl = long_tiles(r, r->pg.seg);
     if (graph_chunk > 0 && nsteps >= graph_chunk) {
@@ -1212,6 +1266,7 @@ int sfp_run_steps(sfp_run* r, int64_t nsteps, int graph_chunk, void* stream) {
     }
     int rc = launch_fold(r);
     if (rc) return rc;
+    if ((rc = cg.done())) return rc;
     SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
     SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
     return SFP_OK;
@@ -1223,6 +1278,8 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     cudaStream_t cs = as_stream(stream);
     SFP_CUDA(cudaEventRecord(r->ev_in, cs));
     SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    cfield_guard cg(r);
+    if (const int rc0 = cg.put()) return rc0;
     std::vector<cudaEvent_t> ev(6 * nsteps, nullptr);
     int rc = SFP_OK;
     for (auto& e : ev)
@@ -1230,6 +1287,7 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     const bool ml = long_tiles(r, r->mg.seg), pl = long_tiles(r, r->pg.seg);
     for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k) rc = launch_unit(r, r->s, &ev[6 * k], ml, pl);
     if (rc == SFP_OK) rc = launch_fold(r);
+    if (rc == SFP_OK) rc = cg.done();
     if (rc == SFP_OK && cudaStreamSynchronize(r->s) != cudaSuccess) rc = fail(SFP_ECUDA, "synchronize");
     const bool has[3] = {!r->mg.seg.empty(), !r->pg.seg.empty(), !r->dseg.empty()};
     for (int64_t k = 0; k < nsteps && rc == SFP_OK; ++k)
@@ -1322,10 +1380,13 @@ int sfp_run_resume(sfp_run* r, void* stream) {
     SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
     SFP_CUDA(cudaMemcpyAsync(r->h.st, &st, sizeof(st), cudaMemcpyHostToDevice, r->s));
     SFP_CUDA(cudaStreamSynchronize(r->s));
+    cfield_guard cg(r);
+    if (const int rc0 = cg.put()) return rc0;
     void* a[] = {&r->d};
     SFP_CUDA(cudaLaunchKernel((const void*)r->k_appends, dim3(r->grid_a), dim3(SFP_TILE_HOST), a, 0, r->s));
-    const int rc = launch_fold(r);
+    int rc = launch_fold(r);
     if (rc) return rc;
+    if ((rc = cg.done())) return rc;
     SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
     SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
     return SFP_OK;

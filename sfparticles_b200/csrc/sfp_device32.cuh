@@ -24,6 +24,19 @@ constexpr float kInvEs = (float)(1.0 / kEs);
 constexpr float kCOverEs = (float)(sfp::kC / kEs);
 constexpr double kGammaSplit = 1.0e4;
 
+// float64 -> float32, rounded to nearest, as one conversion instruction.
+// The float32 form is compiled with float32 denormals flushed (-ftz=true),
+// under which a plain (float) cast of a double must also flush a denormal
+// result and takes two more instructions per conversion.  The values
+// converted here (positions, momenta, phases, parameters) are either 0 or
+// far above the float32 denormal range; a denormal result would in any case
+// be flushed by the float32 arithmetic it enters.
+SFP_DEVICE_INLINE float d2f(double v) {
+    float r;
+    asm("cvt.rn.f32.f64 %0, %1;" : "=f"(r) : "d"(v));
+    return r;
+}
+
 // cos / sin of a float32 phase of any size: reduce to [-pi, pi], then MUFU
 SFP_DEVICE_INLINE float cos_r(float a) {
     const float k = rintf(a * kInvTwoPi);
@@ -106,8 +119,8 @@ SFP_DEVICE_INLINE void field_gaussian_g(const double* __restrict__ P, double x, 
     const float E0 = g0.x, k0 = g0.y, inv_zR = g0.z, cq = g0.w, inv_w02 = g1.x, inv_kc2 = g1.y, dirc = g1.z;
     const float cep = g1.w, cp = g2.x, sp = g2.y, cut_r = g2.z, kc = g2.w;
     const double dir = P[5], x0 = P[6];
-    const float xf = (float)x, yf = (float)y, zf = (float)z;
-    const float xr = (float)((x - x0) - (dir * sfp::kC) * t);
+    const float xf = d2f(x), yf = d2f(y), zf = d2f(z);
+    const float xr = d2f((x - x0) - (dir * sfp::kC) * t);
     const float r2 = yf * yf + zf * zf;
     // |phi| >= k0 |xr| - k0 r2 / (4 zR) - pi/2 (as in the float64 form):
     // beyond kFieldCut32 kc the envelope is exactly 0, and so is the field.
@@ -150,12 +163,12 @@ SFP_DEVICE_INLINE void field_gaussian(const double* __restrict__ P, double x, do
 
 // simple_laser_pulse (fields.py:102-116)
 SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, double y, double z, double t, float F[6]) {
-    const float E0 = (float)P[0], k0 = (float)P[1], w0 = (float)P[2], ctau = (float)P[3];
+    const float E0 = d2f(P[0]), k0 = d2f(P[1]), w0 = d2f(P[2]), ctau = d2f(P[3]);
     const double dir = P[4], x0 = P[5];
-    const float cep = (float)P[6], cp = (float)P[7], sp = (float)P[8];
+    const float cep = d2f(P[6]), cp = d2f(P[7]), sp = d2f(P[8]);
     const int tord = (int)P[9];
-    const float yf = (float)y, zf = (float)z;
-    const float phi = k0 * (float)((dir * x - dir * x0) - sfp::kC * t);
+    const float yf = d2f(y), zf = d2f(z);
+    const float phi = k0 * d2f((dir * x - dir * x0) - sfp::kC * t);
     const float r2 = yf * yf + zf * zf;
     float num, den;
     const float kc = k0 * ctau;
@@ -168,12 +181,12 @@ SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, doub
         num = phi * phi;
         den = kc * kc;
     } else {
-        num = powf(phi, (float)P[9]);
-        den = powf(kc, (float)P[9]);
+        num = powf(phi, d2f(P[9]));
+        den = powf(kc, d2f(P[9]));
     }
     const float E = E0 * cos_r(phi + cep) * __expf(-(r2 / (w0 * w0)) - num / den);
     const float Ey = E * cp, Ez = E * sp;
-    const float d = (float)dir;
+    const float d = d2f(dir);
     F[0] = 0.0f;
     F[1] = Ey;
     F[2] = Ez;
@@ -184,7 +197,7 @@ SFP_DEVICE_INLINE void field_simple(const double* __restrict__ P, double x, doub
 
 SFP_DEVICE_INLINE void field_static(const double* __restrict__ P, float F[6]) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i) F[i] = (float)P[i];
+    for (int i = 0; i < 6; ++i) F[i] = d2f(P[i]);
 }
 
 // focused_gaussian_laser_pulse: evaluated in float64 (its eps^5 expansion
@@ -193,7 +206,7 @@ SFP_DEVICE_INLINE void field_focused(const double* __restrict__ P, double x, dou
     double D[6];
     sfp::field_focused(P, x, y, z, t, D);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) F[i] = (float)D[i];
+    for (int i = 0; i < 6; ++i) F[i] = d2f(D[i]);
 }
 
 // ---- chi (inline.py:126-134) in Schwinger units ----------------------------
@@ -210,11 +223,11 @@ SFP_DEVICE_INLINE float chi_of(const float F[6], float ux, float uy, float uz, f
 
 // gamma of u (float64 state), float64 above the split
 SFP_DEVICE_INLINE float gamma_of(double ux, double uy, double uz, bool massless) {
-    const float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    const float fx = d2f(ux), fy = d2f(uy), fz = d2f(uz);
     const float u2 = fx * fx + fy * fy + fz * fz;
     if (massless) return sqrtf(u2);
     if (u2 < (float)(kGammaSplit * kGammaSplit)) return sqrtf(1.0f + u2);
-    return (float)sqrt(((1.0 + ux * ux) + uy * uy) + uz * uz);
+    return d2f(sqrt(((1.0 + ux * ux) + uy * uy) + uz * uz));
 }
 
 // ---- rejection sampling (qed/rejection_sampling*.py) -----------------------
@@ -242,7 +255,7 @@ SFP_DEVICE_INLINE float rate_core(float chi_g, float base, const float* __restri
 // form's total-rate lookup (rate: the table staged as float32).  The optical
 // depth it is subtracted from stays float64.
 SFP_DEVICE_INLINE float od_rate(float chi, const sfp_od_table& t, const float* __restrict__ rate) {
-    const float lmin = (float)t.log_chi_min, ldel = (float)t.log_chi_delta, lmax = (float)t.log_chi_max;
+    const float lmin = d2f(t.log_chi_min), ldel = d2f(t.log_chi_delta), lmax = d2f(t.log_chi_max);
     float lc = log10f(chi);
     if (lc < lmin) return 0.0f;
     if (lc > lmax) lc = lmax;

@@ -154,7 +154,7 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
                                       const double* __restrict__ P, const sfp_pc32& K) {
     const float hc = K.hc;
     float g = sfp32::gamma_of(ux, uy, uz, false);
-    float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    float fx = sfp32::d2f(ux), fy = sfp32::d2f(uy), fz = sfp32::d2f(uz);
     float a = __fdividef(hc, g);
     x += (double)(a * fx);
     y += (double)(a * fy);
@@ -170,11 +170,11 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
         gm = sqrtf(1.0f + umx * umx + umy * umy + umz * umz);
     } else {
         const double dx = ux + (double)ex, dy = uy + (double)ey, dz = uz + (double)ez;
-        gm = (float)sqrt(((1.0 + dx * dx) + dy * dy) + dz * dz);
+        gm = sfp32::d2f(sqrt(((1.0 + dx * dx) + dy * dy) + dz * dz));
     }
     const float igm = __fdividef(1.0f, gm);
     if (S.spin) {  // inline.py:39-70: spin rotation with B_eff(u-), as an increment
-        const float ae = (float)S.ae;
+        const float ae = sfp32::d2f(S.ae);
         const float uB = umx * F[3] + umy * F[4] + umz * F[5];
         const float a1 = ae + igm, a2 = __fdividef(ae * gm, gm + 1.0f), a3 = ae + __fdividef(1.0f, gm + 1.0f);
         const float bex = a1 * F[3] - a2 * uB * umx - a3 * (umy * F[2] - umz * F[1]);
@@ -182,7 +182,7 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
         const float bez = a1 * F[5] - a2 * uB * umz - a3 * (umx * F[1] - umy * F[0]);
         const float Tx = bq * bex, Ty = bq * bey, Tz = bq * bez;
         const float f2 = __fdividef(2.0f, 1.0f + Tx * Tx + Ty * Ty + Tz * Tz);
-        const float s0x = (float)sx, s0y = (float)sy, s0z = (float)sz;
+        const float s0x = sfp32::d2f(sx), s0y = sfp32::d2f(sy), s0z = sfp32::d2f(sz);
         const float spx = s0x + (s0y * Tz - s0z * Ty), spy = s0y + (s0z * Tx - s0x * Tz), spz = s0z + (s0x * Ty - s0y * Tx);
         sx += (double)(f2 * (spy * Tz - spz * Ty));
         sy += (double)(f2 * (spz * Tx - spx * Tz));
@@ -197,7 +197,7 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
     uz += (double)(2.0f * ez + f2 * (upx * Ty - upy * Tx));
     g = sfp32::gamma_of(ux, uy, uz, false);
     if (S.rr == SFP_RR_LL || (S.rr == SFP_RR_CLL && !S.spin)) {  // inline.py:104-123
-        fx = (float)ux; fy = (float)uy; fz = (float)uz;
+        fx = sfp32::d2f(ux); fy = sfp32::d2f(uy); fz = sfp32::d2f(uz);
         const float chi = sfp32::chi_of(F, fx, fy, fz, g);
         float factor = K.ll;
         if (S.rr == SFP_RR_CLL) {
@@ -211,14 +211,14 @@ SFP_DEVICE_INLINE void push_massive32(double& x, double& y, double& z, double& u
         g = sfp32::gamma_of(ux, uy, uz, false);
     }
     a = __fdividef(hc, g);
-    x += (double)(a * (float)ux);
-    y += (double)(a * (float)uy);
-    z += (double)(a * (float)uz);
+    x += (double)(a * sfp32::d2f(ux));
+    y += (double)(a * sfp32::d2f(uy));
+    z += (double)(a * sfp32::d2f(uz));
 }
 
 SFP_DEVICE_INLINE void push_photon32(double& x, double& y, double& z, double ux, double uy, double uz, double dt) {
-    const float fx = (float)ux, fy = (float)uy, fz = (float)uz;
-    const float a = (float)(kC * dt) * rsqrtf(fx * fx + fy * fy + fz * fz);
+    const float fx = sfp32::d2f(ux), fy = sfp32::d2f(uy), fz = sfp32::d2f(uz);
+    const float a = sfp32::d2f(kC * dt) * rsqrtf(fx * fx + fy * fy + fz * fz);
     x += (double)(a * fx);
     y += (double)(a * fy);
     z += (double)(a * fz);
@@ -227,6 +227,30 @@ SFP_DEVICE_INLINE void push_photon32(double& x, double& y, double& z, double ux,
 }  // namespace sfp
 
 #if defined(SFP_WANT_STEP)
+
+// ---------------------------------------------------------------------------
+// Field parameters.  A module built for runs of one instance (a Simulation)
+// defines SFP_CONST_FIELD_N, the length of its field's parameter block, and
+// reads the block from this module's constant bank: the field program's
+// reads are at compile-time offsets, so they become constant operands of
+// the arithmetic instead of loads.  The host copies the run's block into
+// sfp_cfield on the run's stream before each launch sequence (sfp_capi.cu,
+// runs sharing a module are ordered).  Modules for several instances read
+// each instance's block from global memory.
+// ---------------------------------------------------------------------------
+#if defined(SFP_CONST_FIELD_N)
+// (a variable at global scope: its name is not mangled)
+__constant__ __align__(16) double sfp_cfield[SFP_CONST_FIELD_N];
+#endif
+
+SFP_DEVICE_INLINE const double* sfp_field_params(const sfp_instance& I) {
+#if defined(SFP_CONST_FIELD_N)
+    (void)I;
+    return sfp_cfield;
+#else
+    return I.field_params;
+#endif
+}
 
 // ---------------------------------------------------------------------------
 // QED tables staged in shared memory (float64, or float32 copies for FP32)
@@ -335,7 +359,7 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
         float F[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (S.push) sfp_field_program32(x, y, z, t, P, F);
         const float g = sfp32::gamma_of(ux, uy, uz, false);
-        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+        const float chi = sfp32::chi_of(F, sfp32::d2f(ux), sfp32::d2f(uy), sfp32::d2f(uz), g);
         if (QED == SFP_QED_REJECTION) {
             // straight-line: the draw and the rate for every lane, the
             // conditions combined at the end (chi = 0 gives W = 0)
@@ -345,8 +369,8 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
             const float dl = r1 * r1 * r1;
             const float base = __fdividef(dl, (1.0f - dl) * chi);
             const float W = -kRate * sfp32::rate_core(dl * chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, 1.0f);
-            ev = (chi > 0.0f) & (r2 < 3.0f * r1 * r1 * W * __fdividef((float)dt, g)) &
-                 !(dl * g < (float)R->photon_threshold);
+            ev = (chi > 0.0f) & (r2 < 3.0f * r1 * r1 * W * __fdividef(sfp32::d2f(dt), g)) &
+                 !(dl * g < sfp32::d2f(R->photon_threshold));
             d = (double)dl;
         } else {
             // float32 rate lookup, float64 optical depth
@@ -403,7 +427,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
         const bool field = F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f || F[5] != 0.f;
         if (field) {
             const float g = sfp32::gamma_of(ux, uy, uz, true);
-            const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+            const float chi = sfp32::chi_of(F, sfp32::d2f(ux), sfp32::d2f(uy), sfp32::d2f(uz), g);
             if (QED == SFP_QED_REJECTION) {
                 if (chi > 0.0f && !((double)chi < T.chi_pair_min)) {
                     float r1, r2;
@@ -412,7 +436,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                     const float base = __fdividef(1.0f, (r1 * (1.0f - r1)) * chi);
                     const float W =
                         kRate * sfp32::rate_core(chi, base, T.iAf, T.dAf, T.inv_dzf, T.zN, T.base_maxf, -1.0f);
-                    ev = r2 < W * __fdividef((float)dt, g);
+                    ev = r2 < W * __fdividef(sfp32::d2f(dt), g);
                     d = (double)r1;
                 }
             } else {
@@ -634,7 +658,11 @@ SFP_DEVICE_INLINE char* sfp_desc_slot(const sfp_segment& S, int c, long long bas
 // flags, always to dst + 16 c, so components land at dst + 256 comp and the
 // flags at dst + 256 NC.  `left` = particles of the segment from the tile's
 // first on; entries past them are zero-filled and not read.  One commit group.
-template <int NC>
+// Every segment has components 0-5 (x .. uz) and, in the spin variant, the
+// spin components; only component 6 under optical depth (tau) can be absent,
+// so only copies that can read it test for a NULL array (at compile time
+// for the others: copy c = lane + 32 k reads components 2k and 2k + 1).
+template <int NC, int OD>
 __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long long left, unsigned char* dst,
                                                int lane) {
     constexpr int NCOPY = NC * 16 + 2;
@@ -647,7 +675,7 @@ __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long lon
             const char* src = D[c >> 4];
             unsigned int nb = 16u;
             if (!full) nb = left - e >= 2 ? 16u : (left - e == 1 ? 8u : 0u);
-            if (!src) nb = 0u;  // the segment has no such array
+            if (OD && 2 * k <= 6 && 6 <= 2 * k + 1 && !src) nb = 0u;  // the segment has no tau array
             sfp::cp_async16(dst + c * 16, nb ? (const void*)(src + (size_t)e * 8) : (const void*)D[NC], nb);
         } else if (c < NCOPY) {
             const int e = sub * 32 + 16 * (c - NC * 16);
@@ -665,7 +693,7 @@ __device__ __forceinline__ void sfp_ring_issue(char* const* D, int sub, long lon
 // of the tile (or the flags at 32 sub + 16 (c - 16 NC)), straight from the
 // descriptor, with none of the general issue's bounds arithmetic; a
 // component the segment lacks is zero-filled.
-template <int NC>
+template <int NC, int OD>
 __device__ __forceinline__ void sfp_ring_issue_full(char* const* D, int sub, unsigned char* dst, int lane) {
     constexpr int NCOPY = NC * 16 + 2;
     const unsigned int off = (unsigned int)sub * 256u + 16u * (unsigned int)(lane & 15);
@@ -674,7 +702,8 @@ __device__ __forceinline__ void sfp_ring_issue_full(char* const* D, int sub, uns
         const int c = lane + 32 * k;
         if (c < NC * 16) {
             const char* p = D[c >> 4];
-            sfp::cp_async16(dst + c * 16, p ? (const void*)(p + off) : (const void*)D[NC], p ? 16u : 0u);
+            const bool has = !(OD && 2 * k <= 6 && 6 <= 2 * k + 1) || p != nullptr;  // see sfp_ring_issue
+            sfp::cp_async16(dst + c * 16, has ? (const void*)(p + off) : (const void*)D[NC], has ? 16u : 0u);
         } else if (c < NCOPY) {
             sfp::cp_async16(dst + c * 16, D[NC] + sub * 32 + 16 * (c - NC * 16), 16u);
         }
@@ -702,7 +731,7 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     constexpr int NC = 6 + OD + (SPIN ? 3 : 0);
     const int lane = threadIdx.x & 31;
     const sfp_instance& I = R->inst[S.instance];
-    const double* __restrict__ P = I.field_params;
+    const double* __restrict__ P = sfp_field_params(I);
     const bool rad = S.radiating != 0, push = S.push != 0;
     const sfp_pc32 K32 = push_consts32(S, t, dt);  // float32 form's push constants of this segment
     __syncwarp();  // the previous tile's lanes are done with the descriptor and the stages
@@ -716,8 +745,8 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
     const int len = LONG ? SFP_TILE_MAX : (int)min(left, (long long)PT);
     const bool full = LONG ? left >= (long long)SFP_TILE_MAX : len == PT;
     auto issue = [&](int sb, unsigned char* dst) {
-        if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
-        else sfp_ring_issue<NC>(D, sb, LONG ? left : (long long)len, dst, lane);
+        if (full) sfp_ring_issue_full<NC, OD>(D, sb, dst, lane);
+        else sfp_ring_issue<NC, OD>(D, sb, LONG ? left : (long long)len, dst, lane);
     };
 #pragma unroll
     for (int k = 0; k < STAGES - 1; ++k) {
@@ -725,14 +754,19 @@ __device__ __forceinline__ unsigned int sfp_massive_tile(const sfp_run_dev* __re
         else cp_async_commit();  // a short tile: nothing to fetch, the group count stays
     }
 #pragma unroll 1
-    for (int sub = 0; LONG ? sub < SFP_TILE_MAX / 32 : 32 * sub < len; ++sub) {
+    // rd: the stage of `sub` (sub % STAGES); the stage refilled, that of
+    // sub + STAGES - 1, is the one before it
+    for (int sub = 0, rd = 0; LONG ? sub < SFP_TILE_MAX / 32 : 32 * sub < len;
+         ++sub, rd = rd == STAGES - 1 ? 0 : rd + 1) {
         __syncwarp();  // every lane has read the stage about to be refilled
         const int nsub = sub + STAGES - 1;
-        if (LONG ? nsub < SFP_TILE_MAX / 32 : 32 * nsub < len) issue(nsub, ring + (nsub % STAGES) * SB);
-        else cp_async_commit();
+        if (LONG ? nsub < SFP_TILE_MAX / 32 : 32 * nsub < len)
+            issue(nsub, ring + (rd == 0 ? STAGES - 1 : rd - 1) * SB);
+        else
+            cp_async_commit();
         cp_async_wait<STAGES - 1>();
         __syncwarp();  // the stage of `sub` is complete for the whole warp
-        const unsigned char* stg = ring + (sub % STAGES) * SB;
+        const unsigned char* stg = ring + rd * SB;
         const double* sd = reinterpret_cast<const double*>(stg);
         const int e = sub * 32 + lane;  // particle index from the tile's first
         const long long i = base + e;
@@ -875,9 +909,9 @@ __device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict_
         const bool field = S.push && (F[0] != 0.f || F[1] != 0.f || F[2] != 0.f || F[3] != 0.f || F[4] != 0.f ||
                                       F[5] != 0.f);
         const float g = sfp32::gamma_of(ux, uy, uz, true);
-        const float chi = sfp32::chi_of(F, (float)ux, (float)uy, (float)uz, g);
+        const float chi = sfp32::chi_of(F, sfp32::d2f(ux), sfp32::d2f(uy), sfp32::d2f(uz), g);
         const bool some = chi > 0.0f && !((double)chi < T.chi_pair_min);
-        return field & some & !(pb[sfp_pair_bin(chi)] * __fdividef((float)R->dt, g) < 0x1p-33f);
+        return field & some & !(pb[sfp_pair_bin(chi)] * __fdividef(sfp32::d2f(R->dt), g) < 0x1p-33f);
     }
 }
 
@@ -985,7 +1019,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         const int si = R->pg.seg[pos];
         const sfp_segment& S = R->seg[si];
         const sfp_instance& I = R->inst[S.instance];
-        const double* __restrict__ P = I.field_params;
+        const double* __restrict__ P = sfp_field_params(I);
         const long long N = R->n_buf_step[si];
         const long long base = (tile - R->pg.tile_start[pos]) * (long long)PT;
         if (base >= N) {  // alignment padding between segments: no photons
@@ -1005,8 +1039,8 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         unsigned int cnt = 0, qn = 0;
         const bool full = LONG ? left >= (long long)SFP_TILE_MAX : len == PT;
         auto issue = [&](int sb, unsigned char* dst) {
-            if (full) sfp_ring_issue_full<NC>(D, sb, dst, lane);
-            else sfp_ring_issue<NC>(D, sb, LONG ? left : (long long)len, dst, lane);
+            if (full) sfp_ring_issue_full<NC, OD>(D, sb, dst, lane);
+            else sfp_ring_issue<NC, OD>(D, sb, LONG ? left : (long long)len, dst, lane);
         };
 #pragma unroll
         for (int k = 0; k < STAGES - 1; ++k) {
@@ -1363,7 +1397,7 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
     const long long pre = G.super_pre[s] + (long long)warp_sum(part);
     const int pos = sfp_find_group_pos(G.tile_start, G.n_seg, tile);
     const sfp_segment& S = R->seg[G.seg[pos]];
-    const double* __restrict__ P = R->inst[S.instance].field_params;
+    const double* __restrict__ P = sfp_field_params(R->inst[S.instance]);
     const long long N = R->n_buf_step[G.seg[pos]];
     const long long base = (tile - G.tile_start[pos]) * (long long)PT;
     const int len = (int)min(N - base, (long long)PT);  // the tile's particles

@@ -48,7 +48,10 @@ def _inline(text: str, seen: set) -> str:
     return _INCLUDE_RE.sub(rep, text.replace("#pragma once", ""))
 
 
-def module_source(field_src: str, form, qed) -> str:
+def module_source(field_src: str, form, qed, n_const=None) -> str:
+    """Source of a module.  ``n_const``: the length of the field's parameter
+    block when the module serves runs of one instance, which then read the
+    block from the module's constant bank (``sfp_cfield``)."""
     seen = set()
     head = _inline('#include "sfp_types.h"\n#include "sfp_device.cuh"\n#include "sfp_device32.cuh"\n', seen)
     parts = [head, "// ---- field program ----\n", field_src]
@@ -56,12 +59,22 @@ def module_source(field_src: str, form, qed) -> str:
         parts.append("#define SFP_WANT_FIELD_EVAL 1\n")
     else:
         parts.append(f"#define SFP_WANT_STEP 1\n#define SFP_STEP_FORM_{form.upper()} 1\n#define SFP_STEP_QED_{qed.upper()} 1\n")
+        if n_const:
+            parts.append(f"#define SFP_CONST_FIELD_N {int(n_const)}\n")
     parts.append(_inline('#include "sfp_step.cuh"\n', seen))
     return "".join(parts)
 
 
 def options(form=None):
-    return ["-arch=sm_100a", "-std=c++17", "-lineinfo", f"-DSFP_TILE={TILE}", "--fmad=true"]
+    """NVRTC options of a module.  The float32 form's step modules flush
+    float32 denormals and take float32 square roots and divisions from the
+    hardware approximations (within 2 ulp): its error budget is set by
+    float32 itself, and the exact IEEE sequences cost issue slots in kernels
+    that are issue-bound.  Float64 arithmetic is unaffected by these flags."""
+    opts = ["-arch=sm_100a", "-std=c++17", "-lineinfo", f"-DSFP_TILE={TILE}", "--fmad=true"]
+    if form == "fp32":
+        opts += ["-ftz=true", "-prec-sqrt=false", "-prec-div=false"]
+    return opts
 
 
 def _key(src: str, opts) -> str:
@@ -88,8 +101,12 @@ def compile_image(src: str, opts) -> bytes:
     return data
 
 
-def get_image(fields, form, qed) -> bytes:
-    src = module_source(fields.cuda_source(), form, qed)
+def get_image(fields, form, qed, single=False) -> bytes:
+    # the constant bank holds 64 KiB: a field of more than 256 terms keeps
+    # its parameters in global memory (the run finds no sfp_cfield)
+    n = len(fields.params())
+    n_const = n if (single and form is not None and 0 < n <= 4096) else None
+    src = module_source(fields.cuda_source(), form, qed, n_const)
     opts = options(form)
     key = _key(src, opts)
     path = os.path.join(CACHE, f"{key}.cubin")
@@ -123,15 +140,19 @@ class Module:
             pass
 
 
-def get_module(fields, form="fp64", qed="rs", load=True):
+def get_module(fields, form="fp64", qed="rs", load=True, single=False):
     """Module for (fields structure, form, qed); form=None gives the
-    field-evaluation module used by the per-op path."""
-    key = (fields.structure(), form, qed)
+    field-evaluation module used by the per-op path.  ``single``: a step
+    module for runs of one instance (field parameters in its constant bank,
+    copied there by the run); otherwise each instance's parameters are read
+    from global memory."""
+    single = bool(single) and form is not None
+    key = (fields.structure(), form, qed, single)
     with _lock:
         m = _modules.get(key)
         if m is not None:
             return m
-        img = get_image(fields, form, qed)
+        img = get_image(fields, form, qed, single)
         if not load:
             return None
         m = Module(img)

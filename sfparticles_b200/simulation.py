@@ -157,6 +157,10 @@ class Simulation(object):
         if form not in ("fp64", "fp32"):
             raise ValueError("form must be 'fp64' or 'fp32'")
         self.form = form
+        # the step module reads the field parameters from its constant bank
+        # (one instance per run); False: from global memory, the module
+        # kind an Ensemble uses
+        self._const_field = True
         if engine not in ("fused", "ops"):
             raise ValueError("engine must be 'fused' or 'ops'")
         if engine == "ops" and form != "fp64":
@@ -394,7 +398,7 @@ class Simulation(object):
         for p in self.all_particles:
             p._to_gpu()
             p._drop_scratch()
-        mod = program.get_module(self.fields, form=self.form, qed=self.qed_method)
+        mod = program.get_module(self.fields, form=self.form, qed=self.qed_method, single=self._const_field)
         params = self.fields.params_device(_device())
         inst = (_lib.Instance * 1)()
         inst[0].seed = self.seed
