@@ -46,7 +46,9 @@ STEPS_FULL = 3000
 DT = T0 / 100
 # algorithmic bytes per unit of work (float64 state in HBM, each byte moved once)
 BYTES_EPM = 97      # pushed e+-: x,y,z,ux,uy,uz read + written (96) + alive flag read
-BYTES_PHOTON = 73   # pushed photon: x,y,z,ux,uy,uz read (48) + flag (1) + x,y,z written (24)
+BYTES_PHOTON = 49   # photon in the step: x,y,z,ux,uy,uz + flag read; its push is the position epoch's advance,
+                    # so nothing is written (photons fly straight: positions are stored as of an epoch)
+BYTES_SYNC = 73     # photon positions written out (sfp_run_sync_positions): state + flag read, x,y,z written
 BYTES_DEAD = 1      # pruned slot: flag read
 BYTES_APPEND = 49   # appended particle: x,y,z,ux,uy,uz + flag written
 BYTES_EMIT_MARK = 9  # emitter in the massive kernel: delta (8) + mark (1) written instead of its state
@@ -56,10 +58,10 @@ BYTES_PAIR = 155    # pair event in the appends kernel: parent state + delta rea
                     # written (98)
 # DRAM bytes (read + write) over algorithmic bytes of one launch, from a
 # one-kernel ncu capture of the collision window at 1e6 e- (photon kernel:
-# 2.36e7 photons, 1.72 GB of state, larger than L2, so traffic scales with
-# the units processed): 1.176e9 + 0.544e9 against 1.719e9.  Only kernels
-# whose state exceeds L2 in that capture are listed.
-NCU_TRAFFIC_RATIO = {"photon": (1.176e9 + 0.544e9) / 1.719e9}
+# 2.38e7 photons, 1.17 GB of state, larger than L2, so traffic scales with
+# the units processed): 1.1695e9 read + 0.0002e9 written against 1.1680e9.
+# Only kernels whose state exceeds L2 in that capture are listed.
+NCU_TRAFFIC_RATIO = {"photon": (1.169514e9 + 0.206080e6) / 1.167978920e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
@@ -172,6 +174,7 @@ def run_c4(args):
     with ClockSampler(dev.index) as clk:
         e0.record()
         ens.run_on_device(args.steps)
+        ens._sync_positions()  # the photon positions written out: part of the timed work
         e1.record()
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -409,6 +412,7 @@ def run_c5(args):
             k = min(64, args.steps - done)
             sim.run_on_device(k)
             done += k
+        sim._sync_positions()  # the photon positions written out: part of the timed work
         e1.record()
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -516,6 +520,7 @@ def run_c1(args):
     with ClockSampler(dev.index) as clk:
         e0.record()
         sim.run_on_device(C1_STEPS)
+        sim._sync_positions()  # the photon positions written out: part of the timed work
         e1.record()
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -951,6 +956,7 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         e0.record()
         sim.run_on_device(n)
+        sim._sync_positions()  # the photon positions written out: part of the timed work
         e1.record()
         torch.cuda.synchronize()
         phases[name] = (e0.elapsed_time(e1), sim.particle_steps - ps_a, n)
@@ -979,6 +985,7 @@ def run_ours(args, rank, world):
     with ClockSampler(dev.index) as clk:
         e0.record()
         sim.run_on_device(args.steps)
+        sim._sync_positions()  # the photon positions written out: part of the timed work
         e1.record()
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -1103,6 +1110,7 @@ def run_ours(args, rank, world):
         ps_a = s.particle_steps
         e0.record()
         s.run_on_device(args.steps)
+        s._sync_positions()
         e1.record()
         torch.cuda.synchronize()
         fms = e0.elapsed_time(e1)

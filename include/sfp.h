@@ -192,6 +192,17 @@ int sfp_run_steps(sfp_run *r, int64_t nsteps, int graph_chunk, void *stream);
  * (k=1) kernels and of its scan + appends kernels (k=2); 0 for kernels the
  * run does not launch (3*nsteps entries). */
 int sfp_run_steps_timed(sfp_run *r, int64_t nsteps, float *kernel_ms, void *stream);
+/* Photon positions are stored as of the run's position epoch: the step
+ * kernels advance a photon's position in registers (photons fly straight,
+ * one push per step) and store nothing for a photon that does not convert.
+ * This writes every photon segment's positions out as of the current step
+ * (alive photons, and photons marked inside a step stopped for room) and
+ * moves the epoch there; asynchronous on `stream`.  Call it before reading
+ * photon x, y, z from the device, and before sfp_run_destroy when the
+ * arrays live on.  Momenta, flags, tau and every massive species are always
+ * current.  No counterpart in the reference, whose photon push
+ * (cpu.py:5-19) writes every step. */
+int sfp_run_sync_positions(sfp_run *r, void *stream);
 /* synchronous: state and per-segment buffered counts (n_seg entries) */
 int sfp_run_read_state(sfp_run *r, sfp_run_state *state, int64_t *n_buffered, void *stream);
 /* clear a halted flag that no stopped step holds */

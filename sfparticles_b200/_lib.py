@@ -103,6 +103,7 @@ _SIGS = {
     "sfp_run_clear_halt": ([P, P], c_i32),
     "sfp_run_pending_need": ([P, P], c_i32),
     "sfp_run_resume": ([P, P], c_i32),
+    "sfp_run_sync_positions": ([P, P], c_i32),
     "sfp_od_inverse_cdf": ([P, P, P, P, c_i64, P], c_i32),
     "sfp_mlp_make_samples": ([P, ctypes.c_uint64, ctypes.c_uint32, c_d, c_d, c_i64, P, P, P], c_i32),
     "sfp_mlp_grad": ([P, P, P, c_i64, P, P, P], c_i32),

@@ -803,6 +803,7 @@ struct sfp_run {
     size_t cfield_bytes = 0;
     cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_appends = nullptr, k_book = nullptr;
     cudaKernel_t k_massive_t = nullptr, k_photon_t = nullptr;  // any tile length
+    cudaKernel_t k_sync = nullptr, k_epoch = nullptr;           // photon positions written out
     int grid_m = 0, grid_p = 0, grid_a = 0, grid_mt = 0, grid_pt = 0;
     size_t smem_m = 0, smem_p = 0, smem_mt = 0, smem_pt = 0;
     std::vector<long long> nb_lo;  // lower bounds of the device's n_buffered (it only grows between reads)
@@ -1001,6 +1002,7 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     const std::string km = "sfp_massive_" + fq + "_s" + std::to_string(mstages) + "_b" + std::to_string(minb);
     const std::string kp = "sfp_photon_" + fq + "_s" + std::to_string(stages) + "_b" + std::to_string(pminb);
     const std::string ka = f64 ? "sfp_appends_fp64" : "sfp_appends_fp32";
+    const std::string ksy = f64 ? "sfp_sync_positions_fp64" : "sfp_sync_positions_fp32";
     const int t_minb = f64 ? 2 : 3;
     const std::string kmt = "sfp_massive_" + fq + "_s" + std::to_string(SFP_T_M_STAGES) + "_b" +
                             std::to_string(t_minb) + "_t";
@@ -1010,6 +1012,7 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
         (rc = module_kernel(m, kmt.c_str(), &r->k_massive_t)) || (rc = module_kernel(m, kpt.c_str(), &r->k_photon_t)) ||
         (rc = module_kernel(m, ka.c_str(), &r->k_appends)) ||
         (rc = module_kernel(m, "sfp_scan_kernel", &r->k_scan)) ||
+        (rc = module_kernel(m, ksy.c_str(), &r->k_sync)) || (rc = module_kernel(m, "sfp_epoch_kernel", &r->k_epoch)) ||
         (rc = module_kernel(m, "sfp_book_kernel", &r->k_book))) {
         delete r;
         return rc;
@@ -1101,6 +1104,7 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
     sfp_step_state st0{};
     st0.t = cfg->t0;
     st0.step = cfg->step0;
+    st0.pos_epoch = cfg->step0;  // the photon positions handed in are those at the start of step0
     st0.skip = 1;
     if (cudaMemcpyAsync(h.st, &st0, sizeof(st0), cudaMemcpyHostToDevice, r->s) != cudaSuccess)
         return cleanup(fail(SFP_ECUDA, "state upload"));
@@ -1300,6 +1304,20 @@ int sfp_run_steps_timed(sfp_run* r, int64_t nsteps, float* kernel_ms, void* stre
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (rc) return rc;
+    SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
+    SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
+    return SFP_OK;
+}
+
+int sfp_run_sync_positions(sfp_run* r, void* stream) {
+    if (!r) return fail(SFP_EINVAL, "sfp_run_sync_positions: NULL run");
+    if (r->pg.seg.empty()) return SFP_OK;
+    cudaStream_t cs = as_stream(stream);
+    SFP_CUDA(cudaEventRecord(r->ev_in, cs));
+    SFP_CUDA(cudaStreamWaitEvent(r->s, r->ev_in, 0));
+    void* a[] = {&r->d};
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_sync, dim3(4 * sm_count()), dim3(256), a, 0, r->s));
+    SFP_CUDA(cudaLaunchKernel((const void*)r->k_epoch, dim3(1), dim3(32), a, 0, r->s));
     SFP_CUDA(cudaEventRecord(r->ev_out, r->s));
     SFP_CUDA(cudaStreamWaitEvent(cs, r->ev_out, 0));
     return SFP_OK;

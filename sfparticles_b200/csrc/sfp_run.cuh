@@ -52,6 +52,12 @@ struct sfp_step_state {
     int ptile;                  // particles per photon-group tile of the prepared step
     int pad0;
     long long particle_steps;   // sum over executed steps of all N_buffered
+    // Photons fly straight: a photon segment stores each position as of the
+    // start of step pos_epoch, and the photon at the start of step `step`
+    // is at stored + (step - pos_epoch) * (its one-step displacement).  The
+    // step kernels advance positions in registers only; sfp_sync_positions
+    // writes them out and moves pos_epoch to step.
+    long long pos_epoch;
 };
 
 // one group of tiles (massive or photon): the tile map of its segments and

@@ -224,6 +224,29 @@ SFP_DEVICE_INLINE void push_photon32(double& x, double& y, double& z, double ux,
     z += (double)(a * fz);
 }
 
+// n steps of the photon push at once (n may be negative): a photon's
+// momentum does not change while it flies, so n pushes add n times the same
+// displacement.  float64: each push adds ((c dt/2) / |u|) u twice (cpu.py:
+// 5-19 with dt/2, push_photon); float32: (c dt / |u|) u as one float32
+// increment (push_photon32).  Equal to n successive pushes up to the
+// rounding of the float64 sum.
+template <int FORM>
+SFP_DEVICE_INLINE void photon_shift(double& x, double& y, double& z, double ux, double uy, double uz, double dt,
+                                    double n) {
+    if (FORM == SFP_FORM_FP64) {
+        const double k = ((kC * (0.5 * dt)) * inv_gamma_photon(ux, uy, uz)) * (2.0 * n);
+        x += k * ux;
+        y += k * uy;
+        z += k * uz;
+    } else {
+        const float fx = sfp32::d2f(ux), fy = sfp32::d2f(uy), fz = sfp32::d2f(uz);
+        const float a = sfp32::d2f(kC * dt) * rsqrtf(fx * fx + fy * fy + fz * fz);
+        x += n * (double)(a * fx);
+        y += n * (double)(a * fy);
+        z += n * (double)(a * fz);
+    }
+}
+
 }  // namespace sfp
 
 #if defined(SFP_WANT_STEP)
@@ -875,14 +898,17 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Photon group.  Same tiles, tickets and ring.  Per photon: the pair event
-// at t; a converted photon is marked (pruned = SFP_MARK, not pushed) and its
-// delta stored for the appends kernel; every other alive photon is pushed.
+// Photon group.  Same tiles, tickets and ring.  Per photon: the position at
+// t (stored position + (step - pos_epoch) pushes, photon_shift), the pair
+// event at t; a converted photon is marked (pruned = SFP_MARK, not pushed)
+// and its delta stored for the appends kernel.  A photon that does not
+// convert writes nothing: its push is the epoch's advance, so the kernel
+// reads 49 bytes per photon (state and flag) and writes only events.
 //
 // Rejection sampling: an event needs r2 < W(r1) dt / gamma, and r2 is never
 // below 2^-33 (float32 draws) or 2^-53 (float64 draws).  The pair-rate bound
 // of the photon's chi bin (R->pair_bound) times dt / gamma below that means
-// no draw passes: the photon is pushed at once, with no draw and no rate.
+// no draw passes: the photon is done at once, with no draw and no rate.
 // The photons it keeps (a few percent in a cascade) go, with their state,
 // to a 32-entry per-warp queue in shared memory and are tested in full 32
 // at a time, so the test's cost is paid by full warps instead of by every
@@ -929,14 +955,15 @@ struct sfp_pair_queue<true> {
     unsigned short e[32];
 };
 
-// the full pair test of the n queued photons (n <= 32), one per lane: mark
-// and store delta, or push and store; returns the events
+// the full pair test of the n queued photons (n <= 32), one per lane: a
+// converted photon is marked and its delta stored; returns the events
 template <int FORM, bool STATE>
 __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
                                                        const sfp_segment& S, const sfp_instance& I,
                                                        const double* __restrict__ P, char* const* D,
                                                        const sfp_pair_queue<STATE>& q, unsigned int n,
-                                                       long long base, double t, double dt, unsigned int step) {
+                                                       long long base, double t, double dt, unsigned int step,
+                                                       double lag) {
     using namespace sfp;
     const int lane = threadIdx.x & 31;
     bool ev = false;
@@ -946,10 +973,11 @@ __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __rest
         if constexpr (STATE) {
             x = q.x[lane], y = q.y[lane], z = q.z[lane];
             ux = q.ux[lane], uy = q.uy[lane], uz = q.uz[lane];
-        } else {  // the row, still as it was at t: the photon is written only below
+        } else {  // the row again, advanced to t as the main loop did
             x = reinterpret_cast<const double*>(D[0])[e], y = reinterpret_cast<const double*>(D[1])[e];
             z = reinterpret_cast<const double*>(D[2])[e], ux = reinterpret_cast<const double*>(D[3])[e];
             uy = reinterpret_cast<const double*>(D[4])[e], uz = reinterpret_cast<const double*>(D[5])[e];
+            if (S.push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);
         }
         double tau = 0.0, delta = 0.0;
         ev = sfp_pair_event<FORM, SFP_QED_REJECTION>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, base + e, tau,
@@ -957,12 +985,6 @@ __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __rest
         if (ev) {
             reinterpret_cast<unsigned char*>(D[6])[e] = SFP_MARK;
             reinterpret_cast<double*>(D[7])[e] = delta;
-        } else if (S.push) {
-            if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
-            else push_photon32(x, y, z, ux, uy, uz, dt);
-            reinterpret_cast<double*>(D[0])[e] = x;
-            reinterpret_cast<double*>(D[1])[e] = y;
-            reinterpret_cast<double*>(D[2])[e] = z;
         }
     }
     return __popc(__ballot_sync(0xffffffffu, ev));
@@ -1001,6 +1023,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     const double t = st->t;
     const double dt = R->dt;
     const unsigned int step = (unsigned int)st->step;
+    const double lag = (double)(st->step - st->pos_epoch);  // steps since the stored positions
     const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
     if (QUEUE)
         for (int k = threadIdx.x; k < SFP_PAIR_BOUND_BINS; k += blockDim.x) s_pb[k] = R->pair_bound[k];
@@ -1062,18 +1085,13 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             const bool alive = (LONG ? e < left : e < len) && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
+            // the position at t; the step's push is carried by the epoch
+            // (pos_epoch), so a photon that does not convert stores nothing
+            if (push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);
             if (QUEUE) {
-                // every lane runs the filter and the push (dead lanes on their
-                // zero-filled stage entries); only the stores are conditional
+                // every lane runs the filter (dead lanes on their zero-filled
+                // stage entries); only the queue writes are conditional
                 const bool keep = alive & bw & sfp_pair_possible<FORM>(R, T, s_pb, S, P, x, y, z, ux, uy, uz, t);
-                double px = x, py = y, pz = z;
-                if (FORM == SFP_FORM_FP64) push_photon(px, py, pz, ux, uy, uz, dt);
-                else push_photon32(px, py, pz, ux, uy, uz, dt);
-                if (!keep && alive && push) {
-                    reinterpret_cast<double*>(D[0])[e] = px;
-                    reinterpret_cast<double*>(D[1])[e] = py;
-                    reinterpret_cast<double*>(D[2])[e] = pz;
-                }
                 // kept photons fill the queue; a full queue is tested at once and
                 // the sub-step's remaining kept photons start the next one
                 const unsigned int kb = __ballot_sync(0xffffffffu, keep);
@@ -1081,7 +1099,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                 if (keep && slot < 32u) sfp_pair_enqueue(q, slot, e, x, y, z, ux, uy, uz);
                 if (qn + nk >= 32u) {
                     __syncwarp();  // the queue entries are written
-                    cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, 32u, base, t, dt, step);
+                    cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, 32u, base, t, dt, step, lag);
                     __syncwarp();  // every lane has read its entry
                     if (keep && slot >= 32u) sfp_pair_enqueue(q, slot - 32u, e, x, y, z, ux, uy, uz);
                     qn = qn + nk - 32u;
@@ -1098,12 +1116,6 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                     // converted photons are pruned, not pushed (cpu.py:190); marked until their pairs are written
                     reinterpret_cast<unsigned char*>(D[NC])[e] = SFP_MARK;
                     reinterpret_cast<double*>(D[NC + 1])[e] = delta;
-                } else if (alive && push) {
-                    if (FORM == SFP_FORM_FP64) push_photon(x, y, z, ux, uy, uz, dt);
-                    else push_photon32(x, y, z, ux, uy, uz, dt);
-                    reinterpret_cast<double*>(D[0])[e] = x;
-                    reinterpret_cast<double*>(D[1])[e] = y;
-                    reinterpret_cast<double*>(D[2])[e] = z;
                 }
                 if (OD && alive && bw && D[6]) reinterpret_cast<double*>(D[6])[e] = tau;
                 cnt += __popc(__ballot_sync(0xffffffffu, ev));
@@ -1111,7 +1123,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         }
         if (QUEUE && qn) {  // the tile's last kept photons
             __syncwarp();
-            cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, qn, base, t, dt, step);
+            cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, qn, base, t, dt, step, lag);
         }
         if (lane == 0) {
             R->pg.tile_cnt[tile] = cnt;
@@ -1317,7 +1329,7 @@ __device__ __forceinline__ void sfp_write_pair_child(const sfp_segment& D, long 
 template <int FORM>
 __device__ __forceinline__ void sfp_write_photon(const sfp_run_dev* __restrict__ R, const sfp_segment& S, long long i,
                                                  long long rank, long long pre, const double* __restrict__ P, double t,
-                                                 double dt) {
+                                                 double dt, double lag) {
     using namespace sfp;
     const sfp_segment& D = R->seg[S.photon_dest];
     const long long slot = R->n_buf_step[S.photon_dest] + pre + rank;
@@ -1326,10 +1338,10 @@ __device__ __forceinline__ void sfp_write_photon(const sfp_run_dev* __restrict__
     const double d = S.delta[i];
     double cx = x, cy = y, cz = z;
     const double cux = d * ux, cuy = d * uy, cuz = d * uz;
-    if (D.push) {
-        if (FORM == SFP_FORM_FP64) push_photon(cx, cy, cz, cux, cuy, cuz, dt);
-        else push_photon32(cx, cy, cz, cux, cuy, cuz, dt);
-    }
+    // the child is pushed in its creation step (simulation.py:117-121): at
+    // the next step it is at x + one push, so it is stored `lag` pushes
+    // behind x, as of pos_epoch like every photon of its segment
+    if (D.push) photon_shift<FORM>(cx, cy, cz, cux, cuy, cuz, dt, -lag);
     D.x[slot] = cx;
     D.y[slot] = cy;
     D.z[slot] = cz;
@@ -1373,10 +1385,18 @@ __device__ __forceinline__ void sfp_write_photon(const sfp_run_dev* __restrict__
 template <int FORM>
 __device__ __forceinline__ void sfp_write_pair(const sfp_run_dev* __restrict__ R, const sfp_segment& S, long long i,
                                                long long rank, long long pre, const double* __restrict__ P, double t,
-                                               double dt) {
+                                               double dt, double lag) {
     const double d = S.delta[i];
-    const double px = S.x[i], py = S.y[i], pz = S.z[i];
+    double px = S.x[i], py = S.y[i], pz = S.z[i];
     const double pux = S.ux[i], puy = S.uy[i], puz = S.uz[i];
+    // the converted photon at t, written out: it is pruned, and pruned
+    // photons keep their stored position (no later advance)
+    if (S.push) {
+        sfp::photon_shift<FORM>(px, py, pz, pux, puy, puz, dt, lag);
+        S.x[i] = px;
+        S.y[i] = py;
+        S.z[i] = pz;
+    }
     S.pruned[i] = 1;
     const long long be = R->n_buf_step[S.ele_dest] + pre + rank;
     const long long bp = R->n_buf_step[S.pos_dest] + pre + rank;
@@ -1388,7 +1408,7 @@ __device__ __forceinline__ void sfp_write_pair(const sfp_run_dev* __restrict__ R
 template <int FORM, bool MASSIVE>
 __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ R, const sfp_group_dev& G, int PT,
                                                 long long tile, unsigned int c, unsigned short* list, double t,
-                                                double dt) {
+                                                double dt, double lag) {
     using namespace sfp;
     const int lane = threadIdx.x & 31;
     const long long s = tile / SFP_SUPER_TILE;
@@ -1431,8 +1451,8 @@ __device__ __forceinline__ void sfp_append_tile(const sfp_run_dev* __restrict__ 
         const unsigned int j = j0 + lane;
         if (j < n) {
             const long long i = base + list[j];
-            if (MASSIVE) sfp_write_photon<FORM>(R, S, i, j, pre, P, t, dt);
-            else sfp_write_pair<FORM>(R, S, i, j, pre, P, t, dt);
+            if (MASSIVE) sfp_write_photon<FORM>(R, S, i, j, pre, P, t, dt, lag);
+            else sfp_write_pair<FORM>(R, S, i, j, pre, P, t, dt, lag);
         }
     }
     __syncwarp();  // the list is read before the next tile rewrites it
@@ -1448,6 +1468,7 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
     const long long n_all = nm + np;
     const double t = st->t;
     const double dt = R->dt;
+    const double lag = (double)(st->step - st->pos_epoch);  // photon positions: steps since stored
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -1465,8 +1486,8 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
             busy &= busy - 1u;
             const long long tg = gw + (j0 + b) * nw;
             const unsigned int c = __shfl_sync(0xffffffffu, mc, b);
-            if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, mt, tg, c, s_list[warp], t, dt);
-            else sfp_append_tile<FORM, false>(R, R->pg, pt, tg - nm, c, s_list[warp], t, dt);
+            if (tg < nm) sfp_append_tile<FORM, true>(R, R->mg, mt, tg, c, s_list[warp], t, dt, lag);
+            else sfp_append_tile<FORM, false>(R, R->pg, pt, tg - nm, c, s_list[warp], t, dt, lag);
         }
     }
 }
@@ -1496,9 +1517,48 @@ __device__ __forceinline__ void sfp_appends_body(const sfp_run_dev* __restrict__
         sfp_photon_body<FORM, QED, STAGES, false>(R);                                                        \
     }
 
+// ---------------------------------------------------------------------------
+// Photon positions written out (sfp_run_sync_positions): every photon of a
+// pushed photon segment that is not pruned (alive, or marked inside a step
+// that stopped for room) advances by the steps since pos_epoch; pruned
+// photons keep the position they were pruned at.  sfp_epoch_kernel, launched
+// after it, then moves pos_epoch to the current step (a second launch, so
+// that every block of the first has read the old epoch).
+// ---------------------------------------------------------------------------
+template <int FORM>
+__device__ __forceinline__ void sfp_sync_positions_body(const sfp_run_dev* __restrict__ R) {
+    const sfp_step_state* st = R->st;
+    const double lag = (double)(st->step - st->pos_epoch);
+    if (lag == 0.0) return;
+    const double dt = R->dt;
+    const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < R->pg.n_seg; ++k) {
+        const int si = R->pg.seg[k];
+        const sfp_segment& S = R->seg[si];
+        if (!S.push) continue;
+        const long long N = R->n_buffered[si];
+        for (long long i = first; i < N; i += stride) {
+            if (S.pruned[i] == 1) continue;
+            double x = S.x[i], y = S.y[i], z = S.z[i];
+            sfp::photon_shift<FORM>(x, y, z, S.ux[i], S.uy[i], S.uz[i], dt, lag);
+            S.x[i] = x;
+            S.y[i] = y;
+            S.z[i] = z;
+        }
+    }
+}
+
+extern "C" __global__ void __launch_bounds__(32) sfp_epoch_kernel(const sfp_run_dev* __restrict__ R) {
+    if (threadIdx.x == 0) R->st->pos_epoch = R->st->step;
+}
+
 #if defined(SFP_STEP_FORM_FP64)
 extern "C" __global__ void __launch_bounds__(SFP_TILE, 2) sfp_appends_fp64(const sfp_run_dev* __restrict__ R) {
     sfp_appends_body<SFP_FORM_FP64>(R);
+}
+extern "C" __global__ void __launch_bounds__(256) sfp_sync_positions_fp64(const sfp_run_dev* __restrict__ R) {
+    sfp_sync_positions_body<SFP_FORM_FP64>(R);
 }
 #if defined(SFP_STEP_QED_RS)
 SFP_MASSIVE_KERNEL(fp64, rs, SFP_FORM_FP64, SFP_QED_REJECTION, 2, 2)
@@ -1520,6 +1580,9 @@ SFP_PHOTON_KERNEL_T(fp64, od, SFP_FORM_FP64, SFP_QED_OPTICAL_DEPTH, 3, 3)
 #if defined(SFP_STEP_FORM_FP32)
 extern "C" __global__ void __launch_bounds__(SFP_TILE, 3) sfp_appends_fp32(const sfp_run_dev* __restrict__ R) {
     sfp_appends_body<SFP_FORM_FP32>(R);
+}
+extern "C" __global__ void __launch_bounds__(256) sfp_sync_positions_fp32(const sfp_run_dev* __restrict__ R) {
+    sfp_sync_positions_body<SFP_FORM_FP32>(R);
 }
 #if defined(SFP_STEP_QED_RS)
 SFP_MASSIVE_KERNEL(fp32, rs, SFP_FORM_FP32, SFP_QED_REJECTION, 2, 3)

@@ -25,7 +25,8 @@ from typing import Sequence
 
 from . import _lib, program
 from .particles import _device, _stream_ptr
-from .simulation import MIN_ROOM, Simulation, _release_cached_blocks, observe_rates, plan_chunk, resolve_pending
+from .simulation import (MIN_ROOM, Simulation, _release_cached_blocks, attach_position_sync, detach_position_sync,
+                         observe_rates, plan_chunk, resolve_pending, sync_positions)
 
 
 class Ensemble(object):
@@ -116,9 +117,15 @@ class Ensemble(object):
         self._run = run
         self._keep = (mod, params)
         self._ps_base = self.particle_steps
+        attach_position_sync(self, allp)
+
+    def _sync_positions(self):
+        sync_positions(self, self.species)
 
     def _end(self):
         if self._run is not None:
+            self._sync_positions()
+            detach_position_sync(self.species)
             _lib.load().sfp_run_destroy(self._run)
         self._run = None
         self._keep = None
@@ -164,6 +171,7 @@ class Ensemble(object):
             before = [p.N_buffered for p in allp]
             _lib.check(L.sfp_run_steps(self._run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
+            self._pos_dirty = True
             self.kernel_launches += self._launches_per_step() * chunk + 1
             done = self._sync_state(st, nbuf)
             halted = bool(st.halted)
@@ -194,6 +202,7 @@ class Ensemble(object):
         for _ in range(int(nstep)):
             ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
+            self._pos_dirty = True
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             self.kernel_launches += self._launches_per_step() + 1
             if st.error or (st.halted and not st.appends_pending):

@@ -53,6 +53,8 @@ _RR_CODE = {RadiationReactionType.NONE: 1, RadiationReactionType.PHOTON: 2, Radi
 _FLOAT_ATTRS_LAZY = ("chi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "photon_delta", "pair_delta")
 _BOOL_ATTRS_LAZY = ("event",)
 _BOOL_ATTRS = ("_to_be_pruned", "event")
+# attributes a device-resident run may hold as of its position epoch (photons)
+_POSITIONS = ("x", "y", "z")
 _SPECIES_COUNTER = [0]
 
 
@@ -151,6 +153,8 @@ class Particles(object):
             raise AttributeError(f"{type(self).__name__!s} has no attribute {name!r}")
         if name not in arr:
             self._materialize(name)
+        if d["_gpu"] and name in _POSITIONS:
+            self._sync_positions()
         a = arr[name]
         if not d["_gpu"]:
             return a
@@ -181,6 +185,15 @@ class Particles(object):
 
     def _touch(self):
         self.__dict__["_version"] += 1
+
+    def _sync_positions(self):
+        """A device-resident run that holds this photon species stores its
+        positions as of the run's position epoch (photons fly straight, and
+        the step kernels advance them in registers): have the run write them
+        out before they are read."""
+        f = self.__dict__.get("_pos_sync")
+        if f is not None:
+            f()
 
     def _materialize(self, name):
         n = self.buffer_size
@@ -218,12 +231,16 @@ class Particles(object):
             self._arr.pop(k, None)
         self._touch()
 
-    def _d(self, name):
-        """Device tensor of an attribute (species must be on the device)."""
+    def _d(self, name, sync=True):
+        """Device tensor of an attribute (species must be on the device).
+        sync=False: photon positions as stored (for handing the arrays to a
+        run, not for reading them)."""
         if not self._gpu:
             self._to_gpu()
         if name not in self._arr:
             self._materialize(name)
+        if sync and name in _POSITIONS:
+            self._sync_positions()
         return self._arr[name]
 
     def _p(self, name):
@@ -253,6 +270,7 @@ class Particles(object):
         if not self._gpu:
             return
         import torch
+        self._sync_positions()
         outs = []
         for k, v in list(self._arr.items()):
             h = _host_empty(v.shape, v.dtype)
@@ -491,6 +509,7 @@ class Particles(object):
         """Remove pruned particles and compact every array (particles.py:503-516)."""
         if self._gpu:
             import torch
+            self._sync_positions()
             # the kept slots once, then one gather per array
             idx = torch.nonzero(self._arr["_to_be_pruned"] == 0).flatten()
             for k, v in list(self._arr.items()):

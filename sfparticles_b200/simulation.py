@@ -128,6 +128,35 @@ def _release_cached_blocks():
             torch._C._host_emptyCache()
 
 
+def attach_position_sync(owner, species):
+    """A run stores its photons' positions as of its position epoch (the
+    step kernels advance them in registers: photons fly straight).  Each
+    photon species of the run gets a hook that writes them out before any
+    read of x, y, z (Particles._sync_positions)."""
+    owner._pos_dirty = False
+    for p in species:
+        if p.m == 0:
+            p.__dict__["_pos_sync"] = owner._sync_positions
+
+
+def detach_position_sync(species):
+    for p in species:
+        p.__dict__.pop("_pos_sync", None)
+
+
+def sync_positions(owner, species):
+    """sfp_run_sync_positions for a run that stepped since its last one."""
+    run = getattr(owner, "_run", None)
+    if run is None or not getattr(owner, "_pos_dirty", False):
+        return
+    owner._pos_dirty = False
+    _lib.check(_lib.load().sfp_run_sync_positions(run, _stream_ptr()), "sfp_run_sync_positions")
+    owner.kernel_launches = getattr(owner, "kernel_launches", 0) + 2
+    for p in species:
+        if p.m == 0:
+            p._touch()
+
+
 def observe_rates(species, before, steps, rates):
     """Update the append rates from the counts before and after `steps` steps."""
     if steps <= 0:
@@ -243,7 +272,7 @@ class Simulation(object):
         for i, p in enumerate(self.all_particles):
             s = segs[i]
             for k in ("x", "y", "z", "ux", "uy", "uz"):
-                setattr(s, k, p._d(k).data_ptr())
+                setattr(s, k, p._d(k, sync=False).data_ptr())
             s.pruned = p._d("_to_be_pruned").data_ptr()
             spin = "sx" in p.attrs
             if spin:
@@ -415,10 +444,16 @@ class Simulation(object):
         self._run = run
         self._keep = (mod, params)
         self._ps_base = self.particle_steps  # the device counter restarts with the run
+        attach_position_sync(self, self.all_particles)
+
+    def _sync_positions(self):
+        sync_positions(self, self.all_particles)
 
     def _end(self):
         run = getattr(self, "_run", None)
         if run is not None:
+            self._sync_positions()
+            detach_position_sync(self.all_particles)
             _lib.load().sfp_run_destroy(run)
         self._run = None
         self._keep = None
@@ -466,6 +501,7 @@ class Simulation(object):
         for _ in range(int(nstep)):
             ms = (ctypes.c_float * 3)()
             _lib.check(L.sfp_run_steps_timed(self._run, 1, ms, _stream_ptr()), "sfp_run_steps_timed")
+            self._pos_dirty = True
             _lib.check(L.sfp_run_read_state(self._run, ctypes.byref(st), nbuf, _stream_ptr()), "read_state")
             self.kernel_launches += self._launches_per_step() + 1
             if st.error or (st.halted and not st.appends_pending):
@@ -520,6 +556,7 @@ class Simulation(object):
             before = [p.N_buffered for p in self.all_particles]
             _lib.check(L.sfp_run_steps(run, chunk, self.graph_chunk if chunk >= self.graph_chunk else 0,
                                        _stream_ptr()), "sfp_run_steps")
+            self._pos_dirty = True
             self.kernel_launches += self._launches_per_step() * chunk + 1
             done = self._sync_state(run, st, nbuf)
             halted = bool(st.halted)

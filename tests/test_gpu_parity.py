@@ -362,6 +362,47 @@ def test_repeated_start_continues_the_run():
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_photon_positions_read_from_a_live_run(form):
+    """A device-resident run stores photon positions as of its position
+    epoch (the step kernels advance them in registers) and writes them out
+    when they are read.  Read in the middle of a run they equal those of a
+    run stopped at that step; a run read there continues to the end state of
+    one never read, up to float64 rounding of the two advances."""
+    cuda_or_skip()
+    import sfparticles_b200 as S
+    g = golden("ref_sim_cascade.npz")
+    case = json.loads(str(g["case"]))
+    n1, n2 = case["steps"] // 2, case["steps"] - case["steps"] // 2
+
+    def new():
+        species = sim_case_species(case, g["init"], g["spin_init"], "gpu")
+        return S.Simulation(*species, dt=float(g["dt"]), fields=golden_case_fields(g), print_every=None,
+                            photon_threshold=case["thr"], seed=case["seed"], form=form)
+
+    a = new()
+    a.run_on_device(n1)
+    pho = a.all_particles[2]
+    assert pho.m == 0
+    alive = ~pho._to_be_pruned[: pho.N_buffered]
+    mid = np.stack([getattr(pho, k)[: pho.N_buffered][alive] for k in ("x", "y", "z")])
+    assert mid.shape[1] > 100  # photons exist at the read
+    c = new()
+    c.run_on_device(n1)
+    c.finish()
+    np.testing.assert_array_equal(mid, np.stack([c.all_particles[2].x, c.all_particles[2].y, c.all_particles[2].z]))
+    a.run_on_device(n2)
+    a.finish()
+    b = new()
+    b.run_on_device(n1 + n2)
+    b.finish()
+    for p, q in zip(a.all_particles, b.all_particles):
+        assert p.N_buffered == q.N_buffered, (p.name, p.N_buffered, q.N_buffered)
+        got = np.stack([getattr(p, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+        ref = np.stack([getattr(q, k) for k in ("x", "y", "z", "ux", "uy", "uz")])
+        assert _rel(got, ref) < 1e-12, (p.name, _rel(got, ref))
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
 def test_kernel_variants_give_the_same_results(form):
     """Every variant of the massive kernel (items per thread, register
     budget) and of the photon kernel (sub-tiles in flight, register budget)
