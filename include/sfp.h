@@ -169,7 +169,8 @@ typedef struct sfp_run_config {
  * instance) holds the field parameters in its constant bank: a run on it
  * must have n_inst == 1, and each sfp_run_steps / sfp_run_steps_timed /
  * sfp_run_resume call first copies inst[0].field_params (SFP_CONST_FIELD_N
- * doubles) there on the run's stream, after the launches of the previous
+ * doubles), and the Philox round keys of inst[0].seed, there on the run's
+ * stream, after the launches of the previous
  * call made on the same module by any run.  Calls on one module from
  * several host threads are serialised.  Other modules read each instance's
  * parameters from global memory. */

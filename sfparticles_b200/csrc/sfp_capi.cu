@@ -801,6 +801,8 @@ struct sfp_run {
     sfp_module* mod = nullptr;
     void* cfield = nullptr;  // the module's sfp_cfield (runs of one instance), or NULL
     size_t cfield_bytes = 0;
+    void* ckeys = nullptr;           // the module's sfp_ckeys: the instance seed's Philox round keys
+    unsigned int* d_keys = nullptr;  // those keys, formed at creation (20 words, device)
     cudaKernel_t k_massive = nullptr, k_photon = nullptr, k_scan = nullptr, k_appends = nullptr, k_book = nullptr;
     cudaKernel_t k_massive_t = nullptr, k_photon_t = nullptr;  // any tile length
     cudaKernel_t k_sync = nullptr, k_epoch = nullptr;           // photon positions written out
@@ -1031,6 +1033,29 @@ int sfp_run_create(sfp_module* m, const sfp_run_config* cfg, int n_inst, const s
             }
             r->cfield = cf;
             r->cfield_bytes = cb;
+            void* ck = nullptr;
+            size_t kb = 0;
+            if (cudaLibraryGetGlobal(&ck, &kb, m->lib, "sfp_ckeys") != cudaSuccess || !ck || kb != 20 * sizeof(unsigned)) {
+                delete r;
+                return fail(SFP_EINVAL, "sfp_run_create: a one-instance step module without its Philox key array");
+            }
+            // the key schedule of Philox-4x32-10 for the instance seed: round r
+            // uses k0 + r 0x9E3779B9 and k1 + r 0xBB67AE85 (sfp::philox4x32_10)
+            unsigned int keys[20];
+            unsigned int k0 = (unsigned int)inst[0].seed, k1 = (unsigned int)(inst[0].seed >> 32);
+            for (int q = 0; q < 10; ++q) {
+                keys[2 * q] = k0;
+                keys[2 * q + 1] = k1;
+                k0 += 0x9E3779B9u;
+                k1 += 0xBB67AE85u;
+            }
+            if (cudaMalloc(&r->d_keys, sizeof(keys)) != cudaSuccess ||
+                cudaMemcpy(r->d_keys, keys, sizeof(keys), cudaMemcpyHostToDevice) != cudaSuccess) {
+                cudaFree(r->d_keys);
+                delete r;
+                return fail(SFP_ENOMEM, "sfp_run_create: Philox key array");
+            }
+            r->ckeys = ck;
         } else {
             cudaGetLastError();  // no such symbol: parameters are read from global memory
         }
@@ -1183,6 +1208,7 @@ struct cfield_guard {
         if (!m->cf_done) SFP_CUDA(cudaEventCreateWithFlags(&m->cf_done, cudaEventDisableTiming));
         else SFP_CUDA(cudaStreamWaitEvent(r->s, m->cf_done, 0));
         SFP_CUDA(cudaMemcpyAsync(r->cfield, r->insts[0].field_params, r->cfield_bytes, cudaMemcpyDeviceToDevice, r->s));
+        SFP_CUDA(cudaMemcpyAsync(r->ckeys, r->d_keys, 20 * sizeof(unsigned int), cudaMemcpyDeviceToDevice, r->s));
         return SFP_OK;
     }
     int done() {
@@ -1414,6 +1440,7 @@ int sfp_run_destroy(sfp_run* r) {
     if (!r) return SFP_OK;
     if (r->s) cudaStreamSynchronize(r->s);
     for (auto& kv : r->graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(r->d_keys);
     cudaFree((void*)r->h.seg);
     cudaFree((void*)r->h.inst);
     cudaFree(r->mg.d_seg);

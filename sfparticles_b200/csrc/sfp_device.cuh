@@ -88,11 +88,15 @@ SFP_DEVICE_INLINE double u01(unsigned int a, unsigned int b) {
     return ((double)k + 0.5) * 0x1p-52;
 }
 
+// the counter of a particle's draw: (slot lo, slot hi | purpose << 24, step, species stream)
+SFP_DEVICE_INLINE U4 philox_counter(unsigned int stream, unsigned int step, unsigned int purpose, long long slot) {
+    const unsigned long long s = (unsigned long long)slot;
+    return U4{(unsigned int)s, ((unsigned int)(s >> 32) & 0x00FFFFFFu) | (purpose << 24), step, stream};
+}
+
 SFP_DEVICE_INLINE void uniform2(unsigned long long seed, unsigned int stream, unsigned int step,
                                 unsigned int purpose, long long slot, double& r1, double& r2) {
-    const unsigned long long s = (unsigned long long)slot;
-    U4 c{(unsigned int)s, ((unsigned int)(s >> 32) & 0x00FFFFFFu) | (purpose << 24), step, stream};
-    U4 o = philox4x32_10(c, (unsigned int)seed, (unsigned int)(seed >> 32));
+    U4 o = philox4x32_10(philox_counter(stream, step, purpose, slot), (unsigned int)seed, (unsigned int)(seed >> 32));
     r1 = u01(o.x, o.y);
     r2 = u01(o.z, o.w);
 }

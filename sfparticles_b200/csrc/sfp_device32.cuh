@@ -52,13 +52,15 @@ SFP_DEVICE_INLINE float sin_r(float a) {
 // (sfp::uniform2: r1 <- word 0, r2 <- word 2), so both forms see the same
 // random numbers to float32 precision and make the same event decisions
 // except within float32 rounding of the acceptance threshold.
-SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, unsigned int step,
-                                 unsigned int purpose, long long slot, float& r1, float& r2) {
-    const unsigned long long s = (unsigned long long)slot;
-    sfp::U4 c{(unsigned int)s, ((unsigned int)(s >> 32) & 0x00FFFFFFu) | (purpose << 24), step, stream};
-    sfp::U4 o = sfp::philox4x32_10(c, (unsigned int)seed, (unsigned int)(seed >> 32));
+SFP_DEVICE_INLINE void uniform2f_of(sfp::U4 o, float& r1, float& r2) {
     r1 = ((float)(o.x >> 8) + 0.5f) * 0x1p-24f;
     r2 = __uint2float_rn(o.z) * 0x1p-32f + 0x1p-33f;
+}
+SFP_DEVICE_INLINE void uniform2f(unsigned long long seed, unsigned int stream, unsigned int step,
+                                 unsigned int purpose, long long slot, float& r1, float& r2) {
+    uniform2f_of(sfp::philox4x32_10(sfp::philox_counter(stream, step, purpose, slot), (unsigned int)seed,
+                                    (unsigned int)(seed >> 32)),
+                 r1, r2);
 }
 
 // atan of a float32, branch-free: t = min(|a|, 1/|a|), atan(t) = t P(t^2)

@@ -275,6 +275,44 @@ SFP_DEVICE_INLINE const double* sfp_field_params(const sfp_instance& I) {
 #endif
 }
 
+// The step's rejection-sampling draws: Philox-4x32-10 keyed by the instance
+// seed (sfp::uniform2 / sfp32::uniform2f).  A one-instance module takes the
+// ten rounds' keys (the seed's key schedule, k0 and k1 per round) from its
+// constant bank, copied by the host with the field parameters, instead of
+// forming them with two additions per round: the same numbers.
+#if defined(SFP_CONST_FIELD_N)
+__constant__ unsigned int sfp_ckeys[20];
+#endif
+
+SFP_DEVICE_INLINE sfp::U4 sfp_step_philox(sfp::U4 c, unsigned long long seed) {
+#if defined(SFP_CONST_FIELD_N)
+    (void)seed;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned int lo0 = 0xD2511F53u * c.x;
+        const unsigned int hi0 = __umulhi(0xD2511F53u, c.x);
+        const unsigned int lo1 = 0xCD9E8D57u * c.z;
+        const unsigned int hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = sfp::U4{hi1 ^ c.y ^ sfp_ckeys[2 * r], lo1, hi0 ^ c.w ^ sfp_ckeys[2 * r + 1], lo0};
+    }
+    return c;
+#else
+    return sfp::philox4x32_10(c, (unsigned int)seed, (unsigned int)(seed >> 32));
+#endif
+}
+
+SFP_DEVICE_INLINE void sfp_step_uniform2(unsigned long long seed, unsigned int stream, unsigned int step,
+                                         unsigned int purpose, long long slot, double& r1, double& r2) {
+    const sfp::U4 o = sfp_step_philox(sfp::philox_counter(stream, step, purpose, slot), seed);
+    r1 = sfp::u01(o.x, o.y);
+    r2 = sfp::u01(o.z, o.w);
+}
+
+SFP_DEVICE_INLINE void sfp_step_uniform2f(unsigned long long seed, unsigned int stream, unsigned int step,
+                                          unsigned int purpose, long long slot, float& r1, float& r2) {
+    sfp32::uniform2f_of(sfp_step_philox(sfp::philox_counter(stream, step, purpose, slot), seed), r1, r2);
+}
+
 // ---------------------------------------------------------------------------
 // QED tables staged in shared memory (float64, or float32 copies for FP32)
 // ---------------------------------------------------------------------------
@@ -367,7 +405,7 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
         if (QED == SFP_QED_REJECTION) {
             if (chi != 0.0) {
                 double r1, r2;
-                uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
+                sfp_step_uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
                 ev = photon_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
             }
         } else if (R->mlp_params) {
@@ -387,7 +425,7 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
             // straight-line: the draw and the rate for every lane, the
             // conditions combined at the end (chi = 0 gives W = 0)
             float r1, r2;
-            sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+            sfp_step_uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
             const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
             const float dl = r1 * r1 * r1;
             const float base = __fdividef(dl, (1.0f - dl) * chi);
@@ -436,7 +474,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
         if (QED == SFP_QED_REJECTION) {
             if (chi != 0.0 && !(chi < T.chi_pair_min)) {
                 double r1, r2;
-                uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
+                sfp_step_uniform2(I.seed, S.stream, step, 0u, i, r1, r2);
                 ev = pair_event_rs(chi, ig, dt, r1, r2, T.iAt, T.dAt, T.zN, T.zmax, d);
             }
         } else {
@@ -454,7 +492,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
             if (QED == SFP_QED_REJECTION) {
                 if (chi > 0.0f && !((double)chi < T.chi_pair_min)) {
                     float r1, r2;
-                    sfp32::uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
+                    sfp_step_uniform2f(I.seed, S.stream, step, 0u, i, r1, r2);
                     const float kRate = (float)((kAlpha * kMe) * (kC * kC) / kHbar);
                     const float base = __fdividef(1.0f, (r1 * (1.0f - r1)) * chi);
                     const float W =
