@@ -437,7 +437,7 @@ __device__ __forceinline__ bool sfp_photon_event(const sfp_run_dev* __restrict__
             // float32 rate lookup, float64 optical depth
             double u = 0.0;
             ev = !((double)chi < T.od_chi_min_ph) &&
-                 od_tau_step((double)sfp32::od_rate(chi, R->od_photon, T.od_phf), 1.0 / (double)g, dt, tau, I.seed,
+                 od_tau_step((double)sfp32::od_rate(chi, R->od_photon, T.od_phf), (double)__fdividef(1.0f, g), dt, tau, I.seed,
                              S.stream, step, i, u);
             if (R->mlp_params) {
                 d = u;
@@ -504,7 +504,7 @@ __device__ __forceinline__ bool sfp_pair_event(const sfp_run_dev* __restrict__ R
                 // float32 rate lookup, float64 optical depth
                 double u = 0.0;
                 ev = !((double)chi < T.od_chi_min_pa) &&
-                     od_tau_step((double)sfp32::od_rate(chi, R->od_pair, T.od_paf), 1.0 / (double)g, dt, tau, I.seed,
+                     od_tau_step((double)sfp32::od_rate(chi, R->od_pair, T.od_paf), (double)__fdividef(1.0f, g), dt, tau, I.seed,
                                  S.stream, step, i, u);
                 d = ev ? od_bisect((double)chi, u, R->od_pair) : 0.0;
             }
@@ -1099,9 +1099,34 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         __syncwarp();
         unsigned int cnt = 0, qn = 0;
         const bool full = LONG ? left >= (long long)SFP_TILE_MAX : len == PT;
+        // full long tiles of the float32 form without optical depth: each
+        // lane's three component copies (components 2k + lane/16, k = 0..2)
+        // read from per-tile pointers held in registers, lanes 0-1 copy the
+        // flags; no descriptor reads per stage.  (The float64 form and the
+        // any-tile kernel have no registers to spare for them.)
+        constexpr bool REGPTR = FORM == SFP_FORM_FP32 && !OD && LONG;
+        const char* q0 = nullptr;
+        const char* q1 = nullptr;
+        const char* q2 = nullptr;
+        if (REGPTR && full) {
+            const int h = lane >> 4, o = 16 * (lane & 15);
+            q0 = D[h] + o;
+            q1 = D[2 + h] + o;
+            q2 = D[4 + h] + o;
+        }
         auto issue = [&](int sb, unsigned char* dst) {
-            if (full) sfp_ring_issue_full<NC, OD>(D, sb, dst, lane);
-            else sfp_ring_issue<NC, OD>(D, sb, LONG ? left : (long long)len, dst, lane);
+            if (REGPTR && full) {
+                const unsigned int off = (unsigned int)sb * 256u;
+                sfp::cp_async16(dst + lane * 16, q0 + off, 16u);
+                sfp::cp_async16(dst + (lane + 32) * 16, q1 + off, 16u);
+                sfp::cp_async16(dst + (lane + 64) * 16, q2 + off, 16u);
+                if (lane < 2) sfp::cp_async16(dst + (lane + 96) * 16, D[NC] + sb * 32 + 16 * lane, 16u);
+                sfp::cp_async_commit();
+            } else if (full) {
+                sfp_ring_issue_full<NC, OD>(D, sb, dst, lane);
+            } else {
+                sfp_ring_issue<NC, OD>(D, sb, LONG ? left : (long long)len, dst, lane);
+            }
         };
 #pragma unroll
         for (int k = 0; k < STAGES - 1; ++k) {
