@@ -947,11 +947,16 @@ __device__ __forceinline__ void sfp_massive_body(const sfp_run_dev* __restrict__
 // below 2^-33 (float32 draws) or 2^-53 (float64 draws).  The pair-rate bound
 // of the photon's chi bin (R->pair_bound) times dt / gamma below that means
 // no draw passes: the photon is done at once, with no draw and no rate.
-// The photons it keeps (a few percent in a cascade) go, with their state,
-// to a 32-entry per-warp queue in shared memory and are tested in full 32
-// at a time, so the test's cost is paid by full warps instead of by every
-// warp that holds one such photon.  Results are those of testing
-// every photon.  Optical depth updates every photon's tau and tests each.
+// Before any field is evaluated, a photon's energy alone bounds its chi
+// (chi <= gamma (|E| + c|B|)_max / E_s, sfp_pair_reachable): most photons
+// of a cascade are too soft for any draw to pass anywhere in the pulse and
+// are done after reading their momentum.  The others go, with their stored
+// state, to a 32-entry per-warp queue in shared memory; full queues get the
+// position at t, the field, chi and the bound above, and the few photons
+// kept (a few percent) the draws and the rate, so this work is paid by full
+// warps instead of by every warp that holds one such photon.  Results are
+// those of testing every photon.  Optical depth updates every photon's tau
+// and tests each.
 // ---------------------------------------------------------------------------
 template <int FORM>
 __device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
@@ -979,7 +984,38 @@ __device__ __forceinline__ bool sfp_pair_possible(const sfp_run_dev* __restrict_
     }
 }
 
-// a warp's queue of kept photons: tile index and, with STATE, the state at t
+// chi per unit of gamma that no photon can exceed in this instance's field:
+// chi <= gamma (|E| + c|B|) / E_s, with sfp_field_bound(P) >= |E| + c|B| over
+// all space and time (generated with the field program), rounded up with a
+// margin for the rounding of the computed chi; +inf when the field has no
+// bound (a focused pulse, a user callable)
+SFP_DEVICE_INLINE float sfp_chi_per_gamma(const double* __restrict__ P) {
+    const double b = sfp_field_bound(P);
+    if (!(b < 1e299)) return __int_as_float(0x7f800000);
+    return __double2float_ru(b * (1.0 / sfp32::kEs) * (1.0 + 0x1p-10));
+}
+
+// Whether a photon's pair test can pass anywhere in the field, from its
+// energy alone: its chi is at most gamma cpg, and pbmax (the prefix maximum
+// of the pair-rate bound table, nondecreasing in chi) at that chi bounds the
+// rate.  False implies that sfp_pair_possible is false for this photon (the
+// same gamma and dt / gamma, a larger chi bin, a larger bound), so such a
+// photon skips the field evaluation: results are those of testing it.
+template <int FORM>
+__device__ __forceinline__ bool sfp_pair_reachable(float cpg, const float* __restrict__ pbmax, double ux, double uy,
+                                                   double uz, double dt) {
+    using namespace sfp;
+    if (FORM == SFP_FORM_FP64) {
+        const double ig = inv_gamma_photon(ux, uy, uz);
+        const float chimax = __double2float_ru((double)cpg / ig);
+        return !((double)pbmax[sfp_pair_bin(chimax)] * (dt * ig) < 0x1p-53);
+    } else {
+        const float g = sfp32::gamma_of(ux, uy, uz, true);
+        return !(pbmax[sfp_pair_bin(g * cpg)] * __fdividef(sfp32::d2f(dt), g) < 0x1p-33f);
+    }
+}
+
+// a warp's queue of photons whose pair test can pass: tile index and, with STATE, the stored state
 // (the float32 form: no second read of their rows); without it the batch
 // reads the rows again (the float64 form, whose kernel has no registers to
 // spare for the state held across a batch)
@@ -993,36 +1029,45 @@ struct sfp_pair_queue<true> {
     unsigned short e[32];
 };
 
-// the full pair test of the n queued photons (n <= 32), one per lane: a
-// converted photon is marked and its delta stored; returns the events
+// the n queued photons (n <= 32), one per lane: their positions at t, the
+// field filter (sfp_pair_possible), then the full pair test of those it
+// keeps; a converted photon is marked and its delta stored; returns the
+// events.  Every lane runs the filter (lanes past n on zeros, masked), as
+// the field program votes across the warp.
 template <int FORM, bool STATE>
 __device__ __forceinline__ unsigned int sfp_pair_batch(const sfp_run_dev* __restrict__ R, const sfp_qed_smem& T,
-                                                       const sfp_segment& S, const sfp_instance& I,
-                                                       const double* __restrict__ P, char* const* D,
-                                                       const sfp_pair_queue<STATE>& q, unsigned int n,
-                                                       long long base, double t, double dt, unsigned int step,
-                                                       double lag) {
+                                                       const float* __restrict__ pb, const sfp_segment& S,
+                                                       const sfp_instance& I, const double* __restrict__ P,
+                                                       char* const* D, const sfp_pair_queue<STATE>& q,
+                                                       unsigned int n, long long base, double t, double dt,
+                                                       unsigned int step, double lag) {
     using namespace sfp;
     const int lane = threadIdx.x & 31;
-    bool ev = false;
-    if ((unsigned int)lane < n) {
-        const int e = q.e[lane];
-        double x, y, z, ux, uy, uz;
+    const bool in = (unsigned int)lane < n;
+    const int e = in ? (int)q.e[lane] : 0;
+    double x = 0.0, y = 0.0, z = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+    if (in) {
         if constexpr (STATE) {
             x = q.x[lane], y = q.y[lane], z = q.z[lane];
             ux = q.ux[lane], uy = q.uy[lane], uz = q.uz[lane];
-        } else {  // the row again, advanced to t as the main loop did
+        } else {  // the row again (indices only in the float64 form's queue)
             x = reinterpret_cast<const double*>(D[0])[e], y = reinterpret_cast<const double*>(D[1])[e];
             z = reinterpret_cast<const double*>(D[2])[e], ux = reinterpret_cast<const double*>(D[3])[e];
             uy = reinterpret_cast<const double*>(D[4])[e], uz = reinterpret_cast<const double*>(D[5])[e];
-            if (S.push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);
         }
-        double tau = 0.0, delta = 0.0;
-        ev = sfp_pair_event<FORM, SFP_QED_REJECTION>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, base + e, tau,
-                                                     delta);
-        if (ev) {
-            reinterpret_cast<unsigned char*>(D[6])[e] = SFP_MARK;
-            reinterpret_cast<double*>(D[7])[e] = delta;
+    }
+    if (S.push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);  // the stored position advanced to t
+    const bool keep = in & sfp_pair_possible<FORM>(R, T, pb, S, P, x, y, z, ux, uy, uz, t);
+    bool ev = false;
+    if (__any_sync(0xffffffffu, keep)) {
+        if (keep) {
+            double tau = 0.0, delta = 0.0;
+            ev = sfp_pair_event<FORM, SFP_QED_REJECTION>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, base + e, tau,
+                                                         delta);
+            if (ev) {
+                reinterpret_cast<unsigned char*>(D[6])[e] = SFP_MARK;
+                reinterpret_cast<double*>(D[7])[e] = delta;
+            }
         }
     }
     return __popc(__ballot_sync(0xffffffffu, ev));
@@ -1054,6 +1099,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     constexpr bool QSTATE = FORM == SFP_FORM_FP32;  // the queue holds the kept photons' state
     __shared__ sfp_pair_queue<QSTATE> s_q[QUEUE ? SFP_TILE / 32 : 1];  // per-warp queue of kept photons
     __shared__ float s_pb[QUEUE ? SFP_PAIR_BOUND_BINS : 1];
+    __shared__ float s_pbmax[QUEUE ? SFP_PAIR_BOUND_BINS : 1];  // its prefix maximum
     sfp_step_state* st = R->st;
     if (st->skip || st->n_ptiles == 0) return;
     const long long n_tiles = st->n_ptiles;
@@ -1065,6 +1111,14 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
     const sfp_qed_smem T = sfp_stage_tables<FORM, QED>(R, s_tab);
     if (QUEUE)
         for (int k = threadIdx.x; k < SFP_PAIR_BOUND_BINS; k += blockDim.x) s_pb[k] = R->pair_bound[k];
+    __syncthreads();
+    if (QUEUE && threadIdx.x == 0) {
+        float m = 0.0f;
+        for (int k = 0; k < SFP_PAIR_BOUND_BINS; ++k) {
+            m = fmaxf(m, s_pb[k]);
+            s_pbmax[k] = m;
+        }
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = reinterpret_cast<unsigned char*>(s_tab) + R->ring_off + (size_t)warp * STAGES * SB;
@@ -1081,6 +1135,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         const sfp_segment& S = R->seg[si];
         const sfp_instance& I = R->inst[S.instance];
         const double* __restrict__ P = sfp_field_params(I);
+        const float cpg = QUEUE ? sfp_chi_per_gamma(P) : 0.0f;  // chi per gamma no photon exceeds here
         const long long N = R->n_buf_step[si];
         const long long base = (tile - R->pg.tile_start[pos]) * (long long)PT;
         if (base >= N) {  // alignment padding between segments: no photons
@@ -1148,13 +1203,14 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
             const bool alive = (LONG ? e < left : e < len) && stg[NC * 256 + lane] == 0;
             double x = sd[lane], y = sd[32 + lane], z = sd[64 + lane];
             double ux = sd[96 + lane], uy = sd[128 + lane], uz = sd[160 + lane];
-            // the position at t; the step's push is carried by the epoch
-            // (pos_epoch), so a photon that does not convert stores nothing
-            if (push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);
+            // the step's push is carried by the epoch (pos_epoch), so a photon
+            // that does not convert stores nothing
             if (QUEUE) {
-                // every lane runs the filter (dead lanes on their zero-filled
-                // stage entries); only the queue writes are conditional
-                const bool keep = alive & bw & sfp_pair_possible<FORM>(R, T, s_pb, S, P, x, y, z, ux, uy, uz, t);
+                // from its energy alone, whether a photon's pair test can pass
+                // anywhere in the field; those that can go, with their stored
+                // state, to the queue, where the position at t, the field and
+                // the rate bound are evaluated for full warps
+                const bool keep = alive & bw & push & sfp_pair_reachable<FORM>(cpg, s_pbmax, ux, uy, uz, dt);
                 // kept photons fill the queue; a full queue is tested at once and
                 // the sub-step's remaining kept photons start the next one
                 const unsigned int kb = __ballot_sync(0xffffffffu, keep);
@@ -1162,7 +1218,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                 if (keep && slot < 32u) sfp_pair_enqueue(q, slot, e, x, y, z, ux, uy, uz);
                 if (qn + nk >= 32u) {
                     __syncwarp();  // the queue entries are written
-                    cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, 32u, base, t, dt, step, lag);
+                    cnt += sfp_pair_batch<FORM, QSTATE>(R, T, s_pb, S, I, P, D, q, 32u, base, t, dt, step, lag);
                     __syncwarp();  // every lane has read its entry
                     if (keep && slot >= 32u) sfp_pair_enqueue(q, slot - 32u, e, x, y, z, ux, uy, uz);
                     qn = qn + nk - 32u;
@@ -1173,6 +1229,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
                 double tau = OD ? sd[192 + lane] : 0.0;
                 bool ev = false;
                 double delta = 0.0;
+                if (push) photon_shift<FORM>(x, y, z, ux, uy, uz, dt, lag);  // the position at t
                 if (alive && bw)
                     ev = sfp_pair_event<FORM, QED>(R, T, S, I, P, x, y, z, ux, uy, uz, t, step, i, tau, delta);
                 if (ev) {
@@ -1186,7 +1243,7 @@ __device__ __forceinline__ void sfp_photon_body(const sfp_run_dev* __restrict__ 
         }
         if (QUEUE && qn) {  // the tile's last kept photons
             __syncwarp();
-            cnt += sfp_pair_batch<FORM, QSTATE>(R, T, S, I, P, D, q, qn, base, t, dt, step, lag);
+            cnt += sfp_pair_batch<FORM, QSTATE>(R, T, s_pb, S, I, P, D, q, qn, base, t, dt, step, lag);
         }
         if (lane == 0) {
             R->pg.tile_cnt[tile] = cnt;

@@ -145,7 +145,32 @@ class Fields:
 
         p64 = program("double", _DEVICE_FN)
         p32 = program("float", _DEVICE_FN32)
-        return "\n".join(helpers) + "\n" + p64 + p32
+        return "\n".join(helpers) + "\n" + p64 + p32 + self._bound_source()
+
+    def _bound_source(self) -> str:
+        """CUDA C++ of ``sfp_field_bound(P)``: an upper bound of |E| + c|B| over
+        all space and time, the sum of the terms' bounds.  A Gaussian or simple
+        pulse has |E| <= |E0| (its transverse and temporal envelopes and the
+        focusing factor w0/w are at most 1; for the simple pulse only with an
+        even temporal order) and c|B| = |E|; a static field has its own
+        magnitudes; a focused pulse or a user callable has no bound here
+        (1e300).  The photon kernel turns it into a bound of chi per unit of
+        gamma (chi <= gamma (|E| + c|B|) / E_s)."""
+        lines = ["SFP_DEVICE_INLINE double sfp_field_bound(const double* __restrict__ P) {", "    double b = 0.0;"]
+        for k, t in enumerate(self.terms()):
+            o = k * N_PARAMS
+            if t.kind == KIND_GAUSSIAN:
+                lines.append(f"    b += 2.0 * fabs(P[{o}]);")
+            elif t.kind == KIND_SIMPLE:
+                lines.append(f"    b += fmod(P[{o + 9}], 2.0) == 0.0 ? 2.0 * fabs(P[{o}]) : 1e300;")
+            elif t.kind == KIND_STATIC:
+                lines.append(f"    b += sqrt(P[{o}] * P[{o}] + P[{o + 1}] * P[{o + 1}] + P[{o + 2}] * P[{o + 2}]) + "
+                             f"299792458.0 * sqrt(P[{o + 3}] * P[{o + 3}] + P[{o + 4}] * P[{o + 4}] + "
+                             f"P[{o + 5}] * P[{o + 5}]);")
+            else:
+                lines.append("    b += 1e300;")
+        lines += ["    return b;", "}", ""]
+        return "\n".join(lines)
 
     def params_device(self, device=None):
         """Parameter array on the CUDA device (cached per device)."""

@@ -124,3 +124,56 @@ def test_device_table_matches_the_restatement(rs):
     assert np.array_equal(np.isinf(got), np.isinf(ref)) and np.array_equal(got == 0, ref == 0)
     fin = np.isfinite(ref) & (ref > 0)
     np.testing.assert_allclose(got[fin], ref[fin], rtol=5e-7)
+
+
+def _host_bound(fields, tmp_path):
+    """The generated sfp_field_bound(P), compiled for the host."""
+    import subprocess
+    src = fields.cuda_source()
+    a = src.index("SFP_DEVICE_INLINE double sfp_field_bound")
+    code = ("#include <cmath>\nusing std::fabs; using std::sqrt; using std::fmod;\n#define SFP_DEVICE_INLINE inline\n"
+            + src[a:] + '\nextern "C" double bound(const double* P) { return sfp_field_bound(P); }\n')
+    # a new file name per field: the loader would hand back an earlier library of the same path
+    name = "b%d" % len(list(tmp_path.glob("b*.so")))
+    (tmp_path / f"{name}.cpp").write_text(code)
+    so = tmp_path / f"{name}.so"
+    subprocess.check_call(["g++", "-O1", "-shared", "-fPIC", str(tmp_path / f"{name}.cpp"), "-o", str(so)])
+    lib = ctypes.CDLL(str(so))
+    lib.bound.restype = ctypes.c_double
+    lib.bound.argtypes = [ctypes.c_void_p]
+    p = np.ascontiguousarray(fields.params(), dtype=np.float64)
+    return float(lib.bound(p.ctypes.data))
+
+
+def test_field_bound_covers_the_fields(tmp_path):
+    """The photon kernel skips the field evaluation of a photon whose energy
+    alone bounds its chi below any pair test (chi <= gamma (|E| + c|B|)_max
+    / E_s).  The generated bound must cover |E| + c|B| of the field at every
+    point: checked against the oracle's fields over the pulse, its peak
+    included, for a Gaussian pulse plus a static field and a simple pulse of
+    even temporal order; a simple pulse of odd order gets no bound."""
+    from sfparticles_b200 import fields as F
+    rng = np.random.default_rng(5)
+    ctau = C * 25e-15 / (2 * np.sqrt(np.log(2) / 2))
+    cases = [
+        (F.gaussian_laser_pulse(200.0, 3e-6, ctau, direction=-1, x0=0.0) + F.static_field(Ex=3e12, By=5e3),
+         orc.gaussian_laser_pulse(200.0, 3e-6, ctau, direction=-1, x0=0.0) + orc.static_field(Ex=3e12, By=5e3)),
+        (F.simple_laser_pulse(50.0, 2e-6, ctau, t_order=2, direction=1, x0=0.0),
+         orc.simple_laser_pulse(50.0, 2e-6, ctau, t_order=2, direction=1, x0=0.0)),
+    ]
+    for prod, ref in cases:
+        b = _host_bound(prod, tmp_path)
+        assert 0.0 < b < 1e299
+        worst = 0.0
+        for t in (-20e-15, 0.0, 7e-15):
+            n = 200_000
+            # points around the pulse centre (x = x0 + dir c t), the focus and the axis
+            x = rng.normal(0.0, 3e-6, n) + rng.choice([-1.0, 1.0], n) * C * t
+            y, z = rng.normal(0.0, 1.5e-6, n), rng.normal(0.0, 1.5e-6, n)
+            Ex, Ey, Ez, Bx, By, Bz = orc.field_eval(ref, x, y, z, t)
+            m = np.sqrt(Ex ** 2 + Ey ** 2 + Ez ** 2) + C * np.sqrt(Bx ** 2 + By ** 2 + Bz ** 2)
+            assert np.all(m <= b), (float(m.max()), b)
+            worst = max(worst, float(m.max()))
+        assert worst > 0.5 * b  # the pulse's peak was sampled: the bound is not loose by much
+    odd = F.simple_laser_pulse(50.0, 2e-6, ctau, t_order=3)
+    assert _host_bound(odd, tmp_path) >= 1e299
