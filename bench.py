@@ -59,9 +59,9 @@ BYTES_PAIR = 155    # pair event in the appends kernel: parent state + delta rea
 # DRAM bytes (read + write) over algorithmic bytes of one launch, from a
 # one-kernel ncu capture of the collision window at 1e6 e- (photon kernel:
 # 2.38e7 photons, 1.17 GB of state, larger than L2, so traffic scales with
-# the units processed): 1.1695e9 read + 0.0002e9 written against 1.1680e9.
+# the units processed): 1.1695e9 read + 0.0036e9 written against 1.1680e9.
 # Only kernels whose state exceeds L2 in that capture are listed.
-NCU_TRAFFIC_RATIO = {"photon": (1.169514e9 + 0.206080e6) / 1.167978920e9}
+NCU_TRAFFIC_RATIO = {"photon": (1.169452e9 + 3.648256e6) / 1.167978920e9}
 
 WORKLOAD = "scaled cascade: 1e7 e- (gamma0 2000 +-1%, sigma_perp 1um, sigma_par 5um) x LP Gaussian a0=200 " \
            "(0.8um, w0 3um, 25fs FWHM), photons + pairs, dt=T0/100, 3000 steps"
